@@ -1,0 +1,423 @@
+"""Benchmark: DFT sky-model subtraction, component-visibility evals/s.
+
+One step = one pass of the DFT subtract over one chunk of the config-2 dataset
+(64 antennas / 2016 baselines, 4 IFs x 256 channels, 4 polarizations, 20000
+point components with spectral index), `--rows` records per chunk (default
+100800 = 50 integrations; the full 4.032e6-row dataset, ~198 GB, is 40 such
+chunks and does not fit in HBM).  Evals = components x rows x channels x IFs.
+
+  value   device-resident: records already in HBM, one kernel launch per step,
+          CUDA events on the launch stream.
+  e2e     the reference-facing C ABI call ObitCUDASkyModelDFTCalc-equivalent
+          (obit_dft_calc) on a pinned HOST buffer: H2D, kernels and D2H per step.
+
+Multi-GPU (torchrun): every rank subtracts the same model from its own chunk
+(weak scaling, no data-path collective); the component table is broadcast once.
+`--impl reference` times the reference CPU DFT restatement (oracle/_ref) on the
+host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_PER_EVAL = 10.0  # complex rotate (6) + accumulate (4), algorithmic
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=100800)
+    ap.add_argument("--ncomp", type=int, default=20000)
+    ap.add_argument("--flavor", default="recur", choices=["recur", "plain"])
+    ap.add_argument("--K", type=int, default=0)
+    ap.add_argument("--ct", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---- workload ------------------------------------------------------------------
+
+
+def workload_geometry(rank: int, rows: int, ncomp: int):
+    """uvw for this rank's chunk and the (shared) component table."""
+    from obit_b200 import uvdata as U
+
+    nbl = 2016
+    nint_total = 2000
+    nint = max(1, (rows + nbl - 1) // nbl)
+    rng = np.random.default_rng(2)
+    pos = U.array_layout(64, 36e3, rng)
+    freq = 1.4e9
+    fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
+    # this rank's integrations: a contiguous slice of the 2000-integration track
+    i0 = (rank * nint) % max(1, nint_total - nint + 1)
+    uvw_all = U.make_uvw(pos, nint_total, 45.0, 4.0, 34.0, freq).reshape(nint_total, nbl, 3)
+    uvw = uvw_all[i0:i0 + nint].reshape(-1, 3)[:rows]
+    sky = U.make_comps(U.MOD_POINT_SPEC, ncomp, np.random.default_rng(4), radius_deg=1.0,
+                       nterm=1, ref_freq=freq)
+    return uvw, fa, freq, sky
+
+
+def build_vis(torch, uvw, nstok, nchan, nif, device, seed):
+    rows = uvw.shape[0]
+    nrparm = 5
+    ncorr = nstok * nchan * nif
+    lrec = nrparm + 3 * ncorr
+    g = torch.Generator(device=device).manual_seed(seed)
+    vis = torch.empty((rows, lrec), dtype=torch.float32, device=device)
+    c = vis[:, nrparm:].view(rows, ncorr, 3)
+    c[:, :, :2] = 0.01 * torch.randn((rows, ncorr, 2), generator=g, device=device)
+    c[:, :, 2] = 1.0
+    vis[:, 0:3] = torch.from_numpy(uvw.astype(np.float32)).to(device)
+    vis[:, 3] = 256.0
+    vis[:, 4] = 0.0
+    return vis
+
+
+# ---- clocks ----------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        pw = [float(s[3]) for s in self.samples if s[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None,
+                "samples": len(self.samples), "reasons": sorted(reasons)}
+
+
+# ---- peaks -------------------------------------------------------------------------
+
+
+def fp32_peak_tflops(torch, device) -> float:
+    """Measured FP32 peak: cuBLAS SGEMM 8192^3 with TF32 disabled (best of 5)."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn((n, n), device=device)
+    b = torch.randn((n, n), device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+# ---- CPU baseline ------------------------------------------------------------------
+
+
+def cpu_baseline(rows_uvw, fa, freq, sky, seconds: float):
+    """Reference CPU DFT restatement (oracle/_ref: the reference's ObitSinCosVec /
+    ObitExpVec, FP32 phase, rows split over pthreads as ObitSkyModelFTDFT) on a
+    bounded sample of the same workload; returns (evals/s, cores, sample text, kind)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    from obit_b200 import uvdata as U
+    from obit_b200.skymodel import SkyModelParams
+
+    cores = oracle.nthreads_default()
+    have_ref = oracle.have_refcpu()
+    kind = "port"
+
+    def run(nrow):
+        uvw = rows_uvw[:nrow]
+        uv = U.make_uvdata(uvw, 4, 256, 4, freq, fa, np.random.default_rng(9))
+        t0 = time.perf_counter()
+        if have_ref:
+            oracle.apply_refcpu(uv, sky, SkyModelParams(), nthreads=cores)
+        else:
+            oracle.apply_fp64(uv, sky, SkyModelParams(), nthreads=cores)
+        return time.perf_counter() - t0
+
+    nrow = cores
+    dt = run(nrow)
+    if dt < seconds / 3:
+        nrow = max(cores, int(nrow * (seconds / max(dt, 1e-3))))
+        nrow = min(nrow, len(rows_uvw))
+        dt = run(nrow)
+    evals = nrow * 1024 * sky.ncomp
+    name = "reference CPU DFT restatement with the reference's ObitSinCosVec/ObitExpVec" if have_ref \
+        else "FP64 oracle (reference vector math not built)"
+    return evals / dt, cores, f"{nrow} rows x 1024 channels x {sky.ncomp} components ({name}), {dt:.1f} s", kind
+
+
+# ---- arms ------------------------------------------------------------------------
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    uvw, fa, freq, sky = workload_geometry(0, max(args.rows, 64), args.ncomp)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    from obit_b200 import uvdata as U
+    from obit_b200.skymodel import SkyModelParams
+
+    cores = oracle.nthreads_default()
+    have_ref = oracle.have_refcpu()
+    nrow = max(cores, 8)
+    uv = U.make_uvdata(uvw[:nrow], 4, 256, 4, freq, fa, np.random.default_rng(9))
+    fn = oracle.apply_refcpu if have_ref else oracle.apply_fp64
+    for _ in range(args.warmup):
+        fn(uv, sky, SkyModelParams(), nthreads=cores)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fn(uv, sky, SkyModelParams(), nthreads=cores)
+        ts.append(time.perf_counter() - t0)
+    evals = nrow * 1024 * sky.ncomp
+    v = evals * len(ts) / sum(ts) / 1e9
+    line = {
+        "impl": "reference", "metric": "component-visibility evals/s (DFT subtract)",
+        "value": v, "unit": "Gevals/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(ts) / len(ts), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP32 phase, FP64 component sum)", "data": "synthetic",
+        "config": config_block(args, sky, nrow_override=nrow),
+        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": cores,
+                         "kind": "reference" if have_ref else "port",
+                         "sample": f"{nrow} rows x 1024 channels x {sky.ncomp} components per step"},
+        "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, sky, nrow_override=None, kernel=None):
+    rows = nrow_override or args.rows
+    return {"workload": f"config2 chunk: {rows} records (64 antennas, 2016 baselines) x 4 IF x 256 "
+                        f"ch x 4 pol, {sky.ncomp} point components with spectral index; the "
+                        "4.032e6-record dataset is streamed in such chunks",
+            "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024, "polarizations": 4,
+            "model": "PointSpec nterm=1", "w_term": True,
+            "l2": "inputs larger than L2 (record chunk >> 126 MB)",
+            "kernel": kernel}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from obit_b200 import _lib
+    from obit_b200 import uvdata as U
+    from obit_b200.skymodel import GPUSkyModel, SkyModelParams
+
+    uvw, fa, freq, sky = workload_geometry(rank, args.rows, args.ncomp)
+    if world > 1:  # replicate the component table from rank 0 (one broadcast, outside timing)
+        t = torch.from_numpy(sky.comps).to(device)
+        dist.broadcast(t, 0)
+        sky.comps = t.cpu().numpy()
+    rows = uvw.shape[0]
+    nstok, nchan, nif = 4, 256, 4
+    d_vis = build_vis(torch, uvw, nstok, nchan, nif, device, seed=100 + rank)
+    lrec = d_vis.shape[1]
+
+    # host-side descriptor and the GPU sky model (C host mirror -> C ABI)
+    want_e2e = not args.no_e2e
+    host = torch.empty((rows, lrec), dtype=torch.float32, pin_memory=True) if want_e2e else None
+    if want_e2e:
+        host.copy_(d_vis.cpu())
+        uvh = U.UVData(host.numpy(), nstok, nchan, nif, freq, fa)
+    else:
+        uvh = U.UVData(np.zeros((rows, lrec), np.float32)[:1], nstok, nchan, nif, freq, fa)
+        uvh.vis = np.zeros((1, lrec), np.float32)
+    params = SkyModelParams(nVisPIO=rows if want_e2e else 1, GPU_no=local, numberPoln=2)
+    gm = GPUSkyModel(f"bench{rank}")
+    gm.DFTInit(sky, uvh, params)
+    flavor = _lib.OBIT_DFT_PLAIN if args.flavor == "plain" else _lib.OBIT_DFT_RECUR
+    gm.set_kernel(flavor, args.K, args.ct)
+    gm.DFTSetMod(sky)
+    lib = _lib.load()
+
+    stream = torch.cuda.Stream(device=device)
+    sp = stream.cuda_stream
+    evals = rows * nchan * nif * sky.ncomp
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            gm.calc_device(d_vis.data_ptr(), rows, sp)
+    torch.cuda.synchronize()
+    gm.check()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    per_launch = []
+    with sampler:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            gm.calc_device(d_vis.data_ptr(), rows, sp)
+            b.record(stream)
+            per_launch.append((a, b))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    gm.check()
+    t_ms = ev0.elapsed_time(ev1)
+    launch_ms = [a.elapsed_time(b) for a, b in per_launch]
+    if world > 1:
+        tt = torch.tensor([t_ms], device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * evals * args.steps / (t_ms * 1e-3)
+
+    # e2e: host buffer through obit_dft_calc (H2D + kernels + D2H inside)
+    e2e = None
+    if want_e2e:
+        gi = gm.gpuinfo
+        C.memmove(gi.contents.h_data, host.data_ptr(), rows * lrec * 4)
+        gi.contents.nvis = rows
+        gi.contents.h_visInfo.contents.nvis = rows
+        for _ in range(1):
+            _lib.check(lib.obit_dft_calc(gi))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            _lib.check(lib.obit_dft_calc(gi))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([dt], device=device)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dt = float(tt.item())
+        e2e = {"value": world * evals * args.steps / dt / 1e9, "unit": "Gevals/s",
+               "h2d_bytes_per_step": rows * lrec * 4, "d2h_bytes_per_step": rows * lrec * 4,
+               "timing": "wall clock around the synchronous C-ABI call, max over ranks"}
+
+    line = None
+    if rank == 0:
+        peak = fp32_peak_tflops(torch, device)
+        avg_launch_s = statistics.mean(launch_ms) * 1e-3
+        achieved = evals * FLOPS_PER_EVAL / avg_launch_s / 1e12
+        cpu = None
+        if not args.no_cpu:
+            v, cores, sample, kind = cpu_baseline(uvw, fa, freq, sky, args.cpu_seconds)
+            cpu = {"value": v / 1e9, "unit": "Gevals/s", "cores": cores, "kind": kind, "sample": sample}
+        kern = f"{args.flavor} K={gm_kernel_K(args)} ct={args.ct or 64}"
+        line = {
+            "metric": "component-visibility evals/s (DFT subtract, max rel err <= 1e-5 vs FP64)",
+            "value": value / 1e9, "unit": "Gevals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (split-FP32 phase)" if args.flavor == "recur" else "f32 (FP64 phase)",
+            "data": "synthetic (seeded uvw, noise visibilities, random components)",
+            "config": config_block(args, sky, kernel=kern),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
+                         "flops_per_eval": FLOPS_PER_EVAL},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    gm.DFTShutdown()
+    gm.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def gm_kernel_K(args):
+    if args.K:
+        return args.K
+    return 16 if args.flavor == "recur" else 16
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,201 @@
+/*
+ * obit_dft.h - C ABI of the B200 DFT sky-model predict / subtract library
+ * (libobit_dft.so).  Plain C: pointers, ints and floats, no C++ or torch types.
+ *
+ * Two levels are exported:
+ *
+ *  1. The reference's CUDA-layer entry points, same names and argument, so the
+ *     library links in place of ObitCUDASkyModel.o under the unmodified
+ *     ObitGPUSkyModel.c:
+ *       ObitCUDASkyModelDFTInit / SetMod / Calc / Shutdown (GPUInfo*)
+ *     replacing ObitSystem/Obit/include/ObitCUDASkyModel.h:44-54 (defined at
+ *     ObitSystem/Obit/src/ObitCUDASkyModel.cu:727-783).  The structures below
+ *     keep the field order and types of ObitCUDASkyModelInfoDef.h:42-195 so a
+ *     GPUInfo filled by ObitGPUSkyModelDFTInit / DFTSetMod
+ *     (ObitSystem/Obit/src/ObitGPUSkyModel.c:207-491) is read as is.
+ *
+ *  2. Status-returning forms of the same four calls plus additions the
+ *     reference has no equivalent for (FP64 frequency side table, CPU-reference
+ *     polarization rules, kernel choice, a device-resident call and a
+ *     multi-facet batch).  Every call returns OBIT_DFT_OK (0) or an error code;
+ *     obit_dft_last_error() gives the calling thread's last message.  Nothing
+ *     in the library calls exit(), abort() or cudaDeviceReset().
+ */
+#ifndef OBIT_DFT_H
+#define OBIT_DFT_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference-layout types (ObitCUDASkyModelInfoDef.h:42-195) ---------- */
+
+/* Sky model component types supported on the GPU
+ * (ObitCUDASkyModelInfoDef.h:44-52). */
+enum gpuModType {
+  GPUModTypePoint = 0,  /* point */
+  GPUModTypePointSpec,  /* point, spectrum as polynomial in ln(nu/nu0) */
+  GPUModTypePointTSpec, /* point, tabulated spectrum per coarse plane */
+  GPUModTypeGauss,      /* elliptical Gaussian */
+  GPUModTypeGaussSpec,  /* Gaussian, polynomial spectrum */
+  GPUModTypeGaussTSpec  /* Gaussian, tabulated spectrum */
+};
+typedef enum gpuModType GPUModType;
+
+/* Operation applied to the data (ObitCUDASkyModelInfoDef.h:58-63). */
+enum gpuOpType {
+  GPUOpTypeSub = 0, /* data -= model */
+  GPUOpTypeDiv,     /* data /= model, weight *= |model| */
+  GPUOpTypeRepl     /* data = model */
+};
+typedef enum gpuOpType GPUOpType;
+
+/* Visibility layout (ObitCUDASkyModelInfoDef.h:66-123).  Increments incf,
+ * incif, incs are in correlations (3 floats each), as ObitGPUSkyModel.c fills
+ * them (desc->incf/3 ...). */
+typedef struct {
+  int nvis;   /* records in the buffer */
+  int nprod;  /* correlations per record */
+  int nrparm; /* random parameters per record */
+  int lenvis; /* floats per record */
+  int nchan;
+  int ilocu, ilocv, ilocw, iloct, ilocb, ilocsu; /* random-parameter offsets */
+  int chanb, chane; /* selected channels, 0-relative inclusive */
+  int incf;         /* correlations between channels */
+  int nIF;
+  int IFb, IFe;     /* selected IFs */
+  int incif;        /* correlations between IFs */
+  int nstok;
+  int stokb, stoke; /* selected polarizations */
+  int incs;         /* correlations between polarizations */
+  int stype;        /* 0 IQUV, 1 RR/LL/RL/LR, 2 XX/YY/XY/YX */
+  int kincif;       /* IF increment in freqScale */
+  int kincf;        /* channel increment in freqScale */
+  float *freqRat;   /* host: uv reference freq / model (or coarse-plane) freq */
+  float *d_freqRat; /* device copy of freqRat */
+  float *freqScale; /* device: nu/nu_uvref per (channel, IF), nchan*nIF floats */
+} GPUVisInfo;
+
+/* Model description (ObitCUDASkyModelInfoDef.h:125-146). */
+typedef struct {
+  int nterm;          /* spectral terms */
+  int size;           /* floats per component */
+  int doSwap;         /* multiply the model of polarization 3 (LR) by i */
+  GPUModType type;
+  GPUOpType opType;
+  int *specIndex;     /* host: coarse plane per (channel, IF), tabulated spectra */
+  int *d_specIndex;   /* device copy of specIndex */
+  int nmodel[4];      /* components per polarization */
+  float *model[4];    /* device component tables per polarization */
+  float stokFact[4];  /* multiplier per polarization */
+} GPUModelInfo;
+
+/* Per-instance state (ObitCUDASkyModelInfoDef.h:148-195).  stream/cycleDone
+ * are arrays of cudaStream_t / cudaEvent_t, declared as void* so that this
+ * header needs no CUDA include; the layout is the same. */
+typedef struct {
+  int nvis;
+  int nchan;
+  int nrparm;
+  int lenvis;
+  int modelSize;
+  int nstream;
+  int prtLv;
+  int oldnVisPIO;
+  int cuda_device;
+  int bufferSize;
+  int nmodel[4];
+  float *d_model[4];
+  float *d_freq;
+  float *h_data;   /* pinned host buffer of nvis records */
+  float **d_data;  /* nstream device buffers of (nvis+3)*lenvis/nstream floats */
+  GPUVisInfo *d_visInfo, *h_visInfo;
+  GPUModelInfo *d_modelInfo, *h_modelInfo;
+  void **stream;
+  void **cycleDone;
+} GPUInfo;
+
+/* ---- level 1: the reference's CUDA-layer symbols ------------------------ */
+
+/* Replaces ObitCUDASkyModelDFTInit (ObitCUDASkyModel.h:44-45,
+ * ObitCUDASkyModel.cu:727-731): binds library state to this GPUInfo on
+ * gpuInfo->cuda_device.  Call after the GPUInfo fields are filled. */
+void ObitCUDASkyModelDFTInit(GPUInfo *gpuInfo);
+
+/* Replaces ObitCUDASkyModelDFTSetMod (ObitCUDASkyModel.h:47-48,
+ * ObitCUDASkyModel.cu:733-744): takes the component table now in
+ * gpuInfo->d_model[0] (nmodel[0] rows of modelSize floats) and the model
+ * description in h_modelInfo. */
+void ObitCUDASkyModelDFTSetMod(GPUInfo *gpuInfo);
+
+/* Replaces ObitCUDASkyModelDFTCalc (ObitCUDASkyModel.h:50-51,
+ * ObitCUDASkyModel.cu:746-765): applies the model to the nvis records in the
+ * pinned buffer gpuInfo->h_data, in place, synchronously. */
+void ObitCUDASkyModelDFTCalc(GPUInfo *gpuInfo);
+
+/* Replaces ObitCUDASkyModelDFTShutdown (ObitCUDASkyModel.h:53-54,
+ * ObitCUDASkyModel.cu:767-783): releases this GPUInfo's library state.  Unlike
+ * the reference it does not reset the device. */
+void ObitCUDASkyModelDFTShutdown(GPUInfo *gpuInfo);
+
+/* ---- level 2: status-returning API -------------------------------------- */
+
+enum {
+  OBIT_DFT_OK = 0,
+  OBIT_DFT_EBADARG = 1,     /* invalid argument or descriptor */
+  OBIT_DFT_ECUDA = 2,       /* CUDA runtime error */
+  OBIT_DFT_EUNSUPPORTED = 3,/* model type / layout not supported */
+  OBIT_DFT_EKERNEL = 4      /* a kernel reported an internal error */
+};
+
+/* Kernel flavors for obit_dft_set_kernel. */
+enum {
+  OBIT_DFT_RECUR = 0, /* split-FP32 phase + complex channel recurrence (default) */
+  OBIT_DFT_PLAIN = 1  /* FP64 phase, one sin/cos per component-visibility */
+};
+
+/* Status forms of the four calls above. */
+int obit_dft_init(GPUInfo *gpuInfo);
+int obit_dft_set_mod(GPUInfo *gpuInfo);
+int obit_dft_calc(GPUInfo *gpuInfo);
+int obit_dft_shutdown(GPUInfo *gpuInfo);
+
+/* FP64 frequency side table (no reference counterpart; the reference passes
+ * only FP32 freqScale).  freqArr: nchan*nIF channel frequencies in Hz indexed
+ * like freqScale (ObitUVDesc.freqArr, ObitUVDesc.c:506-617); uvRefFreq: the
+ * data reference frequency (desc->freq); modelRefFreq: reference frequency of
+ * polynomial spectra (image CRVAL of the frequency axis; 0 = uvRefFreq);
+ * specFreq/nSpec: coarse-plane frequencies of tabulated spectra (may be NULL).
+ * With it the phase is formed from FP64 frequencies; without it from the FP32
+ * freqScale the reference supplies. */
+int obit_dft_set_freq(GPUInfo *gpuInfo, const double *freqArr, int nfreq, double uvRefFreq,
+                      double modelRefFreq, const double *specFreq, int nSpec);
+
+/* Polarization rules of the reference CPU DFT (ObitSkyModel.c:2787-2849)
+ * instead of the per-polarization stokFact of GPUModelInfo: the model is
+ * multiplied by stokFactor after each polarization actually written, and by
+ * i for every polarization when doFlip.  cpuRules = 0 restores stokFact. */
+int obit_dft_set_poln(GPUInfo *gpuInfo, int cpuRules, float stokFactor, int doFlip);
+
+/* Kernel flavor, channels per thread (1, 4, 8, 16, 32) and components per
+ * shared-memory tile; 0 keeps the current / tuned value. */
+int obit_dft_set_kernel(GPUInfo *gpuInfo, int flavor, int chanPerThread, int compsPerTile);
+
+/* Device-resident form of Calc: applies the model to nvis records already in
+ * device memory at d_vis (lenvis floats each), asynchronously on `stream`
+ * (a cudaStream_t; NULL = default stream).  No host copies. */
+int obit_dft_calc_device(GPUInfo *gpuInfo, float *d_vis, int nvis, void *stream);
+
+/* Reads and clears the kernels' device error flag (synchronizes the device):
+ * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */
+int obit_dft_check(GPUInfo *gpuInfo);
+
+/* Last error message of the calling thread ("" if none). */
+const char *obit_dft_last_error(void);
+
+/* Library version (major*10000 + minor*100 + patch). */
+int obit_dft_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OBIT_DFT_H */

@@ -1,0 +1,79 @@
+// Host-side planning for the DFT kernels: channel blocks, tile shape, shared
+// memory, and the launch itself.  Plain C++ over the kernel parameter block;
+// no torch types.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dft_kernels.cuh"
+
+namespace obit {
+
+// Everything the planner needs to describe one visibility layout + model.
+struct LayoutDesc {
+  int lrec = 0, nrparm = 0, ilocu = 0, ilocv = 1, ilocw = 2;
+  int nchan = 1, nif = 1, nstok = 1;
+  int incs = 3, incf = 3, incif = 3;  // floats
+  int kincf = 1, kincif = 1;          // frequency-table increments
+  int chanb = 0, chane = 0;           // selected channels (0-rel, inclusive)
+  int ifb = 0, ife = 0;               // selected IFs
+  int stokb = 0, stoke = 0;           // selected polarizations
+  std::vector<double> fscale;         // nu/nu_uvref per (chan, IF) table index
+  std::vector<double> lnspec;         // Spec: ln(nu/nu_model); TSpec: ln(nu/nu_plane)
+  std::vector<int> specIndex;         // TSpec plane per (chan, IF)
+};
+
+struct ModelDesc {
+  int kind = kPoint;  // ModelKind
+  int nterm = 0;
+  int lcomp = 4;      // floats per component in the source table
+  int ncomp = 0;
+  int nspec = 0;      // planes for tabulated spectra
+};
+
+struct ApplyDesc {
+  int op = kOpSub;
+  int flipMask = 0;
+  int cumulative = 1;
+  float stokFactor = 1.0f;
+  float polFact[kMaxPol] = {1.f, 1.f, 1.f, 1.f};
+};
+
+struct TuneDesc {
+  int flavor = kFlavorRecur;
+  int K = 16;   // channels per thread
+  int ct = 64;  // components per shared-memory tile
+};
+
+// A compiled plan: block table on the device plus the fixed kernel fields.
+struct Plan {
+  KParams kp{};                    // vis / nvis / rowBase / comps filled at launch
+  std::vector<BlockDesc> blocks;   // host copy
+  BlockDesc* d_blocks = nullptr;   // device copy (owned)
+  size_t smemBytes = 0;
+  int gridCap = 0;                 // CTAs resident across the device
+  TuneDesc tune;
+  ModelDesc model;
+  bool linear = true;              // every block has a uniform channel increment
+  double maxNonLin = 0.0;          // largest deviation from a linear frequency run
+};
+
+// Padded component stride (floats): multiple of 4 so tiles are 16-byte aligned.
+int comp_stride(const ModelDesc& m);
+
+// Build the plan (allocates the device block table).  Returns 0 or an error
+// code with a message in err.
+int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
+               Plan* plan, std::string* err);
+void free_plan(Plan* plan);
+
+// Launch on `stream` over rows [rowBase, rowBase + nvis) of d_vis.
+int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const float* d_comps,
+                int* d_err, cudaStream_t stream, std::string* err);
+
+// Supported channel-block lengths.
+bool valid_K(int K);
+
+}  // namespace obit

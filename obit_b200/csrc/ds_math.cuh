@@ -1,0 +1,68 @@
+// Split-FP32 ("double-single") arithmetic used to form the DFT phase argument
+// without FP64.  A value is carried as an unevaluated sum hi + lo of two floats
+// with |lo| <= ulp(hi)/2, giving ~48 significant bits.
+//
+// The building blocks are the classical error-free transformations:
+//   two_sum   (Knuth, TAOCP vol. 2, 4.2.2, Theorem B)
+//   fast_two_sum (Dekker 1971, requires |a| >= |b|)
+//   two_prod  via fused multiply-add (exact product error)
+// and the Dekker/Bailey double-single product.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace obit {
+
+struct ds {
+  float hi, lo;
+};
+
+__device__ __forceinline__ ds two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  float bb = __fsub_rn(s, a);
+  float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+  return {s, e};
+}
+
+__device__ __forceinline__ ds fast_two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  float e = __fsub_rn(b, __fsub_rn(s, a));
+  return {s, e};
+}
+
+__device__ __forceinline__ ds two_prod(float a, float b) {
+  float p = __fmul_rn(a, b);
+  float e = __fmaf_rn(a, b, -p);
+  return {p, e};
+}
+
+// (a.hi + a.lo) * (b.hi + b.lo), relative error ~2^-46.
+__device__ __forceinline__ ds ds_mul(ds a, ds b) {
+  float p = __fmul_rn(a.hi, b.hi);
+  float e = __fmaf_rn(a.hi, b.hi, -p);
+  e = __fmaf_rn(a.hi, b.lo, __fmaf_rn(a.lo, b.hi, e));
+  return fast_two_sum(p, e);
+}
+
+// x*u + y*v + z*w for float inputs, returned as a double-single.  The three
+// products are exact as pairs; the sums are error-free except for the final
+// accumulation of the low parts.
+__device__ __forceinline__ ds ds_dot3(float x, float u, float y, float v, float z, float w) {
+  ds p1 = two_prod(x, u);
+  ds p2 = two_prod(y, v);
+  ds p3 = two_prod(z, w);
+  ds s = two_sum(p1.hi, p2.hi);
+  ds t = two_sum(s.hi, p3.hi);
+  float lo = __fadd_rn(__fadd_rn(__fadd_rn(p1.lo, p2.lo), __fadd_rn(p3.lo, s.lo)), t.lo);
+  return fast_two_sum(t.hi, lo);
+}
+
+// Fractional part of a double-single number of turns, in [-0.5, 0.5] (up to
+// rounding), returned as float plus the float rounding residual.
+__device__ __forceinline__ ds ds_frac_turns(ds t) {
+  float n = rintf(t.hi);
+  float d = __fsub_rn(t.hi, n);  // exact: n is the nearest integer to t.hi
+  ds r = fast_two_sum(d, t.lo);  // |d| <= 0.5 >= |t.lo| except when both tiny
+  return r;
+}
+
+}  // namespace obit

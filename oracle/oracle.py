@@ -1,0 +1,177 @@
+"""Test infrastructure: ctypes front end of the CPU oracles (oracle_dft.c and
+the reference-derived restatement in _ref/).  Only tests, the smoke check and
+bench.py's CPU-baseline leg import this module; the product never does.
+
+A job is described with the same objects the product takes (UVData, SkyComps,
+SkyModelParams), mapped to the reference CPU semantics used by the host mirror:
+polarization factors follow stokFactor/doFlip (ObitSkyModel.c:2787-2849) and the
+channel frequency ratio is FP64 freqArr/freq (exact=True) or the FP32
+freqScale the reference GPU interface carries (exact=False).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_A = HERE / "liboracle_dft.so"
+LIB_B = HERE / "_ref" / "libobit_refcpu.so"
+
+
+class OracleJob(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "nvis", "lrec", "nrparm", "ilocu", "ilocv", "ilocw", "incs", "incf", "incif", "nchan",
+        "nif", "kincf", "kincif", "startChannel", "numberChannel", "startIF", "numberIF",
+        "startPoln", "numberPoln", "modType", "nterm", "lcomp", "ncomp")] + [
+        ("comps", C.POINTER(C.c_float)),
+        ("doDivide", C.c_int), ("doReplace", C.c_int), ("flipMask", C.c_int),
+        ("stokFactor", C.c_float), ("polFact", C.c_float * 4),
+        ("fscale", C.POINTER(C.c_double)), ("fscale32", C.POINTER(C.c_float)),
+        ("lnspec", C.POINTER(C.c_double)), ("specIndex", C.POINTER(C.c_int)),
+    ]
+
+
+_libA = None
+_libB = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+def lib_a() -> C.CDLL:
+    global _libA
+    if _libA is None:
+        if not LIB_A.exists():
+            build()
+        _libA = C.CDLL(str(LIB_A))
+        for fn in (_libA.oracle_model_fp64,):
+            fn.restype = C.c_int
+            fn.argtypes = [C.POINTER(OracleJob), C.POINTER(C.c_float), C.POINTER(C.c_double),
+                           C.POINTER(C.c_double), C.c_int]
+        _libA.oracle_apply_fp64.restype = C.c_int
+        _libA.oracle_apply_fp64.argtypes = [C.POINTER(OracleJob), C.POINTER(C.c_float), C.c_int]
+    return _libA
+
+
+def have_refcpu() -> bool:
+    return LIB_B.exists()
+
+
+def lib_b() -> C.CDLL:
+    global _libB
+    if _libB is None:
+        if not LIB_B.exists():
+            raise FileNotFoundError(f"{LIB_B} not built (needs the reference sources once)")
+        _libB = C.CDLL(str(LIB_B))
+        _libB.refcpu_apply.restype = C.c_int
+        _libB.refcpu_apply.argtypes = [C.POINTER(OracleJob), C.POINTER(C.c_float), C.c_int]
+    return _libB
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class Job:
+    """An OracleJob plus the arrays it points into."""
+
+    def __init__(self, uv, sky, params=None, exact: bool = True):
+        from obit_b200.skymodel import OP_DIV, OP_REPL, SkyModelParams
+        p = params or SkyModelParams()
+        j = OracleJob()
+        j.nvis = uv.nvis
+        j.lrec = uv.lrec
+        j.nrparm = uv.nrparm
+        j.ilocu, j.ilocv, j.ilocw = uv.ilocu, uv.ilocv, uv.ilocw
+        j.incs, j.incf, j.incif = uv.incs, uv.incf, uv.incif
+        j.nchan, j.nif = uv.nchan, uv.nif
+        j.kincf, j.kincif = uv.kincf, uv.kincif
+        j.startChannel = (p.startChannel if p.startChannel > 0 else 1) - 1
+        j.numberChannel = p.numberChannel if p.numberChannel > 0 else uv.nchan - j.startChannel
+        j.startIF = (p.startIF if p.startIF > 0 else 1) - 1
+        j.numberIF = p.numberIF if p.numberIF > 0 else uv.nif - j.startIF
+        j.startPoln = (p.startPoln if p.startPoln > 0 else 1) - 1
+        j.numberPoln = p.numberPoln if p.numberPoln > 0 else min(2, uv.nstok)
+        j.modType = sky.gpu_type
+        j.nterm = sky.nterm
+        self.comps = np.ascontiguousarray(sky.comps, dtype=np.float32)
+        j.lcomp = self.comps.shape[1]
+        j.ncomp = self.comps.shape[0]
+        j.comps = _p(self.comps, C.c_float)
+        j.doDivide = int(p.op == OP_DIV)
+        j.doReplace = int(p.op == OP_REPL)
+        j.flipMask = 0xF if p.doFlip else 0
+        j.stokFactor = p.stokFactor
+        for i in range(4):
+            j.polFact[i] = 1.0
+        fa = np.asarray(uv.freqArr, dtype=np.float64)
+        self.fscale32 = np.ascontiguousarray(uv.fscale, dtype=np.float32)
+        if exact:
+            self.fscale = np.ascontiguousarray(fa / uv.freq)
+        else:
+            self.fscale = self.fscale32.astype(np.float64)
+        j.fscale = _p(self.fscale, C.c_double)
+        j.fscale32 = _p(self.fscale32, C.c_float)
+        self.lnspec = None
+        self.specIndex = None
+        if sky.gpu_type in (1, 4):
+            ref = sky.refFreq if sky.refFreq > 0 else uv.freq
+            nu = fa if exact else self.fscale * uv.freq
+            self.lnspec = np.ascontiguousarray(np.log(nu / ref))
+        elif sky.gpu_type in (2, 5):
+            self.specIndex = np.ascontiguousarray(sky.specIndex, dtype=np.int32)
+            nu = fa if exact else self.fscale * uv.freq
+            self.lnspec = np.ascontiguousarray(np.log(nu / sky.specFreq[self.specIndex]))
+            j.specIndex = _p(self.specIndex, C.c_int)
+        if self.lnspec is not None:
+            j.lnspec = _p(self.lnspec, C.c_double)
+        self.job = j
+        self.uv = uv
+
+
+def nthreads_default() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None):
+    """FP64 component sum and L1 norm per (row, IF, channel):
+    returns (model complex128 (nvis, nif, nchan), l1 float64 (nvis, nif, nchan));
+    unselected entries are NaN."""
+    jb = Job(uv, sky, params, exact)
+    nfreq = uv.nchan * uv.nif
+    model = np.full((uv.nvis, nfreq, 2), np.nan)
+    l1 = np.full((uv.nvis, nfreq), np.nan)
+    vis = np.ascontiguousarray(uv.vis, dtype=np.float32)
+    rc = lib_a().oracle_model_fp64(C.byref(jb.job), _p(vis, C.c_float), _p(model, C.c_double),
+                                   _p(l1, C.c_double), nthreads or nthreads_default())
+    if rc:
+        raise ValueError(f"oracle_model_fp64 returned {rc}")
+    # table index ifq = ichan*kincf + iIF*kincif with kincf=1, kincif=nchan
+    m = (model[..., 0] + 1j * model[..., 1]).reshape(uv.nvis, uv.nif, uv.nchan)
+    return m, l1.reshape(uv.nvis, uv.nif, uv.nchan)
+
+
+def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None):
+    """FP64 oracle applied to a copy of uv.vis; returns the new float32 records."""
+    jb = Job(uv, sky, params, exact)
+    out = np.ascontiguousarray(uv.vis, dtype=np.float32).copy()
+    rc = lib_a().oracle_apply_fp64(C.byref(jb.job), _p(out, C.c_float), nthreads or nthreads_default())
+    if rc:
+        raise ValueError(f"oracle_apply_fp64 returned {rc}")
+    return out
+
+
+def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):
+    """Reference-faithful CPU restatement (FP32 phase, reference sin/cos)
+    applied to a copy of uv.vis; returns the new float32 records."""
+    jb = Job(uv, sky, params, exact=True)
+    out = np.ascontiguousarray(uv.vis, dtype=np.float32).copy()
+    rc = lib_b().refcpu_apply(C.byref(jb.job), _p(out, C.c_float), nthreads or nthreads_default())
+    if rc:
+        raise ValueError(f"refcpu_apply returned {rc}")
+    return out

@@ -1,0 +1,84 @@
+/*
+ * Test infrastructure: CPU oracles for the Obit DFT sky-model predict/subtract.
+ *
+ * Nothing in the product links this header.  It describes one buffer of
+ * Obit random-group visibility records plus a CLEAN-component table, the
+ * same inputs ThreadSkyModelFTDFT reads from ObitSkyModel / ObitUVDesc
+ * (ObitSystem/Obit/src/ObitSkyModel.c:2354-2857) and ThreadSkyModelMFFTDFT
+ * reads from ObitSkyModelMF (ObitSystem/Obit/src/ObitSkyModelMF.c:1971-2440).
+ *
+ * Two implementations consume it:
+ *   oracle_dft.c  (A) every FP32 input promoted to double; phase, sin/cos,
+ *                     exp and the component sum in FP64.  Judge of max/RMS error.
+ *   refcpu_dft.c  (B) the reference CPU loop restated with its FP32 phase
+ *                     rounding, linked against the reference's own
+ *                     ObitSinCosVec / ObitExpVec (built from the reference
+ *                     sources into oracle/_ref/).  Timed CPU baseline.
+ */
+#ifndef OBIT_ORACLE_DFT_H
+#define OBIT_ORACLE_DFT_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Component model types: numbering of GPUModType,
+ * ObitSystem/Obit/include/ObitCUDASkyModelInfoDef.h:44-52. */
+enum {
+  ORACLE_POINT = 0,
+  ORACLE_POINT_SPEC = 1,
+  ORACLE_POINT_TSPEC = 2,
+  ORACLE_GAUSS = 3,
+  ORACLE_GAUSS_SPEC = 4,
+  ORACLE_GAUSS_TSPEC = 5
+};
+
+typedef struct OracleJob {
+  /* visibility record geometry (ObitUVDesc: lrec, nrparm, ilocu/v/w) */
+  int nvis, lrec, nrparm, ilocu, ilocv, ilocw;
+  /* increments between Stokes, channels and IFs, in floats (desc->incs...) */
+  int incs, incf, incif;
+  int nchan, nif;
+  /* increments into the per-(channel, IF) frequency tables */
+  int kincf, kincif;
+  /* selection; starts are 0-relative (startChannelPB-1 etc.) */
+  int startChannel, numberChannel, startIF, numberIF, startPoln, numberPoln;
+  /* component table: ncomp rows of lcomp floats, reference layout */
+  int modType, nterm, lcomp, ncomp;
+  const float *comps;
+  /* operation */
+  int doDivide, doReplace;
+  /* per-polarization handling: model for the j-th selected polarization is
+   * (flip bit j ? i : 1) * polFact[j] * stokFactor^(number of earlier
+   * polarizations actually written), the CPU reference's rule
+   * (ObitSkyModel.c:2787-2849); polFact carries GPUModelInfo.stokFact. */
+  int flipMask;
+  float stokFactor;
+  float polFact[4];
+  /* frequency tables indexed ichan*kincf + iIF*kincif */
+  const double *fscale;   /* nu / nu_uv_reference, used by the FP64 oracle */
+  const float *fscale32;  /* the FP32 desc->fscale, used by restatement B */
+  const double *lnspec;   /* Spec: ln(nu/nu_model_ref); TSpec: ln(nu/nu_plane) */
+  const int *specIndex;   /* TSpec: coarse plane per (channel, IF) */
+} OracleJob;
+
+/* (A) FP64 model: for every row and selected (channel, IF) writes the raw
+ * complex component sum S = sum_c amp_c exp(i phase_c) (no flip, no
+ * polarization factor) to model[(row*nfreq + ifq)*2 + {0,1}] and the L1 norm
+ * sum_c |amp_c| to l1[row*nfreq + ifq], where nfreq = nchan*nif and
+ * ifq = ichan*kincf + iIF*kincif.  Unselected entries are left untouched.
+ * Returns 0, or -1 for an unsupported model type. */
+int oracle_model_fp64(const OracleJob *job, const float *vis, double *model,
+                      double *l1, int nthreads);
+
+/* (A) FP64 model applied to vis in place (subtract / divide / replace) with
+ * the CPU reference's weight and polarization rules; arithmetic in double,
+ * results rounded to float. Returns 0, or -1 for an unsupported model type. */
+int oracle_apply_fp64(const OracleJob *job, float *vis, int nthreads);
+
+/* (B) reference-faithful restatement; in oracle/_ref/libobit_refcpu.so only. */
+int refcpu_apply(const OracleJob *job, float *vis, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
