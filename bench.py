@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--ct", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM FP32 peak measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -381,7 +382,7 @@ def main():
 
     line = None
     if rank == 0:
-        peak = fp32_peak_tflops(torch, device)
+        peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
         avg_launch_s = statistics.mean(launch_ms) * 1e-3
         achieved = evals * FLOPS_PER_EVAL / avg_launch_s / 1e12
         cpu = None

@@ -322,8 +322,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
         const float* cp = sComp + c * p.cstride;
         const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
         // turns = (X u + Y v + Z w) / (2 pi)
-        const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w),
-                            ds{0.15915494f, 4.3430166e-09f});
+        const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
         sP[idx] = make_float2(P.hi, P.lo);
         for (int d = 0; d < p.ndf; d++) {
           ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});

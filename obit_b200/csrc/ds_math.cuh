@@ -12,6 +12,10 @@
 
 namespace obit {
 
+// 1/(2 pi) as a split-FP32 pair: hi = float(1/(2 pi)), lo = float(1/(2 pi) - hi).
+constexpr float kInv2PiHi = 0.15915493667125702f;
+constexpr float kInv2PiLo = 6.4206382432985265e-09f;
+
 struct ds {
   float hi, lo;
 };
