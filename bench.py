@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--flavor", default="recur", choices=["recur", "plain"])
     ap.add_argument("--K", type=int, default=0)
     ap.add_argument("--ct", type=int, default=0)
+    ap.add_argument("--Bt", type=int, default=0, help="channel blocks per CTA tile (0: planner)")
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (128 or 256)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM FP32 peak measurement")
@@ -311,7 +313,7 @@ def main():
     gm = GPUSkyModel(f"bench{rank}")
     gm.DFTInit(sky, uvh, params)
     flavor = _lib.OBIT_DFT_PLAIN if args.flavor == "plain" else _lib.OBIT_DFT_RECUR
-    gm.set_kernel(flavor, args.K, args.ct)
+    gm.set_kernel(flavor, args.K, args.ct, args.Bt, args.threads)
     gm.DFTSetMod(sky)
     lib = _lib.load()
 
@@ -389,7 +391,9 @@ def main():
         if not args.no_cpu:
             v, cores, sample, kind = cpu_baseline(uvw, fa, freq, sky, args.cpu_seconds)
             cpu = {"value": v / 1e9, "unit": "Gevals/s", "cores": cores, "kind": kind, "sample": sample}
-        kern = f"{args.flavor} K={gm_kernel_K(args)} ct={args.ct or 64}"
+        pi = gm.plan_info()
+        kern = (f"{args.flavor} K={pi['K']} ct={pi['ct']} Bt={pi['Bt']} R={pi['R']} "
+                f"threads={pi['threads']}")
         line = {
             "metric": "component-visibility evals/s (DFT subtract, max rel err <= 1e-5 vs FP64)",
             "value": value / 1e9, "unit": "Gevals/s", "n_gpus": world, "steps": args.steps,
@@ -412,12 +416,6 @@ def main():
     gm.close()
     if world > 1:
         dist.destroy_process_group()
-
-
-def gm_kernel_K(args):
-    if args.K:
-        return args.K
-    return 16 if args.flavor == "recur" else 16
 
 
 if __name__ == "__main__":

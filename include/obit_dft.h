@@ -176,14 +176,26 @@ int obit_dft_set_freq(GPUInfo *gpuInfo, const double *freqArr, int nfreq, double
  * i for every polarization when doFlip.  cpuRules = 0 restores stokFact. */
 int obit_dft_set_poln(GPUInfo *gpuInfo, int cpuRules, float stokFactor, int doFlip);
 
-/* Kernel flavor, channels per thread (1, 4, 8, 16, 32) and components per
- * shared-memory tile; 0 keeps the current / tuned value. */
+/* Kernel flavor, channels per thread (recurrence: 2, 4, 8, 16, 32; plain:
+ * 1, 2, 4, 8, 16) and components per shared-memory tile; 0 keeps the current
+ * value. */
 int obit_dft_set_kernel(GPUInfo *gpuInfo, int flavor, int chanPerThread, int compsPerTile);
+
+/* CTA tile shape: channel blocks per tile (1, 2, 4, ..., 32; 0 = planner's
+ * choice) and threads per CTA (128 or 256; 0 = 256).  Rows per tile are
+ * threads / blocks (at least 8). */
+int obit_dft_set_tile(GPUInfo *gpuInfo, int blocksPerTile, int threadsPerCTA);
 
 /* Device-resident form of Calc: applies the model to nvis records already in
  * device memory at d_vis (lenvis floats each), asynchronously on `stream`
  * (a cudaStream_t; NULL = default stream).  No host copies. */
 int obit_dft_calc_device(GPUInfo *gpuInfo, float *d_vis, int nvis, void *stream);
+
+/* The plan the next call will use (building it if needed): info[0..7] =
+ * flavor, channels per thread, components per tile, blocks per tile, rows per
+ * tile, threads per CTA, channel blocks per row, channel-increment classes.
+ * Writes min(n, 8) entries. */
+int obit_dft_plan_info(GPUInfo *gpuInfo, int *info, int n);
 
 /* Reads and clears the kernels' device error flag (synchronizes the device):
  * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */

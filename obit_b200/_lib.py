@@ -93,7 +93,9 @@ SIGNATURES = {
                                     C.c_double, C.POINTER(C.c_double), C.c_int]),
     "obit_dft_set_poln": (C.c_int, [_GPUINFO_P, C.c_int, C.c_float, C.c_int]),
     "obit_dft_set_kernel": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int, C.c_int]),
+    "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),
+    "obit_dft_plan_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_last_error": (C.c_char_p, []),
     "obit_dft_version": (C.c_int, []),
@@ -134,8 +136,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    path = _build.LIB
-    if not path.exists():
+    path = Path(os.environ["OBIT_DFT_LIB"]) if os.environ.get("OBIT_DFT_LIB") else _build.LIB
+    if not path.exists() and path == _build.LIB:
         if build_if_missing and os.environ.get("OBIT_DFT_NO_BUILD") != "1":
             _build.build()
         if not path.exists():

@@ -4,20 +4,23 @@
 // parameters then {re, im, weight} per correlation) is one "row".  The selected
 // (channel, IF) pairs of a row are cut on the host into channel blocks of at
 // most K channels that share one IF, one channel increment and (for tabulated
-// spectra) one coarse plane.  A CTA tile is R rows x Bt blocks; each thread owns
-// one (row, block) pair and keeps its K complex model sums in registers.
+// spectra) one coarse plane.  A CTA tile is R rows x Bt blocks (R * Bt = 256);
+// thread t owns row t % R of block t / R and keeps its K complex model sums in
+// registers, so a warp covers 32 rows of one block (R >= 32) or 32/R blocks.
 //
-// Per component and tile the work splits in three levels:
-//   (row, component)          prepass: phase argument P = (X u + Y v + Z w)/2pi in
-//                             split-FP32, one accurate step phasor exp(2 pi i P df)
-//                             per channel-increment class, and the Gaussian form
-//                             g1 u^2 + g2 v^2 + g3 u v; stored in shared memory and
-//                             shared by every block of the row.
-//   (row, component, block)   anchor phasor exp(2 pi i P f0) from the range-reduced
-//                             split-FP32 product, amplitude exponent fitted as
-//                             e0 + e1 k + e2 k^2 over the block.
-//   (row, component, channel) complex recurrence z <- z * w (w <- w * q for
-//                             channel-dependent amplitudes) and z accumulated.
+// Per component tile (ct components staged by a bulk copy) the work splits in
+// levels that are each computed once and shared:
+//   (row, component)            phase argument P = (X u + Y v + Z w) / 2pi in
+//                               split-FP32; per channel-increment class the unit
+//                               step s = exp(2 pi i P df) (accurate sin/cos) and
+//                               s^(K/2); the Gaussian form g1 u^2 + g2 v^2 + g3 u v.
+//   (component, block, channel) spectral amplitude A exp(E(k)) with E fitted as a
+//                               quadratic in k over the block (row-independent).
+//   (row, component, block)     anchor exp(2 pi i P f0) from the range-reduced
+//                               split-FP32 product (MUFU sin/cos).
+//   (row, component, channel)   two packed recurrences z <- z * s over the block's
+//                               halves k and k + K/2 (one f32x2 complex multiply
+//                               advances both) and the packed accumulate.
 // Component partial sums are plain FP32 within a tile and folded into a
 // compensated (Kahan) total at each tile boundary.
 #pragma once
@@ -25,6 +28,7 @@
 #include <stdint.h>
 
 #include "ds_math.cuh"
+#include "f32x2.cuh"
 
 namespace obit {
 
@@ -32,6 +36,7 @@ constexpr int kThreads = 256;
 constexpr int kMaxNTerm = 4;   // spectral terms supported (ObitSkyModel nSpecTerm)
 constexpr int kMaxDf = 8;      // distinct channel increments per launch
 constexpr int kMaxPol = 4;
+constexpr int kMaxBt = 32;     // blocks per tile (R >= 8)
 
 // Model families; numbering matches GPUModType (ObitCUDASkyModelInfoDef.h:44-52).
 enum ModelKind : int {
@@ -71,7 +76,7 @@ struct KParams {
   float polFact[kMaxPol];
   const BlockDesc* blocks;
   int nblocks;      // blocks per row
-  int Bt, R;        // tile shape: blocks per tile, rows per tile (Bt * R <= kThreads)
+  int Bt, R;        // tile shape: blocks per tile, rows per tile (Bt * R == kThreads)
   int nBlockTiles;  // ceil(nblocks / Bt)
   int ndf;
   float df_hi[kMaxDf], df_lo[kMaxDf];
@@ -89,24 +94,26 @@ struct Fields {
   static constexpr bool kGaussian = (MODE == kGauss || MODE == kGaussSpec || MODE == kGaussTSpec);
   static constexpr bool kSpec = (MODE == kPointSpec || MODE == kGaussSpec);
   static constexpr bool kTSpec = (MODE == kPointTSpec || MODE == kGaussTSpec);
+  static constexpr bool kTable = kSpec || kTSpec;  // row-independent amplitude table
   static constexpr bool kQuad = (MODE != kPoint);
   static constexpr int kSpecOff = (MODE == kPointSpec) ? 4 : 7;   // first spectral coefficient
   static constexpr int kAlphaOff = (MODE == kPointTSpec) ? 4 : 7; // TSpec spectral index
   static constexpr int kTabOff = (MODE == kPointTSpec) ? 5 : 8;   // TSpec first plane flux
 };
 
+// exp(x) as one MUFU.EX2 of x log2(e); flushes results below ~1e-38 to zero.
 __device__ __forceinline__ float exp_fast(float x) {
-  // exp(x) = 2^(x log2 e); one MUFU.EX2 after the scaling multiply
-  return exp2f(x * 1.4426950408889634f);
+  float y, t = x * 1.4426950408889634f;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(t));
+  return y;
 }
 
-// Complex multiply-accumulate helpers.
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(__fmaf_rn(a.x, b.x, -a.y * b.y), __fmaf_rn(a.x, b.y, a.y * b.x));
 }
 
-// Accurate unit phasor exp(2 pi i r) for |r| <= ~0.5 turns with residual rlo
-// (first-order correction of the float rounding of r).
+// Accurate unit phasor exp(2 pi i r) for |r| <= ~0.5 turns; r.lo corrects the
+// float rounding of r to first order.
 __device__ __forceinline__ float2 phasor_accurate(ds r) {
   float s, c;
   sincospif(2.0f * r.hi, &s, &c);
@@ -114,7 +121,7 @@ __device__ __forceinline__ float2 phasor_accurate(ds r) {
   return make_float2(__fmaf_rn(-d, s, c), __fmaf_rn(d, c, s));
 }
 
-// Anchor phasor: MUFU sin/cos of the reduced angle (error does not compound).
+// Anchor phasor: MUFU sin/cos of the reduced angle (its error does not compound).
 __device__ __forceinline__ float2 phasor_fast(float r) {
   float s, c;
   __sincosf(6.283185307179586f * r, &s, &c);
@@ -122,17 +129,22 @@ __device__ __forceinline__ float2 phasor_fast(float r) {
 }
 
 //--------------------------------------------------------------------------
-// Shared memory layout per CTA (dynamic), sized by the host:
+// Shared memory per CTA (dynamic), sized by the host:
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
-//   uvw    : R * 3 floats
-//   P      : ct * R float2       (phase turns, split-FP32)
-//   S      : ndf * ct * R float2 (step phasors)
-//   Q      : ct * R floats       (Gaussian form, Gaussian models only)
+//   uvw    : R * 3 floats (padded to a multiple of 4)
+//   blk    : Bt BlockDesc (this tile's channel blocks)
+//   P      : ct * R float2            (phase turns, split-FP32)
+//   S      : ndf * ct * R float4      (step s and s^(K/2))
+//   Q      : ct * R floats            (Gaussian form, Gaussian models)
+//   G      : ct * Bt * (K + 2) floats (spectral amplitudes, spectral models)
 // The model stage of the epilogue (R * Bt * K float2) reuses the same space.
 //--------------------------------------------------------------------------
-__host__ __device__ inline size_t smem_floats_main(int R, int ct, int cstride, int ndf, bool gauss) {
-  size_t n = (size_t)ct * cstride + (size_t)R * 3 + 2 * (size_t)ct * R + 2 * (size_t)ndf * ct * R;
+__host__ __device__ inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf,
+                                                   bool gauss, bool table) {
+  size_t n = (size_t)ct * cstride + (size_t)((R * 3 + 3) & ~3) +
+             (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
   if (gauss) n += (size_t)ct * R;
+  if (table) n += (size_t)ct * Bt * (K + 2);  // rows of K/2 + 1 float pairs
   return n;
 }
 __host__ __device__ inline size_t smem_floats_stage(int R, int Bt, int K) {
@@ -140,7 +152,8 @@ __host__ __device__ inline size_t smem_floats_stage(int R, int Bt, int K) {
 }
 
 // Apply the staged model of one tile to its records (subtract / divide /
-// replace), with the CPU reference's polarization rules.
+// replace), with the CPU reference's polarization rules.  stage is indexed
+// ((row * Bt) + block) * K + channel.
 template <int K>
 __device__ __forceinline__ void apply_tile(const KParams& p, const float2* stage, int row0,
                                            int blk0, int nblkTile) {
@@ -238,11 +251,147 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
   return !failed;
 }
 
+__device__ __forceinline__ void init_bar(uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_s) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void inval_bar(uint64_t* bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_s) : "memory");
+  }
+}
+
+// (u, v, w) of the tile's rows at the reference frequency (zero past nvis).
+__device__ __forceinline__ void load_uvw(const KParams& p, float* sUVW, int row0) {
+  for (int i = threadIdx.x; i < p.R; i += blockDim.x) {
+    const int row = row0 + i;
+    float u = 0.f, v = 0.f, w = 0.f;
+    if (row < p.nvis) {
+      const float* rec = p.vis + (size_t)(p.rowBase + row) * p.lrec;
+      u = rec[p.ilocu];
+      v = rec[p.ilocv];
+      w = rec[p.ilocw];
+    }
+    sUVW[3 * i] = u;
+    sUVW[3 * i + 1] = v;
+    sUVW[3 * i + 2] = w;
+  }
+}
+
+// One channel step of a packed chain (two channels k and k + H): accumulate the
+// model term, then advance the phasor by the unit step s (and the Gaussian
+// taper by its ratio).  g points at the pair's spectral amplitudes.
+template <int MODE>
+__device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, const f2x* g, f2x& gg,
+                                           f2x& hh, const f2x qq, const f2x sr, const f2x si,
+                                           const f2x nsi) {
+  using F = Fields<MODE>;
+  if constexpr (MODE == kPoint) {
+    ar = add2(ar, zr);
+    ai = add2(ai, zi);
+  } else if constexpr (MODE == kGauss) {
+    ar = fma2(gg, zr, ar);
+    ai = fma2(gg, zi, ai);
+    gg = mul2(gg, hh);
+    hh = mul2(hh, qq);
+  } else if constexpr (F::kGaussian) {  // Gaussian with spectrum
+    const f2x t = mul2(gg, *g);
+    ar = fma2(t, zr, ar);
+    ai = fma2(t, zi, ai);
+    gg = mul2(gg, hh);
+    hh = mul2(hh, qq);
+  } else {  // spectral table
+    const f2x gv = *g;
+    ar = fma2(gv, zr, ar);
+    ai = fma2(gv, zi, ai);
+  }
+  const f2x t1 = mul2(zi, nsi);
+  const f2x t2 = mul2(zi, sr);
+  const f2x nr = fma2(zr, sr, t1);
+  zi = fma2(zr, si, t2);
+  zr = nr;
+}
+
+// Recurrence state of one component over one block: two packed chains, a over
+// channels (j, j + H) and b over (j + Q, j + Q + H), Q = H/2, with the shared
+// unit step, and the Gaussian taper ratios when present.
+template <int H>
+struct CompChains {
+  f2x ZRa, ZIa, ZRb, ZIb;
+  f2x SR, SI, NSI;
+  f2x GGa, HHa, GGb, HHb, QQ;
+};
+
+// Per (row, component, block) prologue: anchor phasor at the block's first
+// channel from the split-FP32 phase, the chain starts z0, z_Q, z_H, z_(Q+H)
+// (complex products with s^Q), and the Gaussian taper exp(Q (f0 + k df)^2) at
+// the chain starts with its ratios.
+template <int MODE, int H>
+__device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, float4 st,
+                                           const float* sQ, int qidx, const float* sComp,
+                                           int cstride, ds f0, float f0hi, float df) {
+  using F = Fields<MODE>;
+  constexpr int Q = H / 2;
+  float2 z0 = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
+  if constexpr (MODE == kPoint) {
+    const float A = sComp[c * cstride];
+    z0.x *= A;
+    z0.y *= A;
+  }
+  if constexpr (Q > 0) {
+    const float2 sq = make_float2(st.z, st.w);
+    const float2 zq = cmul(z0, sq);
+    const float2 zh = cmul(zq, sq);
+    const float2 z3 = cmul(zh, sq);
+    x.ZRa = pk2(z0.x, zh.x);
+    x.ZIa = pk2(z0.y, zh.y);
+    x.ZRb = pk2(zq.x, z3.x);
+    x.ZIb = pk2(zq.y, z3.y);
+  } else {
+    const float2 zh = cmul(z0, make_float2(st.x, st.y));
+    x.ZRa = pk2(z0.x, zh.x);
+    x.ZIa = pk2(z0.y, zh.y);
+    x.ZRb = x.ZIb = 0ull;
+  }
+  x.SR = pk2(st.x, st.x);
+  x.SI = pk2(st.y, st.y);
+  x.NSI = pk2(-st.y, -st.y);
+  x.GGa = x.HHa = x.GGb = x.HHb = x.QQ = 0ull;
+  if constexpr (F::kGaussian) {
+    const float Qf = sQ[qidx];
+    const float e0 = Qf * f0hi * f0hi;
+    const float e1 = 2.0f * Qf * f0hi * df;
+    const float e2 = Qf * df * df;
+    float A = 1.0f;
+    if constexpr (MODE == kGauss) A = sComp[c * cstride];
+    auto E = [&](float k) { return A * exp_fast(__fmaf_rn(k, __fmaf_rn(k, e2, e1), e0)); };
+    auto D = [&](float k) { return exp_fast(__fmaf_rn(e2, 2.0f * k + 1.0f, e1)); };
+    const float fh = (float)H, fq = (float)Q;
+    x.GGa = pk2(E(0.f), E(fh));
+    x.HHa = pk2(D(0.f), D(fh));
+    if constexpr (Q > 0) {
+      x.GGb = pk2(E(fq), E(fq + fh));
+      x.HHb = pk2(D(fq), D(fq + fh));
+    }
+    const float q = exp_fast(2.0f * e2);
+    x.QQ = pk2(q, q);
+  }
+}
+
 //--------------------------------------------------------------------------
-// Recurrence kernel.  K channels per thread, MODE model family.
+// Recurrence kernel.  K channels per thread (even), MODE model family.
 //--------------------------------------------------------------------------
 template <int K, int MODE>
 __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(const KParams p) {
+  static_assert(K >= 2 && (K & 1) == 0, "K must be even");
+  constexpr int H = K / 2;
   using F = Fields<MODE>;
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) uint64_t bar;
@@ -250,22 +399,24 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
   float* sUVW = sComp + ct * p.cstride;
-  float2* sP = reinterpret_cast<float2*>(sUVW + ((R * 3 + 1) & ~1));
-  float2* sS = sP + ct * R;
+  BlockDesc* sBlk = reinterpret_cast<BlockDesc*>(sUVW + ((R * 3 + 3) & ~3));
+  float2* sP = reinterpret_cast<float2*>(sBlk + Bt);
+  float4* sS = reinterpret_cast<float4*>(sP + ct * R);
   float* sQ = reinterpret_cast<float*>(sS + p.ndf * ct * R);
+  float* sG = sQ + (F::kGaussian ? ct * R : 0);
   float2* stage = reinterpret_cast<float2*>(smem);
 
-  if (threadIdx.x == 0) {
-    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(&bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_s) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
+  init_bar(&bar);
   uint32_t phase = 0;
 
-  const int tr = threadIdx.x / Bt;
-  const int tb = threadIdx.x - tr * Bt;
-  const bool active = (tr < R);
+  // R and Bt are powers of two (R * Bt == kThreads)
+  const int lgR = __ffs(R) - 1;
+  const int lgBt = __ffs(Bt) - 1;
+  constexpr int lgH = (H >= 16) ? 4 : (H >= 8) ? 3 : (H >= 4) ? 2 : (H >= 2) ? 1 : 0;
+  static_assert((1 << lgH) == H, "K/2 must be a power of two");
+  constexpr int Q = H / 2;  // offset of the second packed chain
+  const int tr = threadIdx.x & (R - 1);  // row within the tile
+  const int tb = threadIdx.x >> lgR;     // block within the tile
 
   const int nRowTiles = (p.nvis + R - 1) / R;
   const int nItems = nRowTiles * p.nBlockTiles;
@@ -277,171 +428,160 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
     const int nblkTile = min(Bt, p.nblocks - blk0);
     __syncthreads();  // the previous item's epilogue is done with the stage
 
-    // rows' (u, v, w) at the reference frequency
-    for (int i = threadIdx.x; i < R; i += blockDim.x) {
-      const int row = row0 + i;
-      float u = 0.f, v = 0.f, w = 0.f;
-      if (row < p.nvis) {
-        const float* rec = p.vis + (size_t)(p.rowBase + row) * p.lrec;
-        u = rec[p.ilocu];
-        v = rec[p.ilocv];
-        w = rec[p.ilocw];
-      }
-      sUVW[3 * i] = u;
-      sUVW[3 * i + 1] = v;
-      sUVW[3 * i + 2] = w;
-    }
-
-    // this thread's channel block
-    BlockDesc bd;
-    const bool mine = active && (tb < nblkTile);
-    if (mine) {
-      bd = p.blocks[blk0 + tb];
-    } else {
-      bd = p.blocks[0];
-    }
+    load_uvw(p, sUVW, row0);
+    for (int i = threadIdx.x; i < Bt; i += blockDim.x) sBlk[i] = p.blocks[blk0 + min(i, nblkTile - 1)];
+    __syncthreads();
+    const BlockDesc& bd = sBlk[tb];
+    const bool mine = (tb < nblkTile);
     const ds f0 = {bd.f0_hi, bd.f0_lo};
-    const float df = bd.df;
 
-    float2 tot[K], cmp[K];
+    f2x TR[H], TI[H], CR[H], CI[H];  // compensated totals: halves k and k + H
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-      tot[k] = make_float2(0.f, 0.f);
-      cmp[k] = make_float2(0.f, 0.f);
-    }
+    for (int j = 0; j < H; j++) TR[j] = TI[j] = CR[j] = CI[j] = 0ull;
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // previous tile's readers are done with shared memory
       if (!stage_comps(p, sComp, c0, &bar, phase)) return;
       __syncthreads();
 
-      // prepass over (component, row) pairs of this tile
+      // (row, component): phase turns, steps, Gaussian form
       for (int idx = threadIdx.x; idx < ct * R; idx += blockDim.x) {
-        const int c = idx / R;
-        const int r = idx - c * R;
+        const int c = idx >> lgR;
+        const int r = idx & (R - 1);
         const float* cp = sComp + c * p.cstride;
         const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-        // turns = (X u + Y v + Z w) / (2 pi)
         const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
         sP[idx] = make_float2(P.hi, P.lo);
         for (int d = 0; d < p.ndf; d++) {
-          ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
-          ds fr = ds_frac_turns(t);
-          fr.hi -= rintf(fr.hi);
-          sS[d * ct * R + idx] = phasor_accurate(fr);
+          // reduced step angle: exact integer removal from the high part, the
+          // low part kept for the first-order correction
+          const ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
+          const float2 s = phasor_accurate(ds{__fsub_rn(t.hi, rintf(t.hi)), t.lo});
+          // s^Q, Q = K/4: offset between the two packed chains of a block
+          float2 sq = s;
+#pragma unroll
+          for (int m = 1; m < Q; m <<= 1) sq = cmul(sq, sq);
+          sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
         }
-        if (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
+        if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
+      }
+      // (component, block): spectral amplitudes A exp(e0 + e1 k + e2 k^2) for the
+      // block's K channels, stored as pairs (k, k + H) so one 64-bit load feeds
+      // both halves.  Two packed amplitude recurrences g <- g r, r <- r q start
+      // from exact exponentials at k = 0 and k = H (H steps each).
+      if constexpr (F::kTable) {
+        for (int idx = threadIdx.x; idx < ct * Bt; idx += blockDim.x) {
+          const int c = idx >> lgBt;
+          const int b = idx & (Bt - 1);
+          const float* cp = sComp + c * p.cstride;
+          const BlockDesc& bb = sBlk[b];
+          float A, e0, e1, e2;
+          if constexpr (F::kTSpec) {
+            A = cp[F::kTabOff + bb.plane];
+            const float al = cp[F::kAlphaOff];
+            e0 = al * bb.l[0][0];
+            e1 = al * bb.l[0][1];
+            e2 = al * bb.l[0][2];
+          } else {
+            A = cp[0];
+            e0 = e1 = e2 = 0.f;
+#pragma unroll
+            for (int t = 0; t < kMaxNTerm; t++) {
+              if (t < p.nterm) {
+                const float a = cp[F::kSpecOff + t];
+                e0 = __fmaf_rn(a, bb.l[t][0], e0);
+                e1 = __fmaf_rn(a, bb.l[t][1], e1);
+                e2 = __fmaf_rn(a, bb.l[t][2], e2);
+              }
+            }
+          }
+          const float fh = (float)H;
+          f2x GP = pk2(A * exp_fast(e0), A * exp_fast(e0 + fh * (e1 + fh * e2)));
+          f2x RP = pk2(exp_fast(e1 + e2), exp_fast(e1 + e2 * (2.0f * fh + 1.0f)));
+          const float q = exp_fast(2.0f * e2);
+          const f2x QQ = pk2(q, q);
+          // layout [component][block][pair j] with an odd row stride of H + 1
+          // pairs: consecutive threads store to distinct bank pairs
+          f2x* out = reinterpret_cast<f2x*>(sG) + (c * Bt + b) * (H + 1);
+#pragma unroll
+          for (int j = 0; j < H; j++) {
+            out[j] = GP;
+            GP = mul2(GP, RP);
+            RP = mul2(RP, QQ);
+          }
+        }
       }
       __syncthreads();
 
-      float2 acc[K];
+      f2x AR[H], AI[H];  // this tile's partial sums
 #pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = make_float2(0.f, 0.f);
+      for (int j = 0; j < H; j++) AR[j] = AI[j] = 0ull;
 
       if (mine) {
         const int nc = min(ct, p.ncomp - c0);
-        for (int c = 0; c < nc; c++) {
-          const int idx = c * R + tr;
-          const float2 Pp = sP[idx];
-          const float2 st = sS[bd.dfc * ct * R + idx];
-          const float* cp = sComp + c * p.cstride;
-          // anchor phasor at the block's first channel
-          const ds t = ds_mul(ds{Pp.x, Pp.y}, f0);
-          const ds fr = ds_frac_turns(t);
-          float2 z = phasor_fast(fr.hi);
-          if constexpr (!F::kQuad) {
-            const float A = cp[0];
-            z.x *= A;
-            z.y *= A;
-            float2 wv = st;
+        const float df = bd.df;
+        const float4* sSd = sS + bd.dfc * ct * R;
+        // components in pairs: two prologues and four rotation chains in flight
+        // (the tile is zero-filled past ncomp, so a padded partner adds zero)
+        const int ncp = min(ct, (nc + 1) & ~1);
+        for (int c = 0; c < ncp; c += 2) {
+          CompChains<H> x, y;
+          comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
+                              f0, bd.f0_hi, df);
+          comp_setup<MODE, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
+                              (c + 1) * R + tr, sComp, p.cstride, f0, bd.f0_hi, df);
+          const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
+          const f2x* Gy = Gx + Bt * (H + 1);
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-              acc[k].x += z.x;
-              acc[k].y += z.y;
-              z = cmul(z, wv);
-            }
-          } else {
-            // amplitude exponent e0 + e1 k + e2 k^2 over the block
-            float e0 = 0.f, e1 = 0.f, e2 = 0.f;
-            float A;
-            if constexpr (F::kTSpec) {
-              A = cp[F::kTabOff + bd.plane];
-              const float al = cp[F::kAlphaOff];
-              e0 = al * bd.l[0][0];
-              e1 = al * bd.l[0][1];
-              e2 = al * bd.l[0][2];
-            } else {
-              A = cp[0];
-            }
-            if constexpr (F::kSpec) {
-#pragma unroll
-              for (int tt = 0; tt < kMaxNTerm; tt++) {
-                if (tt < p.nterm) {
-                  const float a = cp[F::kSpecOff + tt];
-                  e0 = __fmaf_rn(a, bd.l[tt][0], e0);
-                  e1 = __fmaf_rn(a, bd.l[tt][1], e1);
-                  e2 = __fmaf_rn(a, bd.l[tt][2], e2);
-                }
-              }
-            }
-            if constexpr (F::kGaussian) {
-              // Q (f0 + k df)^2 with f0 ~ 1: expand exactly in k
-              const float Q = sQ[idx];
-              const float f = bd.f0_hi;
-              e0 = __fmaf_rn(Q * f, f, e0);
-              e1 = __fmaf_rn(2.0f * Q * f, df, e1);
-              e2 = __fmaf_rn(Q * df, df, e2);
-            }
-            const float a0 = A * exp_fast(e0);
-            float r0 = exp_fast(e1 + e2);
-            const float q = exp_fast(2.0f * e2);
-            z.x *= a0;
-            z.y *= a0;
-            float2 wv = make_float2(st.x * r0, st.y * r0);
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-              acc[k].x += z.x;
-              acc[k].y += z.y;
-              z = cmul(z, wv);
-              wv.x *= q;
-              wv.y *= q;
+          for (int jj = 0; jj < (Q > 0 ? Q : 1); jj++) {
+            chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, Gx + jj, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
+            chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, Gy + jj, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
+            if constexpr (Q > 0) {
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, Gx + jj + Q, x.GGb, x.HHb, x.QQ,
+                               x.SR, x.SI, x.NSI);
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, Gy + jj + Q, y.GGb, y.HHb, y.QQ,
+                               y.SR, y.SI, y.NSI);
             }
           }
         }
       }
       // compensated fold of this tile's partial sums
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        float y = acc[k].x - cmp[k].x;
-        float s = tot[k].x + y;
-        cmp[k].x = (s - tot[k].x) - y;
-        tot[k].x = s;
-        y = acc[k].y - cmp[k].y;
-        s = tot[k].y + y;
-        cmp[k].y = (s - tot[k].y) - y;
-        tot[k].y = s;
+      for (int j = 0; j < H; j++) {
+        f2x y = sub2(AR[j], CR[j]);
+        f2x s = add2(TR[j], y);
+        CR[j] = sub2(sub2(s, TR[j]), y);
+        TR[j] = s;
+        y = sub2(AI[j], CI[j]);
+        s = add2(TI[j], y);
+        CI[j] = sub2(sub2(s, TI[j]), y);
+        TI[j] = s;
       }
     }
 
     // stage the tile's model and apply it to the records
     __syncthreads();
-    if (active) {
+    {
+      float2* out = stage + (tr * Bt + tb) * K;
 #pragma unroll
-      for (int k = 0; k < K; k++) stage[(tr * Bt + tb) * K + k] = tot[k];
+      for (int j = 0; j < H; j++) {
+        float ra, rb, ia, ib;
+        up2(TR[j], ra, rb);
+        up2(TI[j], ia, ib);
+        out[j] = make_float2(ra, ia);
+        out[j + H] = make_float2(rb, ib);
+      }
     }
     __syncthreads();
     apply_tile<K>(p, stage, row0, blk0, nblkTile);
   }
-  if (threadIdx.x == 0) {
-    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(&bar);
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_s) : "memory");
-  }
+  inval_bar(&bar);
 }
 
 //--------------------------------------------------------------------------
 // Plain comparator: direct FP64 phase and one sin/cos per (row, channel,
-// component), FP32 accumulation.  Same tiling and epilogue; every channel of
-// the block evaluated independently.
+// component), FP32 accumulation.  Same tiling, component staging and epilogue;
+// every channel of the block evaluated independently.
 //--------------------------------------------------------------------------
 template <int K, int MODE>
 __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p) {
@@ -452,16 +592,10 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
   float* sComp = smem;
   float* sUVW = sComp + ct * p.cstride;
   float2* stage = reinterpret_cast<float2*>(smem);
-  if (threadIdx.x == 0) {
-    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(&bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_s) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
+  init_bar(&bar);
   uint32_t phase = 0;
-  const int tr = threadIdx.x / Bt;
-  const int tb = threadIdx.x - tr * Bt;
-  const bool active = (tr < R);
+  const int tr = threadIdx.x % R;
+  const int tb = threadIdx.x / R;
   const int nRowTiles = (p.nvis + R - 1) / R;
   const int nItems = nRowTiles * p.nBlockTiles;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
@@ -471,21 +605,9 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
     const int blk0 = bt * Bt;
     const int nblkTile = min(Bt, p.nblocks - blk0);
     __syncthreads();  // the previous item's epilogue is done with the stage
-    for (int i = threadIdx.x; i < R; i += blockDim.x) {
-      const int row = row0 + i;
-      float u = 0.f, v = 0.f, w = 0.f;
-      if (row < p.nvis) {
-        const float* rec = p.vis + (size_t)(p.rowBase + row) * p.lrec;
-        u = rec[p.ilocu];
-        v = rec[p.ilocv];
-        w = rec[p.ilocw];
-      }
-      sUVW[3 * i] = u;
-      sUVW[3 * i + 1] = v;
-      sUVW[3 * i + 2] = w;
-    }
-    const bool mine = active && (tb < nblkTile);
-    BlockDesc bd = p.blocks[mine ? blk0 + tb : 0];
+    load_uvw(p, sUVW, row0);
+    const bool mine = (tb < nblkTile);
+    const BlockDesc bd = p.blocks[blk0 + min(tb, nblkTile - 1)];
     float2 tot[K], cmp[K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -556,17 +678,12 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
       }
     }
     __syncthreads();
-    if (active) {
 #pragma unroll
-      for (int k = 0; k < K; k++) stage[(tr * Bt + tb) * K + k] = tot[k];
-    }
+    for (int k = 0; k < K; k++) stage[(tr * Bt + tb) * K + k] = tot[k];
     __syncthreads();
     apply_tile<K>(p, stage, row0, blk0, nblkTile);
   }
-  if (threadIdx.x == 0) {
-    const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(&bar);
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_s) : "memory");
-  }
+  inval_bar(&bar);
 }
 
 }  // namespace obit

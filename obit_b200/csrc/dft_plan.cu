@@ -8,7 +8,7 @@
 
 namespace obit {
 
-bool valid_K(int K) { return K == 1 || K == 4 || K == 8 || K == 16 || K == 32; }
+bool valid_K(int K) { return K == 1 || K == 2 || K == 4 || K == 8 || K == 16 || K == 32; }
 
 int comp_stride(const ModelDesc& m) { return (m.lcomp + 3) & ~3; }
 
@@ -45,7 +45,7 @@ KernelFn pick_plain(int mode) {
 KernelFn pick_kernel(int flavor, int K, int mode) {
   if (flavor == kFlavorRecur) {
     switch (K) {
-      case 1: return pick_recur<1>(mode);
+      case 2: return pick_recur<2>(mode);
       case 4: return pick_recur<4>(mode);
       case 8: return pick_recur<8>(mode);
       case 16: return pick_recur<16>(mode);
@@ -54,6 +54,7 @@ KernelFn pick_kernel(int flavor, int K, int mode) {
   } else if (flavor == kFlavorPlain) {
     switch (K) {
       case 1: return pick_plain<1>(mode);
+      case 2: return pick_plain<2>(mode);
       case 4: return pick_plain<4>(mode);
       case 8: return pick_plain<8>(mode);
       case 16: return pick_plain<16>(mode);
@@ -100,7 +101,7 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
     *err = "nterm " + std::to_string(M.nterm) + " outside 0.." + std::to_string(kMaxNTerm);
     return 3;
   }
-  if (!valid_K(T.K) || !pick_kernel(T.flavor, T.K, M.kind)) {
+  if (T.K != 0 && (!valid_K(T.K) || !pick_kernel(T.flavor, T.K, M.kind))) {
     *err = "no kernel for flavor " + std::to_string(T.flavor) + " K " + std::to_string(T.K);
     return 3;
   }
@@ -142,7 +143,32 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
     dfs.push_back(d);
     return (int)dfs.size() - 1;
   };
-  const int K = T.K;
+  int K = T.K;
+  if (K == 0) {
+    // Default channels per thread: 32 (two packed chains of 8 steps) for
+    // constant or tabulated amplitudes, 16 when a per-row Gaussian taper adds
+    // registers; never longer than the selected channel run.
+    const bool g = (M.kind == kGauss || M.kind == kGaussSpec || M.kind == kGaussTSpec);
+    K = (T.flavor == kFlavorRecur) ? (g ? 16 : 32) : 8;
+    const int run = L.chane - L.chanb + 1;
+    while (K > 2 && K / 2 >= run) K /= 2;
+  }
+  // Frequencies that do not advance uniformly within an IF cannot use long
+  // recurrences: such plans use one-channel blocks and the shortest kernel.
+  bool uniform = true;
+  for (int iIF = L.ifb; iIF <= L.ife && uniform; iIF++) {
+    const int i0 = L.chanb * L.kincf + iIF * L.kincif;
+    if (L.chane <= L.chanb + 1) continue;
+    const double f0 = L.fscale[i0], d = L.fscale[i0 + L.kincf] - f0;
+    for (int ch = L.chanb + 2; ch <= L.chane; ch++) {
+      const double f = L.fscale[ch * L.kincf + iIF * L.kincif];
+      if (std::fabs(f - (f0 + (ch - L.chanb) * d)) > 1e-13 * std::fabs(f0)) {
+        uniform = false;
+        break;
+      }
+    }
+  }
+  if (!uniform) K = (T.flavor == kFlavorRecur) ? 2 : 1;
   for (int iIF = L.ifb; iIF <= L.ife; iIF++) {
     int ch = L.chanb;
     while (ch <= L.chane) {
@@ -163,7 +189,7 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
         for (int k = 2; k < len; k++)
           dev = std::max(dev, std::fabs(L.fscale[ifq0 + k * L.kincf] - (f0 + k * df)));
         plan->maxNonLin = std::max(plan->maxNonLin, dev);
-        if (dev > 1e-13 * std::fabs(f0)) {
+        if (!uniform || dev > 1e-13 * std::fabs(f0)) {
           plan->linear = false;
           len = 1;  // fall back to one-channel blocks here
         }
@@ -217,8 +243,27 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
   kp.stokFactor = A.stokFactor;
   for (int i = 0; i < kMaxPol; i++) kp.polFact[i] = A.polFact[i];
   kp.nblocks = nblocks;
-  kp.Bt = std::min(nblocks, kThreads);
-  kp.R = std::max(1, kThreads / kp.Bt);
+  // Tile shape R x Bt = threads (128 or 256), R a power of two >= 8 (warp lanes
+  // are rows): the fewest idle blocks, then the most blocks sharing each row's
+  // phase work.
+  const int threads = (T.threads == 128) ? 128 : kThreads;
+  {
+    int bestBt = 1;
+    long best = -1;
+    for (int bt = 1; bt <= kMaxBt && threads / bt >= 8; bt *= 2) {
+      if (T.Bt > 0 && bt != T.Bt) continue;
+      const long tiles = (nblocks + bt - 1) / bt;
+      const long waste = tiles * bt - nblocks;
+      const long score = waste * 64 - (bt <= 16 ? bt : 16);
+      if (best < 0 || score < best) {
+        best = score;
+        bestBt = bt;
+      }
+    }
+    kp.Bt = bestBt;
+  }
+  kp.R = threads / kp.Bt;
+  plan->threads = threads;
   kp.nBlockTiles = (nblocks + kp.Bt - 1) / kp.Bt;
   kp.ndf = (int)dfs.size();
   for (int i = 0; i < kp.ndf; i++) split_ds(dfs[i], &kp.df_hi[i], &kp.df_lo[i]);
@@ -226,14 +271,16 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
   kp.nterm = M.nterm;
   kp.nspec = M.nspec;
   const bool gauss = (M.kind == kGauss || M.kind == kGaussSpec || M.kind == kGaussTSpec);
+  const bool table = (M.kind == kPointSpec || M.kind == kGaussSpec || M.kind == kPointTSpec ||
+                      M.kind == kGaussTSpec);
   // shrink the component tile until two CTAs fit per SM
-  int ct = T.ct;
-  const size_t budget = 110 * 1024;
+  int ct = (T.ct + 1) & ~1;  // even: the recurrence kernel takes components in pairs
+  const size_t budget = (threads == 128) ? 52 * 1024 : 110 * 1024;
   auto need = [&](int c) {
     size_t mainf = (T.flavor == kFlavorRecur)
-                       ? smem_floats_main(kp.R, c, kp.cstride, kp.ndf, gauss)
+                       ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table)
                        : (size_t)c * kp.cstride + (size_t)kp.R * 3;
-    return 4 * std::max(mainf + 2, smem_floats_stage(kp.R, kp.Bt, T.K));
+    return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
   while (ct > 8 && need(ct) > budget) ct /= 2;
   kp.ct = ct;
@@ -243,7 +290,8 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
     return 3;
   }
 
-  KernelFn fn = pick_kernel(T.flavor, T.K, M.kind);
+  KernelFn fn = pick_kernel(T.flavor, K, M.kind);
+  plan->tune.K = K;
   cudaError_t ce =
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smemBytes);
   if (ce != cudaSuccess) {
@@ -253,7 +301,7 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
   int perSM = 0, dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, kThreads, plan->smemBytes);
+  ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, threads, plan->smemBytes);
   if (ce != cudaSuccess || perSM < 1) {
     *err = std::string("kernel cannot be resident: ") + cudaGetErrorString(ce);
     return 2;
@@ -297,7 +345,7 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);
   KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind);
-  fn<<<grid, kThreads, plan.smemBytes, stream>>>(kp);
+  fn<<<grid, plan.threads, plan.smemBytes, stream>>>(kp);
   cudaError_t ce = cudaGetLastError();
   if (ce != cudaSuccess) {
     *err = std::string("kernel launch: ") + cudaGetErrorString(ce);

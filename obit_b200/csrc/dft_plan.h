@@ -43,8 +43,10 @@ struct ApplyDesc {
 
 struct TuneDesc {
   int flavor = kFlavorRecur;
-  int K = 16;   // channels per thread
+  int K = 0;    // channels per thread; 0 = chosen by the planner
   int ct = 64;  // components per shared-memory tile
+  int Bt = 0;   // blocks per tile (power of two); 0 = chosen by the planner
+  int threads = 256;  // CTA size, 128 or 256
 };
 
 // A compiled plan: block table on the device plus the fixed kernel fields.
@@ -53,6 +55,7 @@ struct Plan {
   std::vector<BlockDesc> blocks;   // host copy
   BlockDesc* d_blocks = nullptr;   // device copy (owned)
   size_t smemBytes = 0;
+  int threads = 256;               // CTA size
   int gridCap = 0;                 // CTAs resident across the device
   TuneDesc tune;
   ModelDesc model;

@@ -60,6 +60,17 @@ __device__ __forceinline__ ds ds_dot3(float x, float u, float y, float v, float 
   return fast_two_sum(t.hi, lo);
 }
 
+// Fractional turns of the product (a.hi + a.lo) * (b.hi + b.lo) as one float in
+// [-0.5, 0.5] (up to rounding): the exact high product and its error term, the
+// cross terms, then the nearest integer removed from the high part.  Absolute
+// error ~2^-24 turns plus 2^-46 of the product; used where only the reduced
+// angle is needed.
+__device__ __forceinline__ float ds_mul_frac(ds a, ds b) {
+  const float hi = __fmul_rn(a.hi, b.hi);
+  const float lo = __fmaf_rn(a.hi, b.lo, __fmaf_rn(a.lo, b.hi, __fmaf_rn(a.hi, b.hi, -hi)));
+  return __fadd_rn(__fsub_rn(hi, rintf(hi)), lo);
+}
+
 // Fractional part of a double-single number of turns, in [-0.5, 0.5] (up to
 // rounding), returned as float plus the float rounding residual.
 __device__ __forceinline__ ds ds_frac_turns(ds t) {

@@ -3,7 +3,7 @@
  * include/obit_gpu_skymodel.h for the interface and the deliberate
  * differences from the reference.
  */
-#include "../../include/obit_gpu_skymodel.h"
+#include "obit_gpu_skymodel.h"
 
 #include <cuda_runtime_api.h>
 #include <stdarg.h>

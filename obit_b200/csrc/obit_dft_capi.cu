@@ -15,7 +15,7 @@
 #include <unordered_map>
 #include <vector>
 
-#include "../../include/obit_dft.h"
+#include "obit_dft.h"
 #include "dft_plan.h"
 
 namespace {
@@ -357,15 +357,34 @@ int obit_dft_set_kernel(GPUInfo* g, int flavor, int chanPerThread, int compsPerT
   if (rc) return rc;
   if (flavor != OBIT_DFT_RECUR && flavor != OBIT_DFT_PLAIN)
     return fail(OBIT_DFT_EBADARG, "unknown kernel flavor");
-  if (chanPerThread && !valid_K(chanPerThread))
-    return fail(OBIT_DFT_EBADARG, "channels per thread must be 1, 4, 8, 16 or 32");
-  if (flavor == OBIT_DFT_PLAIN && chanPerThread == 32)
-    return fail(OBIT_DFT_EBADARG, "plain kernel supports up to 16 channels per thread");
+  // 0 leaves the choice to the planner (also when switching flavor)
+  const int K = chanPerThread ? chanPerThread : (flavor == s->tune.flavor ? s->tune.K : 0);
+  if (flavor == OBIT_DFT_RECUR && !(K == 0 || K == 2 || K == 4 || K == 8 || K == 16 || K == 32))
+    return fail(OBIT_DFT_EBADARG, "recurrence kernel: channels per thread must be 2, 4, 8, 16 or 32");
+  if (flavor == OBIT_DFT_PLAIN && !(K == 0 || K == 1 || K == 2 || K == 4 || K == 8 || K == 16))
+    return fail(OBIT_DFT_EBADARG, "plain kernel: channels per thread must be 1, 2, 4, 8 or 16");
   if (compsPerTile < 0 || compsPerTile > 1024) return fail(OBIT_DFT_EBADARG, "bad components per tile");
   s->tune.flavor = flavor;
-  if (chanPerThread) s->tune.K = chanPerThread;
-  if (flavor == OBIT_DFT_PLAIN && s->tune.K > 16) s->tune.K = 16;
+  s->tune.K = K;
   if (compsPerTile) s->tune.ct = compsPerTile;
+  s->planValid = false;
+  return OBIT_DFT_OK;
+}
+
+int obit_dft_set_tile(GPUInfo* g, int blocksPerTile, int threadsPerCTA) {
+  g_last_error.clear();
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  if (blocksPerTile < 0 || blocksPerTile > kMaxBt || (blocksPerTile & (blocksPerTile - 1)))
+    return fail(OBIT_DFT_EBADARG, "blocks per tile must be 0 or a power of two up to 32");
+  if (threadsPerCTA != 0 && threadsPerCTA != 128 && threadsPerCTA != 256)
+    return fail(OBIT_DFT_EBADARG, "threads per CTA must be 128 or 256");
+  const int th = threadsPerCTA ? threadsPerCTA : 256;
+  if (blocksPerTile && th / blocksPerTile < 8)
+    return fail(OBIT_DFT_EBADARG, "a tile needs at least 8 rows (threads / blocks)");
+  s->tune.Bt = blocksPerTile;
+  s->tune.threads = th;
   s->planValid = false;
   return OBIT_DFT_OK;
 }
@@ -382,6 +401,21 @@ int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
   std::string err;
   rc = launch_plan(s->plan, d_vis, 0, nvis, s->d_comps, s->d_err, (cudaStream_t)stream, &err);
   if (rc) return fail(rc, err);
+  return OBIT_DFT_OK;
+}
+
+int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
+  g_last_error.clear();
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  if (!info || n < 1) return fail(OBIT_DFT_EBADARG, "plan info needs an output array");
+  rc = ensure_plan(g, s);
+  if (rc) return rc;
+  const Plan& pl = s->plan;
+  const int v[8] = {pl.tune.flavor, pl.tune.K, pl.kp.ct, pl.kp.Bt, pl.kp.R, pl.threads,
+                    pl.kp.nblocks, pl.kp.ndf};
+  for (int i = 0; i < n && i < 8; i++) info[i] = v[i];
   return OBIT_DFT_OK;
 }
 

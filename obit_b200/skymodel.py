@@ -157,8 +157,19 @@ class GPUSkyModel:
         return self._lib.obit_gpu_skymodel_info(self._h)
 
     def set_kernel(self, flavor: int = _lib.OBIT_DFT_RECUR, chan_per_thread: int = 0,
-                   comps_per_tile: int = 0) -> None:
-        _lib.check(self._lib.obit_dft_set_kernel(self.gpuinfo, flavor, chan_per_thread, comps_per_tile))
+                   comps_per_tile: int = 0, blocks_per_tile: int = 0, threads: int = 0) -> None:
+        """Kernel flavor and tile shape (0 keeps the current / planner's choice)."""
+        _lib.check(self._lib.obit_dft_set_kernel(self.gpuinfo, flavor, chan_per_thread,
+                                                 comps_per_tile))
+        if blocks_per_tile or threads:
+            _lib.check(self._lib.obit_dft_set_tile(self.gpuinfo, blocks_per_tile, threads))
+
+    def plan_info(self) -> dict:
+        """The kernel plan the next call uses (built on demand)."""
+        arr = (C.c_int * 8)()
+        _lib.check(self._lib.obit_dft_plan_info(self.gpuinfo, arr, 8))
+        keys = ("flavor", "K", "ct", "Bt", "R", "threads", "nblocks", "ndf")
+        return dict(zip(keys, list(arr)))
 
     def calc_device(self, d_vis_ptr: int, nvis: int, stream_ptr: int = 0) -> None:
         """Apply the model to nvis records already in device memory (async)."""

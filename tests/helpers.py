@@ -14,7 +14,8 @@ TOL_REL = 1e-5
 
 
 def run_gpu(uv: U.UVData, sky: U.SkyComps, params: SkyModelParams | None = None,
-            flavor: int = OBIT_DFT_RECUR, K: int = 0, ct: int = 0, exact: bool = True) -> U.UVData:
+            flavor: int = OBIT_DFT_RECUR, K: int = 0, ct: int = 0, exact: bool = True,
+            Bt: int = 0, threads: int = 0) -> U.UVData:
     """Apply the model with the GPU path; returns a new UVData."""
     p = params or SkyModelParams()
     if p.nVisPIO <= 0:
@@ -23,8 +24,8 @@ def run_gpu(uv: U.UVData, sky: U.SkyComps, params: SkyModelParams | None = None,
     gm = GPUSkyModel("test")
     try:
         gm.DFTInit(sky, out, p, exact_freq=exact)
-        if flavor != OBIT_DFT_RECUR or K or ct:
-            gm.set_kernel(flavor, K, ct)
+        if flavor != OBIT_DFT_RECUR or K or ct or Bt or threads:
+            gm.set_kernel(flavor, K, ct, Bt, threads)
         gm.DFTSetMod(sky)
         if uv.nvis > 0:
             gm.DFTCalc(out)

@@ -30,17 +30,24 @@ def test_model_types_plain(mod):
     assert mx < TOL_REL, (mx, rms)
 
 
-@pytest.mark.parametrize("K", [1, 4])
+@pytest.mark.parametrize("K", [2, 4, 32])
 def test_channels_per_thread(K):
     uv, sky = small(U.MOD_POINT_SPEC, nrow=40, nchan=70, nif=1, ncomp=100)
     mx, _ = model_error(uv, sky, K=K)
     assert mx < TOL_REL
 
 
-def test_32_channels_per_thread_point():
-    """32-step recurrences stay within the bound for constant amplitudes."""
-    uv, sky = small(U.MOD_POINT, nrow=40, nchan=70, nif=1, ncomp=100)
-    mx, _ = model_error(uv, sky, K=32)
+@pytest.mark.parametrize("Bt", [1, 4, 32])
+def test_tile_shapes(Bt):
+    uv, sky = small(U.MOD_GAUSS_TSPEC, nrow=70, nchan=64, nif=3, ncomp=90)
+    mx, _ = model_error(uv, sky, Bt=Bt, K=8)
+    assert mx < TOL_REL
+
+
+@pytest.mark.parametrize("mod", [U.MOD_POINT, U.MOD_GAUSS_SPEC])
+def test_plain_one_channel_blocks(mod):
+    uv, sky = small(mod, nrow=20, nchan=9, nif=1, ncomp=40)
+    mx, _ = model_error(uv, sky, flavor=OBIT_DFT_PLAIN, K=1)
     assert mx < TOL_REL
 
 
@@ -151,7 +158,8 @@ def test_fp32_freqscale_interface():
     assert mx < TOL_REL
 
 
-def test_high_phase_precision():
+@pytest.mark.parametrize("K", [0, 16])
+def test_high_phase_precision(K):
     """8000 km baselines at 22 GHz, field 0.3 deg off centre: phases ~1e7 rad."""
     rng = np.random.default_rng(4)
     pos = U.array_layout(10, 8.0e6, rng)
@@ -161,13 +169,21 @@ def test_high_phase_precision():
     uv = U.make_uvdata(uvw, 2, 64, 2, freq, fa, np.random.default_rng(5))
     c = 0.3 * U.DG2RAD / np.sqrt(2.0)
     sky = U.make_comps(U.MOD_POINT, 200, np.random.default_rng(6), radius_deg=2 / 60, center=(c, c))
-    mx, rms = model_error(uv, sky)
+    mx, rms = model_error(uv, sky, K=K)
     assert mx < TOL_REL, (mx, rms)
 
 
-def test_sampled_rows_config2_shape():
+@pytest.mark.parametrize("K", [0, 16])
+def test_sampled_rows_config2_shape(K):
     """Full config-2 channel/IF/polarization layout and component count on a
     few rows (the dataset's size-independent part)."""
     w = U.config2(nint=1, ncomp=20000, nant=6)
-    mx, rms = model_error(w.uv, w.sky)
+    mx, rms = model_error(w.uv, w.sky, K=K)
     assert mx < TOL_REL, (mx, rms)
+
+
+@pytest.mark.parametrize("Bt", [2, 16])
+def test_128_thread_ctas(Bt):
+    uv, sky = small(U.MOD_POINT_SPEC, nrow=70, nchan=64, nif=3, ncomp=90)
+    mx, _ = model_error(uv, sky, Bt=Bt, threads=128)
+    assert mx < TOL_REL
