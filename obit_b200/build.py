@@ -24,6 +24,7 @@ OBJ = PKG / "_build"
 
 CU_SOURCES = ["dft_plan.cu", "obit_dft_capi.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
+CXX_SOURCES = ["dft_planner.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -40,7 +41,7 @@ def _cuda_include() -> str:
 
 
 def _inputs() -> list[Path]:
-    files = [CSRC / s for s in CU_SOURCES + C_SOURCES]
+    files = [CSRC / s for s in CU_SOURCES + C_SOURCES + CXX_SOURCES]
     files += list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
     files.append(Path(__file__))
     return files
@@ -78,12 +79,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     for s in C_SOURCES:
         jobs.append(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", f"-I{INCLUDE}",
                      f"-I{_cuda_include()}", "-c", str(CSRC / s), "-o", str(OBJ / (s + ".o"))])
+    for s in CXX_SOURCES:
+        jobs.append(["g++", "-O2", "-fPIC", "-std=c++17", "-Wall", f"-I{INCLUDE}",
+                     f"-I{_cuda_include()}", "-c", str(CSRC / s), "-o", str(OBJ / (s + ".o"))])
     with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
         logs = list(ex.map(lambda c: _run(c, verbose), jobs))
     if ptxas_info:
         for log in logs:
             print(log, file=sys.stderr)
-    objs = [str(OBJ / (s + ".o")) for s in CU_SOURCES + C_SOURCES]
+    objs = [str(OBJ / (s + ".o")) for s in CU_SOURCES + C_SOURCES + CXX_SOURCES]
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lpthread"], verbose)
     os.replace(tmp, LIB)

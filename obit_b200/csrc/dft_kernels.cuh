@@ -27,65 +27,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "dft_types.h"
 #include "ds_math.cuh"
 #include "f32x2.cuh"
 
 namespace obit {
-
-constexpr int kThreads = 256;
-constexpr int kMaxNTerm = 4;   // spectral terms supported (ObitSkyModel nSpecTerm)
-constexpr int kMaxDf = 8;      // distinct channel increments per launch
-constexpr int kMaxPol = 4;
-constexpr int kMaxBt = 32;     // blocks per tile (R >= 8)
-
-// Model families; numbering matches GPUModType (ObitCUDASkyModelInfoDef.h:44-52).
-enum ModelKind : int {
-  kPoint = 0,
-  kPointSpec = 1,
-  kPointTSpec = 2,
-  kGauss = 3,
-  kGaussSpec = 4,
-  kGaussTSpec = 5
-};
-enum OpKind : int { kOpSub = 0, kOpDiv = 1, kOpRepl = 2 };
-enum KernelFlavor : int { kFlavorRecur = 0, kFlavorPlain = 1 };
-
-// One channel block: up to K consecutive channels of one IF.
-struct BlockDesc {
-  float f0_hi, f0_lo;  // frequency ratio nu/nu_uvref of the first channel (split-FP32)
-  float df;            // channel increment of the ratio (float copy, Gaussian exponent)
-  int off0;            // float offset of the first channel's pol-0 triplet in the record
-  int len;             // valid channels, 1..K
-  int dfc;             // channel-increment class (index into KParams.df_*)
-  int plane;           // coarse spectral plane (tabulated spectra)
-  int ifq0;            // frequency-table index of the first channel
-  // Quadratic fits over the block, L^(t+1)(k) ~ l[t][0] + l[t][1] k + l[t][2] k^2,
-  // of the log frequency ratio used by the spectral term (k = 0..len-1).
-  float l[kMaxNTerm][3];
-};
-
-struct KParams {
-  float* vis;  // device records, nvis x lrec floats
-  int nvis, lrec, ilocu, ilocv, ilocw;
-  int incs, incf;  // float increments between polarizations and channels
-  int pol0, npol;  // selected polarizations
-  int op;          // OpKind
-  int flipMask;    // bit j: multiply the j-th selected polarization's model by i
-  int cumulative;  // 1: CPU rule, stokFactor advances only on written polarizations
-  float stokFactor;
-  float polFact[kMaxPol];
-  const BlockDesc* blocks;
-  int nblocks;      // blocks per row
-  int Bt, R;        // tile shape: blocks per tile, rows per tile (Bt * R == kThreads)
-  int nBlockTiles;  // ceil(nblocks / Bt)
-  int ndf;
-  float df_hi[kMaxDf], df_lo[kMaxDf];
-  const float* comps;  // ncomp records of cstride floats (reference field order)
-  int ncomp, cstride, ct, nterm;
-  int nspec;           // planes (tabulated spectra)
-  int rowBase;         // first row index of this launch within vis
-  int* errFlag;        // set non-zero on an internal error (never traps)
-};
 
 // Reference field offsets inside a component record (ObitSkyModel.c:1965-2063,
 // ObitSkyModelMF.c:1497-1514).
@@ -126,29 +72,6 @@ __device__ __forceinline__ float2 phasor_fast(float r) {
   float s, c;
   __sincosf(6.283185307179586f * r, &s, &c);
   return make_float2(c, s);
-}
-
-//--------------------------------------------------------------------------
-// Shared memory per CTA (dynamic), sized by the host:
-//   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
-//   uvw    : R * 3 floats (padded to a multiple of 4)
-//   blk    : Bt BlockDesc (this tile's channel blocks)
-//   P      : ct * R float2            (phase turns, split-FP32)
-//   S      : ndf * ct * R float4      (step s and s^(K/2))
-//   Q      : ct * R floats            (Gaussian form, Gaussian models)
-//   G      : ct * Bt * (K + 2) floats (spectral amplitudes, spectral models)
-// The model stage of the epilogue (R * Bt * K float2) reuses the same space.
-//--------------------------------------------------------------------------
-__host__ __device__ inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf,
-                                                   bool gauss, bool table) {
-  size_t n = (size_t)ct * cstride + (size_t)((R * 3 + 3) & ~3) +
-             (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
-  if (gauss) n += (size_t)ct * R;
-  if (table) n += (size_t)ct * Bt * (K + 2);  // rows of K/2 + 1 float pairs
-  return n;
-}
-__host__ __device__ inline size_t smem_floats_stage(int R, int Bt, int K) {
-  return (size_t)R * Bt * K * 2;
 }
 
 // Apply the staged model of one tile to its records (subtract / divide /

@@ -1,13 +1,13 @@
 // Host-side planning for the DFT kernels: channel blocks, tile shape, shared
-// memory, and the launch itself.  Plain C++ over the kernel parameter block;
-// no torch types.
+// memory (plan_layout, plain C++ in dft_planner.cpp), and the device side of a
+// plan and the launch (dft_plan.cu).  No torch types.
 #pragma once
-#include <cuda_runtime.h>
+#include <cuda_runtime_api.h>
 
 #include <string>
 #include <vector>
 
-#include "dft_kernels.cuh"
+#include "dft_types.h"
 
 namespace obit {
 
@@ -66,8 +66,18 @@ struct Plan {
 // Padded component stride (floats): multiple of 4 so tiles are 16-byte aligned.
 int comp_stride(const ModelDesc& m);
 
-// Build the plan (allocates the device block table).  Returns 0 or an error
-// code with a message in err.
+// Host part of planning: validate, cut the selected channels into blocks,
+// choose channels per thread, tile shape and component tile.  Fills
+// plan->blocks and every KParams field except the pointers and row range.
+// No CUDA calls.  Returns 0 or an error code (3) with a message in err.
+int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
+                Plan* plan, std::string* err);
+
+// Whether a kernel instantiation exists for (flavor, K).
+bool kernel_exists(int flavor, int K);
+
+// Build the plan: plan_layout plus the device block table and launch limits.
+// Returns 0 or an error code with a message in err.
 int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
                Plan* plan, std::string* err);
 void free_plan(Plan* plan);
