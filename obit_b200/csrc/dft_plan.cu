@@ -66,11 +66,15 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
                Plan* plan, std::string* err) {
   int rc = plan_layout(L, M, A, T, plan, err);
   if (rc) return rc;
+  return finalize_plan(plan, nullptr, 0, err);
+}
+
+int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* err) {
   KParams& kp = plan->kp;
   const int K = plan->tune.K;
   const int threads = plan->threads;
   const int nblocks = kp.nblocks;
-  KernelFn fn = pick_kernel(plan->tune.flavor, K, M.kind);
+  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind);
   if (!fn) {
     *err = "no kernel for this flavor and channel count";
     return 3;
@@ -91,19 +95,27 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
   }
   plan->gridCap = perSM * nsm;
 
-  ce = cudaMalloc(&plan->d_blocks, sizeof(BlockDesc) * (size_t)std::max(1, nblocks));
-  if (ce != cudaSuccess) {
-    *err = std::string("cudaMalloc blocks: ") + cudaGetErrorString(ce);
-    return 2;
+  BlockDesc* table = dst;
+  if (!table) {
+    ce = cudaMalloc(&plan->d_blocks, sizeof(BlockDesc) * (size_t)std::max(1, nblocks));
+    if (ce != cudaSuccess) {
+      *err = std::string("cudaMalloc blocks: ") + cudaGetErrorString(ce);
+      return 2;
+    }
+    table = plan->d_blocks;
   }
+  // an owned table is filled synchronously (later launches may use any
+  // stream); a caller's buffer is filled in order on the caller's stream
   if (nblocks)
-    ce = cudaMemcpy(plan->d_blocks, plan->blocks.data(), sizeof(BlockDesc) * nblocks,
-                    cudaMemcpyHostToDevice);
+    ce = dst ? cudaMemcpyAsync(table, plan->blocks.data(), sizeof(BlockDesc) * nblocks,
+                               cudaMemcpyHostToDevice, stream)
+             : cudaMemcpy(table, plan->blocks.data(), sizeof(BlockDesc) * nblocks,
+                          cudaMemcpyHostToDevice);
   if (ce != cudaSuccess) {
-    *err = std::string("cudaMemcpy blocks: ") + cudaGetErrorString(ce);
+    *err = std::string("block table copy: ") + cudaGetErrorString(ce);
     return 2;
   }
-  kp.blocks = plan->d_blocks;
+  kp.blocks = table;
   return 0;
 }
 

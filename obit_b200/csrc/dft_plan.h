@@ -80,6 +80,11 @@ bool kernel_exists(int flavor, int K);
 // Returns 0 or an error code with a message in err.
 int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
                Plan* plan, std::string* err);
+// Device side of a laid-out plan: kernel attributes, launch limits and the
+// block table, copied on `stream` into dst (a device buffer of at least
+// kp.nblocks descriptors) or, when dst is NULL, into a table allocated here
+// and owned by the plan.
+int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* err);
 void free_plan(Plan* plan);
 
 // Launch on `stream` over rows [rowBase, rowBase + nvis) of d_vis.

@@ -16,16 +16,15 @@
 #include <vector>
 
 #include "obit_dft.h"
+#include "abi_internal.h"
 #include "dft_plan.h"
 
 namespace {
 
 using namespace obit;
 
-thread_local std::string g_last_error;
-
 int fail(int code, const std::string& msg) {
-  g_last_error = msg;
+  set_last_error(msg);
   return code;
 }
 
@@ -38,28 +37,16 @@ int fail(int code, const std::string& msg) {
 
 struct State {
   int device = 0;
-  // FP64 frequency side table
-  bool haveFreqD = false;
-  std::vector<double> freqArr, specFreq;
-  double uvRef = 0.0, modelRef = 0.0;
-  // CPU-reference polarization rules
-  bool cpuRules = false;
-  float stokFactor = 1.0f;
-  int doFlip = 0;
-  // kernel choice
-  TuneDesc tune;
-  // model
-  ModelDesc model;
-  int opType = 0, doSwap = 0;
-  float stokFact[4] = {1.f, 1.f, 1.f, 1.f};
-  std::vector<int> specIndex;
+  FreqSide fs;   // FP64 frequency side table
+  PolnRules pr;  // CPU-reference polarization rules
+  TuneDesc tune; // kernel choice
+  ModelCfg mc;   // model description
   float* d_comps = nullptr;
   size_t compBytes = 0;
   bool haveModel = false;
   // plan
   Plan plan;
   bool planValid = false;
-  int planNvis = -1;
   // staging
   int bufRows = 0;                 // rows per device staging buffer
   std::vector<float*> ownBufs;     // used when the caller supplies none
@@ -107,118 +94,17 @@ void release_state(State* s) {
   for (cudaStream_t st : s->ownStreams) cudaStreamDestroy(st);
 }
 
-// Build the layout description from the reference structures plus the
-// optional FP64 side table.
-int make_layout(GPUInfo* g, State* s, LayoutDesc* L) {
-  const GPUVisInfo* v = g->h_visInfo;
-  if (!v) return fail(OBIT_DFT_EBADARG, "GPUInfo.h_visInfo is NULL");
-  L->lrec = v->lenvis;
-  L->nrparm = v->nrparm;
-  L->ilocu = v->ilocu;
-  L->ilocv = v->ilocv;
-  L->ilocw = v->ilocw;
-  L->nchan = v->nchan;
-  L->nif = std::max(1, v->nIF);
-  L->nstok = v->nstok;
-  L->incs = 3 * v->incs;
-  L->incf = 3 * v->incf;
-  L->incif = 3 * v->incif;
-  L->kincf = v->kincf;
-  L->kincif = v->kincif;
-  L->chanb = v->chanb;
-  L->chane = v->chane;
-  L->ifb = v->IFb;
-  L->ife = v->IFe;
-  L->stokb = v->stokb;
-  L->stoke = v->stoke;
-  if (L->lrec <= 0 || L->nchan <= 0 || L->nstok <= 0)
-    return fail(OBIT_DFT_EBADARG, "record length, channel and polarization counts must be positive");
-  const int nfreq = L->nchan * L->nif;
-  // the frequency table must stay inside the record for every selected product
-  const long long lastOff = (long long)L->nrparm + (long long)L->ife * L->incif +
-                            (long long)L->chane * L->incf + (long long)L->stoke * L->incs + 2;
-  if (lastOff >= L->lrec) return fail(OBIT_DFT_EBADARG, "selected products extend past the record");
-  if (L->ilocu < 0 || L->ilocu >= L->nrparm || L->ilocv < 0 || L->ilocv >= L->nrparm ||
-      L->ilocw < 0 || L->ilocw >= L->nrparm)
-    return fail(OBIT_DFT_EBADARG, "u/v/w offsets must index random parameters");
-  L->fscale.assign(nfreq, 1.0);
-  if (s->haveFreqD) {
-    if ((int)s->freqArr.size() < nfreq) return fail(OBIT_DFT_EBADARG, "FP64 frequency table too short");
-    for (int i = 0; i < nfreq; i++) L->fscale[i] = s->freqArr[i] / s->uvRef;
-  } else {
-    if (!v->freqScale) return fail(OBIT_DFT_EBADARG, "GPUVisInfo.freqScale is NULL");
-    std::vector<float> fs(nfreq);
-    CUDA_TRY(cudaMemcpy(fs.data(), v->freqScale, sizeof(float) * nfreq, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < nfreq; i++) L->fscale[i] = (double)fs[i];
-  }
-  const int kind = s->model.kind;
-  if (kind == kPointSpec || kind == kGaussSpec) {
-    L->lnspec.assign(nfreq, 0.0);
-    for (int i = 0; i < nfreq; i++) {
-      double r;
-      if (s->haveFreqD)
-        r = s->freqArr[i] / (s->modelRef > 0 ? s->modelRef : s->uvRef);
-      else
-        r = L->fscale[i] * (v->freqRat ? (double)v->freqRat[0] : 1.0);
-      L->lnspec[i] = std::log(r);
-    }
-  } else if (kind == kPointTSpec || kind == kGaussTSpec) {
-    if ((int)s->specIndex.size() < nfreq)
-      return fail(OBIT_DFT_EBADARG, "tabulated spectra need GPUModelInfo.specIndex");
-    L->specIndex = s->specIndex;
-    L->lnspec.assign(nfreq, 0.0);
-    for (int i = 0; i < nfreq; i++) {
-      const int pl = s->specIndex[i];
-      if (pl < 0 || pl >= s->model.nspec)
-        return fail(OBIT_DFT_EBADARG, "specIndex outside the component's plane table");
-      double r;
-      if (s->haveFreqD && (int)s->specFreq.size() > pl)
-        r = s->freqArr[i] / s->specFreq[pl];
-      else if (v->freqRat)
-        r = L->fscale[i] * (double)v->freqRat[pl];
-      else
-        return fail(OBIT_DFT_EBADARG, "tabulated spectra need freqRat or specFreq");
-      L->lnspec[i] = std::log(r);
-    }
-  }
-  return OBIT_DFT_OK;
-}
-
-int make_apply(const GPUInfo* g, const State* s, const LayoutDesc& L, ApplyDesc* A) {
-  A->op = s->opType;
-  if (A->op < 0 || A->op > 2) return fail(OBIT_DFT_EBADARG, "unknown operation type");
-  if (s->cpuRules) {
-    A->cumulative = 1;
-    A->stokFactor = s->stokFactor;
-    for (int j = 0; j < kMaxPol; j++) A->polFact[j] = 1.0f;
-    A->flipMask = s->doFlip ? 0xF : 0;
-  } else {
-    // GPUModelInfo semantics: stokFact per polarization, doSwap on pol 3 only
-    A->cumulative = 0;
-    A->stokFactor = 1.0f;
-    for (int j = 0; j < kMaxPol; j++) {
-      const int ist = L.stokb + j;
-      A->polFact[j] = (ist < 4) ? s->stokFact[ist] : 1.0f;
-    }
-    A->flipMask = 0;
-    if (s->doSwap && L.stokb <= 3 && L.stoke >= 3) A->flipMask = 1 << (3 - L.stokb);
-  }
-  (void)g;
-  return OBIT_DFT_OK;
-}
-
 int ensure_plan(GPUInfo* g, State* s) {
   if (s->planValid) return OBIT_DFT_OK;
   if (!s->haveModel) return fail(OBIT_DFT_EBADARG, "no model set (call SetMod first)");
   LayoutDesc L;
-  int rc = make_layout(g, s, &L);
-  if (rc) return rc;
   ApplyDesc A;
-  rc = make_apply(g, s, L, &A);
-  if (rc) return rc;
-  free_plan(&s->plan);
   std::string err;
-  rc = build_plan(L, s->model, A, s->tune, &s->plan, &err);
+  int rc = layout_from_info(g->h_visInfo, s->mc, s->fs, &L, &err);
+  if (!rc) rc = apply_from_info(s->mc, s->pr, L, &A, &err);
+  if (rc) return fail(rc, err);
+  free_plan(&s->plan);
+  rc = build_plan(L, s->mc.model, A, s->tune, &s->plan, &err);
   if (rc) return fail(rc, err);
   s->planValid = true;
   return OBIT_DFT_OK;
@@ -240,45 +126,30 @@ extern "C" {
 
 int obit_dft_version(void) { return 100; }
 
-const char* obit_dft_last_error(void) { return g_last_error.c_str(); }
+const char* obit_dft_last_error(void) { return last_error(); }
 
 int obit_dft_init(GPUInfo* g) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   return ensure_state(g, &s);
 }
 
 int obit_dft_set_mod(GPUInfo* g) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
   const GPUModelInfo* m = g->h_modelInfo;
   if (!m) return fail(OBIT_DFT_EBADARG, "GPUInfo.h_modelInfo is NULL");
-  ModelDesc md;
-  md.kind = (int)m->type;
-  md.nterm = m->nterm;
-  md.lcomp = m->size > 0 ? m->size : g->modelSize;
-  md.ncomp = g->nmodel[0] > 0 ? g->nmodel[0] : m->nmodel[0];
-  if (md.kind < kPoint || md.kind > kGaussTSpec)
-    return fail(OBIT_DFT_EUNSUPPORTED, "model type " + std::to_string(md.kind) + " not supported");
-  if (md.ncomp < 0) return fail(OBIT_DFT_EBADARG, "negative component count");
-  const bool spec = (md.kind == kPointSpec || md.kind == kGaussSpec);
-  const bool tspec = (md.kind == kPointTSpec || md.kind == kGaussTSpec);
-  const bool gauss = (md.kind >= kGauss);
-  int minLen = 4;
-  if (gauss) minLen = 7;
-  if (spec) minLen += md.nterm;
-  if (tspec) minLen = (gauss ? 8 : 5) + 1;
-  if (md.ncomp > 0 && md.lcomp < minLen)
-    return fail(OBIT_DFT_EBADARG, "component record shorter than the model type needs");
-  if (spec && (md.nterm < 1 || md.nterm > kMaxNTerm))
-    return fail(OBIT_DFT_EUNSUPPORTED, "spectral term count must be 1.." + std::to_string(kMaxNTerm));
-  md.nspec = tspec ? md.lcomp - (gauss ? 8 : 5) : 0;
+  std::string err;
+  const int lcomp = m->size > 0 ? m->size : g->modelSize;
+  const int ncomp = g->nmodel[0] > 0 ? g->nmodel[0] : m->nmodel[0];
+  ModelCfg mc;
+  rc = model_from_info(m, ncomp, lcomp, g->h_visInfo, &mc, &err);
+  if (rc) return fail(rc, err);
   // padded copy of the component table (16-byte aligned rows for bulk copies)
-  const float* src = g->d_model[0] ? g->d_model[0] : m->model[0];
-  const size_t stride = (size_t)comp_stride(md);
-  const size_t bytes = std::max<size_t>(16, (size_t)md.ncomp * stride * sizeof(float));
+  const ModelDesc& md = mc.model;
+  const size_t bytes = std::max<size_t>(16, (size_t)md.ncomp * comp_stride(md) * sizeof(float));
   if (bytes > s->compBytes) {
     if (s->d_comps) cudaFree(s->d_comps);
     s->d_comps = nullptr;
@@ -286,31 +157,10 @@ int obit_dft_set_mod(GPUInfo* g) {
     CUDA_TRY(cudaMalloc(&s->d_comps, bytes));
     s->compBytes = bytes;
   }
-  if (md.ncomp > 0) {
-    if (!src) return fail(OBIT_DFT_EBADARG, "device component table is NULL");
-    CUDA_TRY(cudaMemset(s->d_comps, 0, (size_t)md.ncomp * stride * sizeof(float)));
-    CUDA_TRY(cudaMemcpy2D(s->d_comps, stride * sizeof(float), src, (size_t)md.lcomp * sizeof(float),
-                          (size_t)md.lcomp * sizeof(float), (size_t)md.ncomp, cudaMemcpyDeviceToDevice));
-  }
-  s->model = md;
-  s->opType = (int)m->opType;
-  s->doSwap = m->doSwap;
-  for (int i = 0; i < 4; i++) s->stokFact[i] = m->stokFact[i];
-  s->specIndex.clear();
-  if (tspec) {
-    const GPUVisInfo* v = g->h_visInfo;
-    if (!v) return fail(OBIT_DFT_EBADARG, "GPUInfo.h_visInfo is NULL");
-    const int nfreq = v->nchan * std::max(1, v->nIF);
-    if (m->specIndex) {
-      s->specIndex.assign(m->specIndex, m->specIndex + nfreq);
-    } else if (m->d_specIndex) {
-      s->specIndex.resize(nfreq);
-      CUDA_TRY(cudaMemcpy(s->specIndex.data(), m->d_specIndex, sizeof(int) * nfreq,
-                          cudaMemcpyDeviceToHost));
-    } else {
-      return fail(OBIT_DFT_EBADARG, "tabulated spectra need specIndex");
-    }
-  }
+  rc = copy_comps(s->d_comps, g->d_model[0] ? g->d_model[0] : m->model[0], md, 0, &err);
+  if (rc) return fail(rc, err);
+  CUDA_TRY(cudaStreamSynchronize(0));
+  s->mc = mc;
   s->haveModel = true;
   s->planValid = false;
   return OBIT_DFT_OK;
@@ -318,40 +168,40 @@ int obit_dft_set_mod(GPUInfo* g) {
 
 int obit_dft_set_freq(GPUInfo* g, const double* freqArr, int nfreq, double uvRefFreq,
                       double modelRefFreq, const double* specFreq, int nSpec) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
   if (!freqArr) {  // clear
-    s->haveFreqD = false;
+    s->fs.have = false;
     s->planValid = false;
     return OBIT_DFT_OK;
   }
   if (nfreq <= 0 || !(uvRefFreq > 0.0)) return fail(OBIT_DFT_EBADARG, "bad FP64 frequency table");
-  s->freqArr.assign(freqArr, freqArr + nfreq);
-  s->uvRef = uvRefFreq;
-  s->modelRef = modelRefFreq;
-  s->specFreq.clear();
-  if (specFreq && nSpec > 0) s->specFreq.assign(specFreq, specFreq + nSpec);
-  s->haveFreqD = true;
+  s->fs.freqArr.assign(freqArr, freqArr + nfreq);
+  s->fs.uvRef = uvRefFreq;
+  s->fs.modelRef = modelRefFreq;
+  s->fs.specFreq.clear();
+  if (specFreq && nSpec > 0) s->fs.specFreq.assign(specFreq, specFreq + nSpec);
+  s->fs.have = true;
   s->planValid = false;
   return OBIT_DFT_OK;
 }
 
 int obit_dft_set_poln(GPUInfo* g, int cpuRules, float stokFactor, int doFlip) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
-  s->cpuRules = cpuRules != 0;
-  s->stokFactor = stokFactor;
-  s->doFlip = doFlip;
+  s->pr.cpuRules = cpuRules != 0;
+  s->pr.stokFactor = stokFactor;
+  s->pr.doFlip = doFlip;
   s->planValid = false;
   return OBIT_DFT_OK;
 }
 
 int obit_dft_set_kernel(GPUInfo* g, int flavor, int chanPerThread, int compsPerTile) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
@@ -372,7 +222,7 @@ int obit_dft_set_kernel(GPUInfo* g, int flavor, int chanPerThread, int compsPerT
 }
 
 int obit_dft_set_tile(GPUInfo* g, int blocksPerTile, int threadsPerCTA) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
@@ -390,7 +240,7 @@ int obit_dft_set_tile(GPUInfo* g, int blocksPerTile, int threadsPerCTA) {
 }
 
 int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
@@ -405,7 +255,7 @@ int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
 }
 
 int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
@@ -420,7 +270,7 @@ int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
 }
 
 int obit_dft_check(GPUInfo* g) {
-  g_last_error.clear();
+  set_last_error("");
   State* s = find_state(g);
   if (!s) return fail(OBIT_DFT_EBADARG, "GPUInfo not initialized");
   CUDA_TRY(cudaSetDevice(s->device));
@@ -429,7 +279,7 @@ int obit_dft_check(GPUInfo* g) {
 }
 
 int obit_dft_calc(GPUInfo* g) {
-  g_last_error.clear();
+  set_last_error("");
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
@@ -496,7 +346,7 @@ int obit_dft_calc(GPUInfo* g) {
 }
 
 int obit_dft_shutdown(GPUInfo* g) {
-  g_last_error.clear();
+  set_last_error("");
   if (!g) return fail(OBIT_DFT_EBADARG, "NULL GPUInfo");
   std::unique_ptr<State> s;
   {
@@ -514,7 +364,7 @@ int obit_dft_shutdown(GPUInfo* g) {
 // ---- the reference's void entry points ----------------------------------
 
 static void report(const char* who, int rc) {
-  if (rc) fprintf(stderr, "%s: error %d: %s\n", who, rc, g_last_error.c_str());
+  if (rc) fprintf(stderr, "%s: error %d: %s\n", who, rc, last_error());
 }
 
 void ObitCUDASkyModelDFTInit(GPUInfo* gpuInfo) {
