@@ -286,15 +286,13 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    from obit_b200 import _lib
+    from obit_b200 import _lib, shard
     from obit_b200 import uvdata as U
     from obit_b200.skymodel import GPUSkyModel, SkyModelParams
 
     uvw, fa, freq, sky = workload_geometry(rank, args.rows, args.ncomp)
     if world > 1:  # replicate the component table from rank 0 (one broadcast, outside timing)
-        t = torch.from_numpy(sky.comps).to(device)
-        dist.broadcast(t, 0)
-        sky.comps = t.cpu().numpy()
+        sky.comps = shard.broadcast_model(torch.from_numpy(sky.comps).to(device)).cpu().numpy()
     rows = uvw.shape[0]
     nstok, nchan, nif = 4, 256, 4
     d_vis = build_vis(torch, uvw, nstok, nchan, nif, device, seed=100 + rank)
@@ -353,9 +351,7 @@ def main():
     t_ms = ev0.elapsed_time(ev1)
     launch_ms = [a.elapsed_time(b) for a, b in per_launch]
     if world > 1:
-        tt = torch.tensor([t_ms], device=device)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+        t_ms = shard.max_over_ranks(t_ms, device)
     value = world * evals * args.steps / (t_ms * 1e-3)
 
     # e2e: host buffer through obit_dft_calc (H2D + kernels + D2H inside)
@@ -375,9 +371,7 @@ def main():
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         if world > 1:
-            tt = torch.tensor([dt], device=device)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            dt = float(tt.item())
+            dt = shard.max_over_ranks(dt, device)
         e2e = {"value": world * evals * args.steps / dt / 1e9, "unit": "Gevals/s",
                "h2d_bytes_per_step": rows * lrec * 4, "d2h_bytes_per_step": rows * lrec * 4,
                "timing": "wall clock around the synchronous C-ABI call, max over ranks"}
