@@ -197,6 +197,27 @@ int obit_dft_calc_device(GPUInfo *gpuInfo, float *d_vis, int nvis, void *stream)
  * Writes min(n, 8) entries. */
 int obit_dft_plan_info(GPUInfo *gpuInfo, int *info, int n);
 
+/* No counterpart in the reference.  The same model application as
+ * obit_dft_calc_device, for callers that cannot let a library allocate device
+ * memory: processes whose device memory is all owned by their own pool (a
+ * caching allocator, or a job sized to fill HBM), and latency-bound callers
+ * that cannot take cudaFree's implicit device synchronization.  The caller passes
+ * only inputs and outputs: the descriptors (host structs; visInfo->freqScale,
+ * modelInfo->model[0] and the records d_vis are device memory, specIndex
+ * host or device), an optional FP64 frequency table as for obit_dft_set_freq
+ * (freqArr NULL uses the FP32 freqScale), and nvis records at d_vis updated in
+ * place on `stream`.  Polarizations follow GPUModelInfo (stokFact, doSwap).
+ * Scratch lives in a fixed 8 MiB device array inside the library (error flag,
+ * channel blocks, padded component table): larger models are rejected with
+ * OBIT_DFT_EUNSUPPORTED.  No cudaMalloc/cudaFree is called.  The first call on
+ * a device resolves the array's address and should precede any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialized.  Returns after the stream has completed the update. */
+int obit_dft_calc_noalloc(const GPUVisInfo *visInfo, const GPUModelInfo *modelInfo,
+                          const double *freqArr, double uvRefFreq, double modelRefFreq,
+                          const double *specFreq, int nSpec, float *d_vis, int nvis,
+                          void *stream);
+
 /* Reads and clears the kernels' device error flag (synchronizes the device):
  * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */
 int obit_dft_check(GPUInfo *gpuInfo);

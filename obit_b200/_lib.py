@@ -96,6 +96,10 @@ SIGNATURES = {
     "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),
     "obit_dft_plan_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
+    "obit_dft_calc_noalloc": (C.c_int, [C.POINTER(GPUVisInfo), C.POINTER(GPUModelInfo),
+                                        C.POINTER(C.c_double), C.c_double, C.c_double,
+                                        C.POINTER(C.c_double), C.c_int, C.c_void_p, C.c_int,
+                                        C.c_void_p]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_last_error": (C.c_char_p, []),
     "obit_dft_version": (C.c_int, []),
