@@ -36,6 +36,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_EVAL = 10.0  # complex rotate (6) + accumulate (4), algorithmic
+# DRAM bytes (read + write) per record of the config-2 layout, from one ncu
+# capture of dft_recur_kernel<32, 1> at 10,080 records (499.93 MB read + 444.28
+# MB written); traffic grows in proportion to records, so a launch's traffic is
+# this figure times its records.
+NCU_DRAM_BYTES_PER_RECORD = (499.93e6 + 444.28e6) / 10080
 
 
 def parse():
@@ -210,7 +215,8 @@ def cpu_baseline(rows_uvw, fa, freq, sky, seconds: float):
         nrow = min(nrow, len(rows_uvw))
         dt = run(nrow)
     evals = nrow * 1024 * sky.ncomp
-    name = "reference CPU DFT restatement with the reference's ObitSinCosVec/ObitExpVec" if have_ref \
+    name = ("restatement of the reference CPU DFT loop (FP32 phase) linked with the reference's own "
+            "ObitSinCosVec/ObitExpVec compiled from its sources") if have_ref \
         else "FP64 oracle (reference vector math not built)"
     return evals / dt, cores, f"{nrow} rows x 1024 channels x {sky.ncomp} components ({name}), {dt:.1f} s", kind
 
@@ -249,8 +255,11 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f32 (FP32 phase, FP64 component sum)", "data": "synthetic",
         "config": config_block(args, sky, nrow_override=nrow),
         "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": cores,
-                         "kind": "reference" if have_ref else "port",
-                         "sample": f"{nrow} rows x 1024 channels x {sky.ncomp} components per step"},
+                         "kind": "port",
+                         "sample": f"{nrow} rows x 1024 channels x {sky.ncomp} components per step "
+                                   "(restatement of the reference CPU DFT loop linked with the reference's "
+                                   "own ObitSinCosVec/ObitExpVec)" if have_ref else
+                                   f"{nrow} rows x 1024 channels x {sky.ncomp} components per step (FP64 oracle)"},
         "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -397,7 +406,10 @@ def main():
             "data": "synthetic (seeded uvw, noise visibilities, random components)",
             "config": config_block(args, sky, kernel=kern),
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": NCU_DRAM_BYTES_PER_RECORD * rows if args.flavor == "recur" else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record "
+                                           "(10,080-record capture) x records per launch",
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
                          "flops_per_eval": FLOPS_PER_EVAL},
             "cpu_baseline": cpu,
