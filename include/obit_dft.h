@@ -218,6 +218,79 @@ int obit_dft_calc_noalloc(const GPUVisInfo *visInfo, const GPUModelInfo *modelIn
                           const double *specFreq, int nSpec, float *d_vis, int nvis,
                           void *stream);
 
+/* ---- multi-facet batch ---------------------------------------------------
+ * The reference applies a multi-facet model one field (and one buffer) at a
+ * time: ObitSkyModel loops over the mosaic's images and calls
+ * ObitGPUSkyModelDFTCalc / ObitCUDASkyModelDFTCalc per buffer
+ * (ObitSystem/Obit/src/ObitGPUSkyModel.c:502-518).  The batch below has no
+ * counterpart there: it applies many facets -- each its own device-resident
+ * records, layout, frequencies and component table, with uneven row and
+ * component counts -- in one persistent kernel launch per model family,
+ * captured once in a CUDA graph and replayed.  Facets of one model family
+ * share one tile shape (channels per thread, components per tile, blocks and
+ * rows per CTA), chosen by obit_dft_batch_autotune or set explicitly. */
+
+/* One facet.  visInfo/modelInfo are read at creation as for the single-facet
+ * calls (modelInfo->model[0] is the device component table of nmodel[0] rows
+ * of `size` floats, copied at creation; visInfo->freqScale is read unless
+ * freqArr is given); d_vis holds nvis records updated in place by each run.
+ * cpuRules/stokFactor/doFlip as for obit_dft_set_poln. */
+typedef struct {
+  const GPUVisInfo *visInfo;
+  const GPUModelInfo *modelInfo;
+  const double *freqArr; /* optional nchan*nIF FP64 channel frequencies (Hz) */
+  double uvRefFreq;      /* data reference frequency (with freqArr) */
+  double modelRefFreq;   /* polynomial-spectrum reference (0 = uvRefFreq) */
+  const double *specFreq;/* coarse-plane frequencies, tabulated spectra */
+  int nSpec;
+  int cpuRules;
+  float stokFactor;
+  int doFlip;
+  float *d_vis;
+  int nvis;
+} ObitDFTFacet;
+
+typedef struct ObitDFTBatch ObitDFTBatch;
+
+/* Plans every facet on the current device (tile shape: the planner's default
+ * for the first facet of each model family until tuned or set), copies the
+ * component tables and builds the facet parameter blocks and work list. */
+int obit_dft_batch_create(const ObitDFTFacet *facets, int nfacet, ObitDFTBatch **out);
+
+/* Times candidate tile shapes per model family on a scratch copy of a row
+ * sample of every facet (the facets' records are not modified) and keeps the
+ * fastest.  best (may be NULL) receives, for the family of the most work,
+ * {K, compsPerTile, blocksPerTile, rowsPerTile, threads, candidates tried}. */
+int obit_dft_batch_autotune(ObitDFTBatch *batch, void *stream, int *best);
+
+/* Fixes the tile shape of every model family (0 keeps the planner's choice
+ * for that field); invalidates the captured graph. */
+int obit_dft_batch_set_tile(ObitDFTBatch *batch, int chanPerThread, int compsPerTile,
+                            int blocksPerTile, int threadsPerCTA);
+
+/* Applies every facet's model to its records: one graph launch on `stream`
+ * holding, per model family, a counter reset and one persistent batch kernel.
+ * The graph is captured at the first run after creation or a tile change.
+ * Asynchronous; obit_dft_batch_check reads the kernels' error flag. */
+int obit_dft_batch_run(ObitDFTBatch *batch, void *stream);
+
+/* Comparator: the same work as one kernel launch per facet on `stream`, with
+ * each facet's own planner-default plan of kernel `flavor`
+ * (OBIT_DFT_RECUR or OBIT_DFT_PLAIN). */
+int obit_dft_batch_run_per_facet(ObitDFTBatch *batch, int flavor, void *stream);
+
+/* Synchronizes the device, reads and clears the batch's error flag. */
+int obit_dft_batch_check(ObitDFTBatch *batch);
+
+/* Batch facts: info[0] facets, [1] model families (kernel launches per run),
+ * [2] work items, [3] component-visibility evaluations per run, then for the
+ * family of the most work [4] K, [5] compsPerTile, [6] blocksPerTile,
+ * [7] rowsPerTile, [8] threads, [9] grid.  Writes min(n, 10) entries. */
+int obit_dft_batch_info(ObitDFTBatch *batch, long long *info, int n);
+
+/* Releases the batch's device memory, graph and streams. */
+int obit_dft_batch_destroy(ObitDFTBatch *batch);
+
 /* Reads and clears the kernels' device error flag (synchronizes the device):
  * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */
 int obit_dft_check(GPUInfo *gpuInfo);

@@ -75,6 +75,16 @@ class ObitDFTErr(C.Structure):
     _fields_ = [("error", C.c_int), ("prtLv", C.c_int), ("message", C.c_char * 512)]
 
 
+class ObitDFTFacet(C.Structure):
+    _fields_ = [
+        ("visInfo", C.POINTER(GPUVisInfo)), ("modelInfo", C.POINTER(GPUModelInfo)),
+        ("freqArr", C.POINTER(C.c_double)), ("uvRefFreq", C.c_double),
+        ("modelRefFreq", C.c_double), ("specFreq", C.POINTER(C.c_double)), ("nSpec", C.c_int),
+        ("cpuRules", C.c_int), ("stokFactor", C.c_float), ("doFlip", C.c_int),
+        ("d_vis", C.c_void_p), ("nvis", C.c_int),
+    ]
+
+
 # ---- exported symbols, with C signatures ------------------------------------
 
 _GPUINFO_P = C.POINTER(GPUInfo)
@@ -100,6 +110,14 @@ SIGNATURES = {
                                         C.POINTER(C.c_double), C.c_double, C.c_double,
                                         C.POINTER(C.c_double), C.c_int, C.c_void_p, C.c_int,
                                         C.c_void_p]),
+    "obit_dft_batch_create": (C.c_int, [C.POINTER(ObitDFTFacet), C.c_int, C.POINTER(C.c_void_p)]),
+    "obit_dft_batch_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "obit_dft_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "obit_dft_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "obit_dft_batch_run_per_facet": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "obit_dft_batch_check": (C.c_int, [C.c_void_p]),
+    "obit_dft_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
+    "obit_dft_batch_destroy": (C.c_int, [C.c_void_p]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_last_error": (C.c_char_p, []),
     "obit_dft_version": (C.c_int, []),

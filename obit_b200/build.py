@@ -22,7 +22,8 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libobit_dft.so"
 OBJ = PKG / "_build"
 
-CU_SOURCES = ["dft_plan.cu", "abi_layout.cu", "obit_dft_capi.cu", "obit_dft_static.cu"]
+CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "abi_layout.cu", "obit_dft_capi.cu",
+              "obit_dft_static.cu", "dft_batch.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
 CXX_SOURCES = ["dft_planner.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -311,13 +311,18 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 //--------------------------------------------------------------------------
 // Recurrence kernel.  K channels per thread (even), MODE model family.
 //--------------------------------------------------------------------------
+
+// One work item: rows [rt R, rt R + R) x channel-block tile bt of plan p, where
+// item = rt * nBlockTiles + bt.  smem is the CTA's dynamic shared memory, bar
+// its bulk-copy mbarrier with the running parity in phase.  Returns false (the
+// error flag set, uniformly across the CTA) when a component copy did not land;
+// the caller must then leave the kernel.
 template <int K, int MODE>
-__global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(const KParams p) {
+__device__ __forceinline__ bool recur_item(const KParams& p, int item, float* smem, uint64_t* bar,
+                                           uint32_t& phase) {
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
   constexpr int H = K / 2;
   using F = Fields<MODE>;
-  extern __shared__ __align__(16) float smem[];
-  __shared__ __align__(8) uint64_t bar;
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
@@ -329,10 +334,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
   float* sG = sQ + (F::kGaussian ? ct * R : 0);
   float2* stage = reinterpret_cast<float2*>(smem);
 
-  init_bar(&bar);
-  uint32_t phase = 0;
-
-  // R and Bt are powers of two (R * Bt == kThreads)
+  // R and Bt are powers of two (R * Bt == CTA size)
   const int lgR = __ffs(R) - 1;
   const int lgBt = __ffs(Bt) - 1;
   constexpr int lgH = (H >= 16) ? 4 : (H >= 8) ? 3 : (H >= 4) ? 2 : (H >= 2) ? 1 : 0;
@@ -341,9 +343,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
   const int tr = threadIdx.x & (R - 1);  // row within the tile
   const int tb = threadIdx.x >> lgR;     // block within the tile
 
-  const int nRowTiles = (p.nvis + R - 1) / R;
-  const int nItems = nRowTiles * p.nBlockTiles;
-  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
+  {
     const int rt = item / p.nBlockTiles;
     const int bt = item - rt * p.nBlockTiles;
     const int row0 = rt * R;
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // previous tile's readers are done with shared memory
-      if (!stage_comps(p, sComp, c0, &bar, phase)) return;
+      if (!stage_comps(p, sComp, c0, bar, phase)) return false;
       __syncthreads();
 
       // (row, component): phase turns, steps, Gaussian form
@@ -497,6 +497,68 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2)) dft_recur_kernel(
     }
     __syncthreads();
     apply_tile<K>(p, stage, row0, blk0, nblkTile);
+  }
+  return true;
+}
+
+template <int K, int MODE>
+__global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
+    dft_recur_kernel(const __grid_constant__ KParams p) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ __align__(8) uint64_t bar;
+  init_bar(&bar);
+  uint32_t phase = 0;
+  const int nItems = ((p.nvis + p.R - 1) / p.R) * p.nBlockTiles;
+  for (int item = blockIdx.x; item < nItems; item += gridDim.x)
+    if (!recur_item<K, MODE>(p, item, smem, &bar, phase)) return;
+  inval_bar(&bar);
+}
+
+// Batched recurrence kernel: many facets (each its own records, layout,
+// channel blocks and component table; one tile shape and model family) in one
+// persistent launch.  The work items of all facets form one list, facets in
+// decreasing cost per item; CTAs take items from a device counter (zero at
+// launch) so uneven facets balance across the SMs, and load a facet's
+// parameter block into shared memory when they move to a new facet.
+template <int K, int MODE>
+__global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
+    dft_recur_batch_kernel(const __grid_constant__ BatchParams bp) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(16) KParams sp;
+  __shared__ int sItem, sFacet;
+  init_bar(&bar);
+  uint32_t phase = 0;
+  const int total = bp.itemStart[bp.nfacet];
+  int cur = -1;
+  for (;;) {
+    __syncthreads();  // every thread is done with the previous item and with sp
+    if (threadIdx.x == 0) {
+      const int it = atomicAdd(bp.counter, 1);
+      int f = 0;
+      if (it < total) {  // facet f with itemStart[f] <= it < itemStart[f + 1]
+        int lo = 0, hi = bp.nfacet - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (bp.itemStart[mid] <= it) lo = mid; else hi = mid - 1;
+        }
+        f = lo;
+      }
+      sItem = it;
+      sFacet = f;
+    }
+    __syncthreads();
+    const int it = sItem;
+    if (it >= total) break;
+    const int f = sFacet;
+    if (f != cur) {
+      const int* src = reinterpret_cast<const int*>(bp.facets + f);
+      int* dst = reinterpret_cast<int*>(&sp);
+      for (int i = threadIdx.x; i < (int)(sizeof(KParams) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+      cur = f;
+      __syncthreads();
+    }
+    if (!recur_item<K, MODE>(sp, it - bp.itemStart[f], smem, &bar, phase)) return;
   }
   inval_bar(&bar);
 }

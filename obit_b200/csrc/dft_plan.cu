@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "dft_kernels.cuh"
@@ -62,6 +63,27 @@ KernelFn pick_kernel(int flavor, int K, int mode) {
 
 }  // namespace
 
+// The dynamic shared-memory limit is an attribute of the kernel function, not
+// of a launch: plans of one kernel with different tile sizes share it.  Only
+// ever raise it (per device), so that a plan finalized earlier with a larger
+// tile still launches after a smaller one was finalized.
+int raise_smem_limit(const void* fn, size_t bytes, std::string* err) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limit;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[{dev, fn}];
+  if (bytes <= cur) return 0;
+  cudaError_t ce = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (ce != cudaSuccess) {
+    *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce);
+    return 2;
+  }
+  cur = bytes;
+  return 0;
+}
+
 int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
                Plan* plan, std::string* err) {
   int rc = plan_layout(L, M, A, T, plan, err);
@@ -79,12 +101,8 @@ int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* 
     *err = "no kernel for this flavor and channel count";
     return 3;
   }
-  cudaError_t ce =
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan->smemBytes);
-  if (ce != cudaSuccess) {
-    *err = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ce);
-    return 2;
-  }
+  if (int rc = raise_smem_limit((const void*)fn, plan->smemBytes, err)) return rc;
+  cudaError_t ce;
   int perSM = 0, dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -140,10 +158,24 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);
   KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind);
-  fn<<<grid, plan.threads, plan.smemBytes, stream>>>(kp);
+  // an error left by an earlier, unrelated runtime call would otherwise be
+  // reported as this launch's
   cudaError_t ce = cudaGetLastError();
   if (ce != cudaSuccess) {
-    *err = std::string("kernel launch: ") + cudaGetErrorString(ce);
+    *err = std::string("error pending before the kernel launch: ") + cudaGetErrorString(ce);
+    return 2;
+  }
+  fn<<<grid, plan.threads, plan.smemBytes, stream>>>(kp);
+  ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, fn);
+    cudaGetLastError();
+    *err = std::string("kernel launch (grid ") + std::to_string(grid) + ", " +
+           std::to_string(plan.threads) + " threads, " + std::to_string(plan.smemBytes) +
+           " B shared; kernel allows " + std::to_string(fa.maxDynamicSharedSizeBytes) +
+           " B dynamic, " + std::to_string(fa.sharedSizeBytes) + " B static, " +
+           std::to_string(fa.maxThreadsPerBlock) + " threads): " + cudaGetErrorString(ce);
     return 2;
   }
   return 0;

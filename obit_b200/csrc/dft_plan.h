@@ -94,4 +94,16 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
 // Supported channel-block lengths.
 bool valid_K(int K);
 
+// Raise (never lower) kernel fn's dynamic shared-memory limit on the current
+// device to at least `bytes`; the limit is shared by every plan of fn.
+int raise_smem_limit(const void* fn, size_t bytes, std::string* err);
+
+// Batched recurrence kernel (dft_batch_kernels.cu): whether K is instantiated;
+// set the shared-memory attribute and report the resident CTAs across the
+// device; launch `grid` persistent CTAs over the batch on `stream`.
+bool batch_kernel_exists(int K);
+int batch_prepare(int K, int mode, int threads, size_t smemBytes, int* gridCap, std::string* err);
+int launch_batch(int K, int mode, const BatchParams& bp, int grid, int threads, size_t smemBytes,
+                 cudaStream_t stream, std::string* err);
+
 }  // namespace obit

@@ -67,6 +67,15 @@ struct KParams {
   int* errFlag;        // set non-zero on an internal error (never traps)
 };
 
+// A batched launch over many facets (one KParams each, same tile shape and
+// model family): items [itemStart[f], itemStart[f + 1]) belong to facet f.
+struct BatchParams {
+  const KParams* facets;  // device array of nfacet parameter blocks
+  const int* itemStart;   // device array of nfacet + 1 cumulative item counts
+  int nfacet;
+  int* counter;           // device work counter, zero at launch
+};
+
 //--------------------------------------------------------------------------
 // Shared memory per CTA of the recurrence kernel (dynamic):
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
