@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--rows", type=int, default=100800)
-    ap.add_argument("--ncomp", type=int, default=20000)
+    ap.add_argument("--rows", type=int, default=None,
+                    help="records per step (default: 100800 for config2/3, the whole track else)")
+    ap.add_argument("--ncomp", type=int, default=None, help="components (default: the config's)")
     ap.add_argument("--flavor", default="recur", choices=["recur", "plain"])
     ap.add_argument("--K", type=int, default=0)
     ap.add_argument("--ct", type=int, default=0)
@@ -60,7 +61,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM FP32 peak measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--workload", default="config2", choices=["config2", "config5"],
+    ap.add_argument("--workload", default="config2",
+                    choices=["config1", "config2", "config3", "config4", "config5"],
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
                          "96-facet uneven batch")
     ap.add_argument("--row-scale", type=float, default=0.01,
@@ -74,24 +76,81 @@ def parse():
 # ---- workload ------------------------------------------------------------------
 
 
-def workload_geometry(rank: int, rows: int, ncomp: int):
-    """uvw for this rank's chunk and the (shared) component table."""
+class Geometry:
+    """One bench workload: this rank's rows (u, v, w), the channel frequencies,
+    the component table and the record shape."""
+
+    def __init__(self, name, uvw, fa, freq, sky, nstok, nchan, nif, desc):
+        self.name, self.uvw, self.fa, self.freq, self.sky = name, uvw, fa, freq, sky
+        self.nstok, self.nchan, self.nif, self.desc = nstok, nchan, nif, desc
+
+    @property
+    def rows(self):
+        return self.uvw.shape[0]
+
+    @property
+    def channels(self):
+        return self.nchan * self.nif
+
+
+DEFAULT_ROWS = {"config1": 42120, "config2": 100800, "config3": 100800, "config4": 119040}
+
+
+def _track(nant, max_bl, nint, freq, seed, rows, rank):
+    """rows of a time-major track of nint integrations, this rank's contiguous slice."""
     from obit_b200 import uvdata as U
 
-    nbl = 2016
-    nint_total = 2000
-    nint = max(1, (rows + nbl - 1) // nbl)
-    rng = np.random.default_rng(2)
-    pos = U.array_layout(64, 36e3, rng)
-    freq = 1.4e9
-    fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
-    # this rank's integrations: a contiguous slice of the 2000-integration track
-    i0 = (rank * nint) % max(1, nint_total - nint + 1)
-    uvw_all = U.make_uvw(pos, nint_total, 45.0, 4.0, 34.0, freq).reshape(nint_total, nbl, 3)
-    uvw = uvw_all[i0:i0 + nint].reshape(-1, 3)[:rows]
-    sky = U.make_comps(U.MOD_POINT_SPEC, ncomp, np.random.default_rng(4), radius_deg=1.0,
-                       nterm=1, ref_freq=freq)
-    return uvw, fa, freq, sky
+    pos = U.array_layout(nant, max_bl, np.random.default_rng(seed))
+    nbl = nant * (nant - 1) // 2
+    per = max(1, (rows + nbl - 1) // nbl)
+    i0 = (rank * per) % max(1, nint - per + 1)
+    uvw = U.make_uvw(pos, nint, 45.0, 4.0, 34.0, freq).reshape(nint, nbl, 3)
+    return uvw[i0:i0 + per].reshape(-1, 3)[:rows]
+
+
+def workload_geometry(name: str, rank: int, rows: int | None, ncomp: int | None) -> Geometry:
+    """The named configuration (seeded as obit_b200.uvdata.config1..4); config2
+    and config3 hold one chunk of `rows` records of the 4.032e6-record track."""
+    from obit_b200 import uvdata as U
+
+    rows = rows or DEFAULT_ROWS[name]
+    if name == "config1":
+        freq = 1.4e9
+        fa = U.freq_axis(64, 1, freq - 32e6, 1e6)
+        uvw = _track(27, 36e3, 120, freq, 1, rows, rank)
+        sky = U.make_comps(U.MOD_POINT, ncomp or 1000, np.random.default_rng(3), radius_deg=0.5)
+        return Geometry(name, uvw, fa, freq, sky, 2, 64, 1,
+                        f"config1: {len(uvw)} records (27 antennas, 351 baselines x 120 "
+                        f"integrations) x 1 IF x 64 ch x 2 pol, {sky.ncomp} point components")
+    if name in ("config2", "config3"):
+        freq = 1.4e9
+        fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
+        if name == "config2":
+            uvw = _track(64, 36e3, 2000, freq, 2, rows, rank)
+            sky = U.make_comps(U.MOD_POINT_SPEC, ncomp or 20000, np.random.default_rng(4),
+                               radius_deg=1.0, nterm=1, ref_freq=freq)
+            what = f"{sky.ncomp} point components with spectral index"
+        else:
+            uvw = _track(64, 36e3, 2000, freq, 3, rows, rank)
+            sky = U.make_comps(U.MOD_GAUSS_SPEC, ncomp or 50000, np.random.default_rng(5),
+                               radius_deg=1.0, nterm=1, gauss_frac=0.3, ref_freq=freq)
+            what = (f"{sky.ncomp} components (70 % point, 30 % elliptical Gaussian) with "
+                    "spectral index")
+        return Geometry(name, uvw, fa, freq, sky, 4, 256, 4,
+                        f"{name} chunk: {len(uvw)} records (64 antennas, 2016 baselines) x 4 IF x "
+                        f"256 ch x 4 pol, {what}; the 4.032e6-record dataset is streamed in such chunks")
+    if name == "config4":
+        freq = 22e9
+        fa = U.freq_axis(64, 8, freq - 512e6, 2e6)
+        uvw = _track(32, 8.0e6, 240, freq, 4, rows, rank)
+        c = 0.3 * U.DG2RAD / math.sqrt(2.0)
+        sky = U.make_comps(U.MOD_POINT, ncomp or 10000, np.random.default_rng(6),
+                           radius_deg=2.0 / 60.0, center=(c, c))
+        return Geometry(name, uvw, fa, freq, sky, 2, 64, 8,
+                        f"config4: {len(uvw)} records (32 antennas to 8000 km, 496 baselines x 240 "
+                        f"integrations) at 22 GHz x 8 IF x 64 ch x 2 pol, {sky.ncomp} point "
+                        "components within 2 arcmin of a position 0.3 deg from the phase centre")
+    raise ValueError(name)
 
 
 def build_vis(torch, uvw, nstok, nchan, nif, device, seed):
@@ -193,7 +252,7 @@ def fp32_peak_tflops(torch, device) -> float:
 # ---- CPU baseline ------------------------------------------------------------------
 
 
-def cpu_baseline(rows_uvw, fa, freq, sky, seconds: float):
+def cpu_baseline(g: Geometry, seconds: float):
     """Reference CPU DFT restatement (oracle/_ref: the reference's ObitSinCosVec /
     ObitExpVec, FP32 phase, rows split over pthreads as ObitSkyModelFTDFT) on a
     bounded sample of the same workload; returns (evals/s, cores, sample text, kind)."""
@@ -206,9 +265,11 @@ def cpu_baseline(rows_uvw, fa, freq, sky, seconds: float):
     have_ref = oracle.have_refcpu()
     kind = "port"
 
+    sky = g.sky
+
     def run(nrow):
-        uvw = rows_uvw[:nrow]
-        uv = U.make_uvdata(uvw, 4, 256, 4, freq, fa, np.random.default_rng(9))
+        uv = U.make_uvdata(g.uvw[:nrow], g.nstok, g.nchan, g.nif, g.freq, g.fa,
+                           np.random.default_rng(9))
         t0 = time.perf_counter()
         if have_ref:
             oracle.apply_refcpu(uv, sky, SkyModelParams(), nthreads=cores)
@@ -220,13 +281,14 @@ def cpu_baseline(rows_uvw, fa, freq, sky, seconds: float):
     dt = run(nrow)
     if dt < seconds / 3:
         nrow = max(cores, int(nrow * (seconds / max(dt, 1e-3))))
-        nrow = min(nrow, len(rows_uvw))
+        nrow = min(nrow, g.rows)
         dt = run(nrow)
-    evals = nrow * 1024 * sky.ncomp
+    evals = nrow * g.channels * sky.ncomp
     name = ("restatement of the reference CPU DFT loop (FP32 phase) linked with the reference's own "
             "ObitSinCosVec/ObitExpVec compiled from its sources") if have_ref \
         else "FP64 oracle (reference vector math not built)"
-    return evals / dt, cores, f"{nrow} rows x 1024 channels x {sky.ncomp} components ({name}), {dt:.1f} s", kind
+    return (evals / dt, cores,
+            f"{nrow} rows x {g.channels} channels x {sky.ncomp} components ({name}), {dt:.1f} s", kind)
 
 
 # ---- arms ------------------------------------------------------------------------
@@ -236,7 +298,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    uvw, fa, freq, sky = workload_geometry(0, max(args.rows, 64), args.ncomp)
+    g = workload_geometry(args.workload, 0, args.rows, args.ncomp)
+    sky = g.sky
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     from obit_b200 import uvdata as U
@@ -245,7 +308,7 @@ def run_reference(args):
     cores = oracle.nthreads_default()
     have_ref = oracle.have_refcpu()
     nrow = max(cores, 8)
-    uv = U.make_uvdata(uvw[:nrow], 4, 256, 4, freq, fa, np.random.default_rng(9))
+    uv = U.make_uvdata(g.uvw[:nrow], g.nstok, g.nchan, g.nif, g.freq, g.fa, np.random.default_rng(9))
     fn = oracle.apply_refcpu if have_ref else oracle.apply_fp64
     for _ in range(args.warmup):
         fn(uv, sky, SkyModelParams(), nthreads=cores)
@@ -254,33 +317,33 @@ def run_reference(args):
         t0 = time.perf_counter()
         fn(uv, sky, SkyModelParams(), nthreads=cores)
         ts.append(time.perf_counter() - t0)
-    evals = nrow * 1024 * sky.ncomp
+    evals = nrow * g.channels * sky.ncomp
     v = evals * len(ts) / sum(ts) / 1e9
     line = {
         "impl": "reference", "metric": "component-visibility evals/s (DFT subtract)",
         "value": v, "unit": "Gevals/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(ts) / len(ts), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP32 phase, FP64 component sum)", "data": "synthetic",
-        "config": config_block(args, sky, nrow_override=nrow),
+        "config": config_block(g, nrow_override=nrow),
         "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": cores,
                          "kind": "port",
-                         "sample": f"{nrow} rows x 1024 channels x {sky.ncomp} components per step "
+                         "sample": f"{nrow} rows x {g.channels} channels x {sky.ncomp} components per step "
                                    "(restatement of the reference CPU DFT loop linked with the reference's "
                                    "own ObitSinCosVec/ObitExpVec)" if have_ref else
-                                   f"{nrow} rows x 1024 channels x {sky.ncomp} components per step (FP64 oracle)"},
+                                   f"{nrow} rows x {g.channels} channels x {sky.ncomp} components per step (FP64 oracle)"},
         "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def config_block(args, sky, nrow_override=None, kernel=None):
-    rows = nrow_override or args.rows
-    return {"workload": f"config2 chunk: {rows} records (64 antennas, 2016 baselines) x 4 IF x 256 "
-                        f"ch x 4 pol, {sky.ncomp} point components with spectral index; the "
-                        "4.032e6-record dataset is streamed in such chunks",
-            "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024, "polarizations": 4,
-            "model": "PointSpec nterm=1", "w_term": True,
-            "l2": "inputs larger than L2 (record chunk >> 126 MB)",
+def config_block(g: Geometry, nrow_override=None, kernel=None):
+    rows = nrow_override or g.rows
+    return {"workload": g.desc if nrow_override is None else g.desc.replace(f"{g.rows} records", f"{rows} records"),
+            "rows_per_step": rows, "components": int(g.sky.ncomp), "channels": g.channels,
+            "polarizations": g.nstok, "model": {0: "Point", 10: "PointSpec nterm=1",
+                                                11: "GaussSpec nterm=1"}.get(g.sky.modType, str(g.sky.modType)),
+            "w_term": True, "l2": "inputs larger than L2" if rows * (5 + 3 * g.nstok * g.channels) * 4 > 126e6
+            else "inputs smaller than L2: L2 flushed between steps",
             "kernel": kernel}
 
 
@@ -433,11 +496,12 @@ def main():
     from obit_b200 import uvdata as U
     from obit_b200.skymodel import GPUSkyModel, SkyModelParams
 
-    uvw, fa, freq, sky = workload_geometry(rank, args.rows, args.ncomp)
+    g = workload_geometry(args.workload, rank, args.rows, args.ncomp)
+    uvw, fa, freq, sky = g.uvw, g.fa, g.freq, g.sky
     if world > 1:  # replicate the component table from rank 0 (one broadcast, outside timing)
         sky.comps = shard.broadcast_model(torch.from_numpy(sky.comps).to(device)).cpu().numpy()
     rows = uvw.shape[0]
-    nstok, nchan, nif = 4, 256, 4
+    nstok, nchan, nif = g.nstok, g.nchan, g.nif
     d_vis = build_vis(torch, uvw, nstok, nchan, nif, device, seed=100 + rank)
     lrec = d_vis.shape[1]
 
@@ -477,9 +541,15 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     per_launch = []
+    # records smaller than L2 (126 MB, x2 margin) would stay cached between
+    # steps: overwrite a 512 MB buffer before each step and time the launches
+    flush = torch.empty(128 << 20, dtype=torch.float32, device=device) if rows * lrec * 4 < 252e6 else None
     with sampler:
         ev0.record(stream)
         for _ in range(args.steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -491,8 +561,8 @@ def main():
     barrier()
     torch.cuda.synchronize()
     gm.check()
-    t_ms = ev0.elapsed_time(ev1)
     launch_ms = [a.elapsed_time(b) for a, b in per_launch]
+    t_ms = ev0.elapsed_time(ev1) if flush is None else sum(launch_ms)
     if world > 1:
         t_ms = shard.max_over_ranks(t_ms, device)
     value = world * evals * args.steps / (t_ms * 1e-3)
@@ -526,7 +596,7 @@ def main():
         achieved = evals * FLOPS_PER_EVAL / avg_launch_s / 1e12
         cpu = None
         if not args.no_cpu:
-            v, cores, sample, kind = cpu_baseline(uvw, fa, freq, sky, args.cpu_seconds)
+            v, cores, sample, kind = cpu_baseline(g, args.cpu_seconds)
             cpu = {"value": v / 1e9, "unit": "Gevals/s", "cores": cores, "kind": kind, "sample": sample}
         pi = gm.plan_info()
         kern = (f"{args.flavor} K={pi['K']} ct={pi['ct']} Bt={pi['Bt']} R={pi['R']} "
@@ -538,10 +608,13 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (split-FP32 phase)" if args.flavor == "recur" else "f32 (FP64 phase)",
             "data": "synthetic (seeded uvw, noise visibilities, random components)",
-            "config": config_block(args, sky, kernel=kern),
+            "config": {**config_block(g, kernel=kern),
+                       "timing": "sum of per-launch CUDA-event times, L2 flushed before each"
+                       if flush is not None else "CUDA events around all steps"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": NCU_DRAM_BYTES_PER_RECORD * rows if args.flavor == "recur" else None,
+                         "traffic": NCU_DRAM_BYTES_PER_RECORD * rows
+                         if (args.flavor == "recur" and g.name == "config2") else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record "
                                            "(10,080-record capture) x records per launch",
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
