@@ -16,7 +16,7 @@ ALL_TYPES = [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC, U.MOD_GAUSS, U.MO
 
 
 @pytest.mark.parametrize("mod", ALL_TYPES)
-@pytest.mark.parametrize("K", [16, 8])
+@pytest.mark.parametrize("K", [32, 16, 8])
 def test_model_types_recur(mod, K):
     uv, sky = small(mod, nrow=80, nchan=40, nif=2, ncomp=257)
     mx, rms = model_error(uv, sky, K=K)

@@ -70,7 +70,8 @@ def test_blocks_cover_selection_once(harness):
 
 def test_default_channels_per_thread(harness):
     assert plan(harness, nchan=256, nif=4)["K"] == 32
-    assert plan(harness, nchan=256, nif=4, kind=3, lcomp=7)["K"] == 16   # Gaussian
+    assert plan(harness, nchan=256, nif=4, kind=3, lcomp=7)["K"] == 32   # Gaussian
+    assert plan(harness, nchan=256, nif=4, kind=1, nterm=2, lcomp=6)["K"] == 16  # 2 spectral terms
     assert plan(harness, nchan=5, nif=1)["K"] == 8                       # short runs
     assert plan(harness, nchan=1, nif=1)["K"] == 2
     assert plan(harness, nchan=64, flavor=1)["K"] == 8                   # plain comparator
