@@ -406,7 +406,10 @@ def run_config5(args):
     stream = torch.cuda.Stream(device=device)
     sp = stream.cuda_stream
     t0 = time.perf_counter()
-    tuned = None if args.no_autotune else batch.autotune(sp)
+    fixed = any((args.K, args.ct, args.Bt, args.threads))
+    if fixed:  # an explicit tile shape replaces the autotuner
+        batch.set_tile(args.K, args.ct, args.Bt, args.threads)
+    tuned = None if (args.no_autotune or fixed) else batch.autotune(sp)
     torch.cuda.synchronize()
     tune_s = time.perf_counter() - t0
     info = batch.info()
