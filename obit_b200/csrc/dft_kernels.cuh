@@ -444,9 +444,28 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         const int nc = min(ct, p.ncomp - c0);
         const float df = bd.df;
         const float4* sSd = sS + bd.dfc * ct * R;
-        // components in pairs: two prologues and four rotation chains in flight
-        // (the tile is zero-filled past ncomp, so a padded partner adds zero)
-        const int ncp = min(ct, (nc + 1) & ~1);
+        // Components in pairs: two prologues and four rotation chains in flight
+        // (the tile is zero-filled past ncomp, so a padded partner adds zero).
+        // A Gaussian taper adds five packed registers per chain pair; at 32
+        // channels per thread two components' state no longer fits beside the
+        // sums, so those take one component at a time.
+        constexpr bool kPairs = !(F::kGaussian && K >= 32);
+        if constexpr (!kPairs) {
+          for (int c = 0; c < nc; c++) {
+            CompChains<H> x;
+            comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
+                                p.cstride, f0, bd.f0_hi, df);
+            const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
+#pragma unroll
+            for (int jj = 0; jj < Q; jj++) {
+              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, Gx + jj, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
+                               x.NSI);
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, Gx + jj + Q, x.GGb, x.HHb, x.QQ,
+                               x.SR, x.SI, x.NSI);
+            }
+          }
+        }
+        const int ncp = kPairs ? min(ct, (nc + 1) & ~1) : 0;
         for (int c = 0; c < ncp; c += 2) {
           CompChains<H> x, y;
           comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
