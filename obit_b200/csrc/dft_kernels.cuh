@@ -15,7 +15,9 @@
 //                               step s = exp(2 pi i P df) (accurate sin/cos) and
 //                               s^(K/2); the Gaussian form g1 u^2 + g2 v^2 + g3 u v.
 //   (component, block, channel) spectral amplitude A exp(E(k)) with E fitted as a
-//                               quadratic in k over the block (row-independent).
+//                               quadratic in k over the block (row-independent;
+//                               point families -- Gaussian families carry taper
+//                               and spectrum in one per-row amplitude recurrence).
 //   (row, component, block)     anchor exp(2 pi i P f0) from the range-reduced
 //                               split-FP32 product (MUFU sin/cos).
 //   (row, component, channel)   two packed recurrences z <- z * s over the block's
@@ -40,7 +42,10 @@ struct Fields {
   static constexpr bool kGaussian = (MODE == kGauss || MODE == kGaussSpec || MODE == kGaussTSpec);
   static constexpr bool kSpec = (MODE == kPointSpec || MODE == kGaussSpec);
   static constexpr bool kTSpec = (MODE == kPointTSpec || MODE == kGaussTSpec);
-  static constexpr bool kTable = kSpec || kTSpec;  // row-independent amplitude table
+  // Point families with a spectrum read a row-independent amplitude table;
+  // Gaussian families fold the spectral exponent into the per-row taper
+  // recurrence (both are exp of a quadratic in the channel index).
+  static constexpr bool kTable = (kSpec || kTSpec) && !kGaussian;
   static constexpr bool kQuad = (MODE != kPoint);
   static constexpr int kSpecOff = (MODE == kPointSpec) ? 4 : 7;   // first spectral coefficient
   static constexpr int kAlphaOff = (MODE == kPointTSpec) ? 4 : 7; // TSpec spectral index
@@ -209,8 +214,9 @@ __device__ __forceinline__ void load_uvw(const KParams& p, float* sUVW, int row0
 }
 
 // One channel step of a packed chain (two channels k and k + H): accumulate the
-// model term, then advance the phasor by the unit step s (and the Gaussian
-// taper by its ratio).  g points at the pair's spectral amplitudes.
+// model term, then advance the phasor by the unit step s (and a Gaussian
+// amplitude -- taper times spectrum -- by its ratio).  g points at the pair's
+// spectral amplitudes (point families with a spectrum).
 template <int MODE>
 __device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, const f2x* g, f2x& gg,
                                            f2x& hh, const f2x qq, const f2x sr, const f2x si,
@@ -219,15 +225,9 @@ __device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, c
   if constexpr (MODE == kPoint) {
     ar = add2(ar, zr);
     ai = add2(ai, zi);
-  } else if constexpr (MODE == kGauss) {
+  } else if constexpr (F::kGaussian) {
     ar = fma2(gg, zr, ar);
     ai = fma2(gg, zi, ai);
-    gg = mul2(gg, hh);
-    hh = mul2(hh, qq);
-  } else if constexpr (F::kGaussian) {  // Gaussian with spectrum
-    const f2x t = mul2(gg, *g);
-    ar = fma2(t, zr, ar);
-    ai = fma2(t, zi, ai);
     gg = mul2(gg, hh);
     hh = mul2(hh, qq);
   } else {  // spectral table
@@ -254,12 +254,15 @@ struct CompChains {
 
 // Per (row, component, block) prologue: anchor phasor at the block's first
 // channel from the split-FP32 phase, the chain starts z0, z_Q, z_H, z_(Q+H)
-// (complex products with s^Q), and the Gaussian taper exp(Q (f0 + k df)^2) at
-// the chain starts with its ratios.
+// (complex products with s^Q), and for Gaussian families the amplitude
+// A exp(Q (f0 + k df)^2 + E_spec(k)) -- taper and spectrum, one exponential
+// quadratic in the channel index k -- at the chain starts with its ratios.
 template <int MODE, int H>
 __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, float4 st,
                                            const float* sQ, int qidx, const float* sComp,
-                                           int cstride, ds f0, float f0hi, float df) {
+                                           int cstride, ds f0, const BlockDesc& bd, float df,
+                                           int nterm) {
+  const float f0hi = bd.f0_hi;
   using F = Fields<MODE>;
   constexpr int Q = H / 2;
   float2 z0 = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
@@ -289,11 +292,28 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
   x.GGa = x.HHa = x.GGb = x.HHb = x.QQ = 0ull;
   if constexpr (F::kGaussian) {
     const float Qf = sQ[qidx];
-    const float e0 = Qf * f0hi * f0hi;
-    const float e1 = 2.0f * Qf * f0hi * df;
-    const float e2 = Qf * df * df;
-    float A = 1.0f;
-    if constexpr (MODE == kGauss) A = sComp[c * cstride];
+    float e0 = Qf * f0hi * f0hi;
+    float e1 = 2.0f * Qf * f0hi * df;
+    float e2 = Qf * df * df;
+    const float* cp = sComp + c * cstride;
+    float A = cp[0];
+    if constexpr (F::kSpec) {  // exp(sum_t a_t L^(t+1)), L^(t+1) fitted over the block
+#pragma unroll
+      for (int t = 0; t < kMaxNTerm; t++) {
+        if (t < nterm) {
+          const float a = cp[F::kSpecOff + t];
+          e0 = __fmaf_rn(a, bd.l[t][0], e0);
+          e1 = __fmaf_rn(a, bd.l[t][1], e1);
+          e2 = __fmaf_rn(a, bd.l[t][2], e2);
+        }
+      }
+    } else if constexpr (F::kTSpec) {  // plane flux x exp(alpha ln(nu / nu_plane))
+      A = cp[F::kTabOff + bd.plane];
+      const float al = cp[F::kAlphaOff];
+      e0 = __fmaf_rn(al, bd.l[0][0], e0);
+      e1 = __fmaf_rn(al, bd.l[0][1], e1);
+      e2 = __fmaf_rn(al, bd.l[0][2], e2);
+    }
     auto E = [&](float k) { return A * exp_fast(__fmaf_rn(k, __fmaf_rn(k, e2, e1), e0)); };
     auto D = [&](float k) { return exp_fast(__fmaf_rn(e2, 2.0f * k + 1.0f, e1)); };
     const float fh = (float)H, fq = (float)Q;
@@ -454,7 +474,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           for (int c = 0; c < nc; c++) {
             CompChains<H> x;
             comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
-                                p.cstride, f0, bd.f0_hi, df);
+                                p.cstride, f0, bd, df, p.nterm);
             const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
 #pragma unroll
             for (int jj = 0; jj < Q; jj++) {
@@ -469,9 +489,9 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         for (int c = 0; c < ncp; c += 2) {
           CompChains<H> x, y;
           comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
-                              f0, bd.f0_hi, df);
+                              f0, bd, df, p.nterm);
           comp_setup<MODE, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
-                              (c + 1) * R + tr, sComp, p.cstride, f0, bd.f0_hi, df);
+                              (c + 1) * R + tr, sComp, p.cstride, f0, bd, df, p.nterm);
           const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
           const f2x* Gy = Gx + Bt * (H + 1);
 #pragma unroll

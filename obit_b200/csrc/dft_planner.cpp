@@ -236,8 +236,9 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   kp.nterm = M.nterm;
   kp.nspec = M.nspec;
   const bool gauss = (M.kind == kGauss || M.kind == kGaussSpec || M.kind == kGaussTSpec);
-  const bool table = (M.kind == kPointSpec || M.kind == kGaussSpec || M.kind == kPointTSpec ||
-                      M.kind == kGaussTSpec);
+  // spectral amplitude table: point families with a spectrum (Gaussian
+  // families fold the spectrum into their per-row amplitude recurrence)
+  const bool table = (M.kind == kPointSpec || M.kind == kPointTSpec);
   // shrink the component tile until the CTAs that the register budget lets
   // share an SM also fit its shared memory (32-channel recurrences run one
   // 256-thread CTA per SM)
