@@ -325,7 +325,7 @@ extern "C" int obit_dft_batch_set_tile(ObitDFTBatch* b, int K, int ct, int Bt, i
   drop_graph(b);
   for (Group& g : b->groups) {
     g.tune.K = K;
-    g.tune.ct = ct ? ct : 64;
+    g.tune.ct = ct ? ct : TuneDesc().ct;
     g.tune.Bt = Bt;
     g.tune.threads = threads ? threads : 256;
     free_group(g);
@@ -437,7 +437,7 @@ extern "C" int obit_dft_batch_autotune(ObitDFTBatch* b, void* stream, int* best)
     for (int K : {16, 32})
       for (int threads : {256, 128})
         for (int Bt = 1; Bt <= kMaxBt && threads / Bt >= 8; Bt *= 2)
-          for (int ct : {32, 64})
+          for (int ct : {64, 128})
             if (Bt >= 4) cands.push_back({K, threads, Bt, ct});
     double bestRate = -1.0;
     TuneDesc bestT = g.tune;

@@ -44,7 +44,7 @@ struct ApplyDesc {
 struct TuneDesc {
   int flavor = kFlavorRecur;
   int K = 0;    // channels per thread; 0 = chosen by the planner
-  int ct = 64;  // components per shared-memory tile
+  int ct = 128;  // components per shared-memory tile (shrunk to fit shared memory)
   int Bt = 0;   // blocks per tile (power of two); 0 = chosen by the planner
   int threads = 256;  // CTA size, 128 or 256
 };
