@@ -215,10 +215,10 @@ __device__ __forceinline__ void load_uvw(const KParams& p, float* sUVW, int row0
 
 // One channel step of a packed chain (two channels k and k + H): accumulate the
 // model term, then advance the phasor by the unit step s (and a Gaussian
-// amplitude -- taper times spectrum -- by its ratio).  g points at the pair's
-// spectral amplitudes (point families with a spectrum).
+// amplitude -- taper times spectrum -- by its ratio).  g is the pair's spectral
+// amplitudes (point families with a spectrum).
 template <int MODE>
-__device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, const f2x* g, f2x& gg,
+__device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, const f2x g, f2x& gg,
                                            f2x& hh, const f2x qq, const f2x sr, const f2x si,
                                            const f2x nsi) {
   using F = Fields<MODE>;
@@ -231,7 +231,7 @@ __device__ __forceinline__ void chain_step(f2x& ar, f2x& ai, f2x& zr, f2x& zi, c
     gg = mul2(gg, hh);
     hh = mul2(hh, qq);
   } else {  // spectral table
-    const f2x gv = *g;
+    const f2x gv = g;
     ar = fma2(gv, zr, ar);
     ai = fma2(gv, zi, ai);
   }
@@ -360,6 +360,10 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   constexpr int lgH = (H >= 16) ? 4 : (H >= 8) ? 3 : (H >= 4) ? 2 : (H >= 2) ? 1 : 0;
   static_assert((1 << lgH) == H, "K/2 must be a power of two");
   constexpr int Q = H / 2;  // offset of the second packed chain
+  // spectral table entries per (component, block) row: 16-byte entries
+  // {pair e, pair e + QE} (QE = max(Q, 1)), plus one of padding
+  constexpr int QE = (Q > 0 ? Q : 1);
+  constexpr int TE = QE + 1;
   const int tr = threadIdx.x & (R - 1);  // row within the tile
   const int tb = threadIdx.x >> lgR;     // block within the tile
 
@@ -443,12 +447,14 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           f2x RP = pk2(exp_fast(e1 + e2), exp_fast(e1 + e2 * (2.0f * fh + 1.0f)));
           const float q = exp_fast(2.0f * e2);
           const f2x QQ = pk2(q, q);
-          // layout [component][block][pair j] with an odd row stride of H + 1
-          // pairs: consecutive threads store to distinct bank pairs
-          f2x* out = reinterpret_cast<f2x*>(sG) + (c * Bt + b) * (H + 1);
+          // layout [component][block][entry e], entry e = {pair e, pair e + QE}:
+          // one 128-bit load feeds a step of both chains; the padded row of
+          // QE + 1 entries puts the 128-bit rows of consecutive threads on
+          // distinct banks
+          f2x* out = reinterpret_cast<f2x*>(sG) + (c * Bt + b) * (2 * TE);
 #pragma unroll
           for (int j = 0; j < H; j++) {
-            out[j] = GP;
+            out[j < QE ? 2 * j : 2 * (j - QE) + 1] = GP;
             GP = mul2(GP, RP);
             RP = mul2(RP, QQ);
           }
@@ -470,17 +476,25 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         // channels per thread two components' state no longer fits beside the
         // sums, so those take one component at a time.
         constexpr bool kPairs = !(F::kGaussian && K >= 32);
+        auto table = [&](int c) {
+          return reinterpret_cast<const ulonglong2*>(sG) + (c * Bt + tb) * TE;
+        };
+        auto entry = [&](const ulonglong2* G, int jj) {
+          if constexpr (F::kTable) return G[jj];
+          else return make_ulonglong2(0ull, 0ull);
+        };
         if constexpr (!kPairs) {
           for (int c = 0; c < nc; c++) {
             CompChains<H> x;
             comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
                                 p.cstride, f0, bd, df, p.nterm);
-            const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
+            const ulonglong2* Gx = table(c);
 #pragma unroll
             for (int jj = 0; jj < Q; jj++) {
-              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, Gx + jj, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
+              const ulonglong2 gx = entry(Gx, jj);
+              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
                                x.NSI);
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, Gx + jj + Q, x.GGb, x.HHb, x.QQ,
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
                                x.SR, x.SI, x.NSI);
             }
           }
@@ -492,16 +506,17 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
                               f0, bd, df, p.nterm);
           comp_setup<MODE, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
                               (c + 1) * R + tr, sComp, p.cstride, f0, bd, df, p.nterm);
-          const f2x* Gx = reinterpret_cast<const f2x*>(sG) + (c * Bt + tb) * (H + 1);
-          const f2x* Gy = Gx + Bt * (H + 1);
+          const ulonglong2* Gx = table(c);
+          const ulonglong2* Gy = table(c + 1);
 #pragma unroll
-          for (int jj = 0; jj < (Q > 0 ? Q : 1); jj++) {
-            chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, Gx + jj, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
-            chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, Gy + jj, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
+          for (int jj = 0; jj < QE; jj++) {
+            const ulonglong2 gx = entry(Gx, jj), gy = entry(Gy, jj);
+            chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
+            chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, gy.x, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
             if constexpr (Q > 0) {
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, Gx + jj + Q, x.GGb, x.HHb, x.QQ,
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
                                x.SR, x.SI, x.NSI);
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, Gy + jj + Q, y.GGb, y.HHb, y.QQ,
+              chain_step<MODE>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, gy.y, y.GGb, y.HHb, y.QQ,
                                y.SR, y.SI, y.NSI);
             }
           }

@@ -101,7 +101,10 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   std::vector<double> dfs;
   auto df_class = [&](double d) -> int {
     for (size_t i = 0; i < dfs.size(); i++)
-      if (std::fabs(dfs[i] - d) <= 1e-15 * std::fabs(d)) return (int)i;
+      // increments that differ only by the rounding of the FP64 frequency
+      // table share a class (one step phasor per class and row-component):
+      // 1e-12 of df changes a step by < 1e-9 turns at 3e6-turn phases
+      if (std::fabs(dfs[i] - d) <= 1e-12 * std::fabs(d)) return (int)i;
     dfs.push_back(d);
     return (int)dfs.size() - 1;
   };
@@ -145,8 +148,8 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
         int len = std::min(K, end - c0 + 1);
         const int ifq0 = c0 * L.kincf + iIF * L.kincif;
         const double f0 = L.fscale[ifq0];
-        double df = 0.0;
-        if (len > 1) df = L.fscale[ifq0 + L.kincf] - f0;
+        double df = 0.0;  // mean increment over the block
+        if (len > 1) df = (L.fscale[ifq0 + (len - 1) * L.kincf] - f0) / (len - 1);
         // a block is usable only if its frequencies advance uniformly
         double dev = 0.0;
         for (int k = 2; k < len; k++)

@@ -84,7 +84,8 @@ struct BatchParams {
 //   P      : ct * R float2            (phase turns, split-FP32)
 //   S      : ndf * ct * R float4      (step s and s^(K/4))
 //   Q      : ct * R floats            (Gaussian form, Gaussian models)
-//   G      : ct * Bt * (K + 2) floats (spectral amplitudes, spectral models)
+//   G      : ct * Bt * 4 * (max(K/4, 1) + 1) floats (spectral amplitudes, point
+//            families with a spectrum: 16-byte entries, one padding entry per row)
 // The model stage of the epilogue (R * Bt * K float2) reuses the same space.
 //--------------------------------------------------------------------------
 OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf, bool gauss,
@@ -92,7 +93,7 @@ OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride
   size_t n = (size_t)ct * cstride + (size_t)((R * 3 + 3) & ~3) +
              (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
   if (gauss) n += (size_t)ct * R;
-  if (table) n += (size_t)ct * Bt * (K + 2);  // rows of K/2 + 1 float pairs
+  if (table) n += (size_t)ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1);
   return n;
 }
 OBIT_HD inline size_t smem_floats_stage(int R, int Bt, int K) { return (size_t)R * Bt * K * 2; }
