@@ -391,15 +391,21 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
       if (!stage_comps(p, sComp, c0, bar, phase)) return false;
       __syncthreads();
 
-      // (row, component): phase turns, steps, Gaussian form
-      for (int idx = threadIdx.x; idx < ct * R; idx += blockDim.x) {
-        const int c = idx >> lgR;
-        const int r = idx & (R - 1);
-        const float* cp = sComp + c * p.cstride;
-        const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-        const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
-        sP[idx] = make_float2(P.hi, P.lo);
-        for (int d = 0; d < p.ndf; d++) {
+      // (row, component): phase turns, steps, Gaussian form.  Items are taken
+      // two at a time so their long dependent chains (split-FP32 products,
+      // accurate sin/cos) interleave.
+      {
+        auto phase_of = [&](int idx) {
+          const int c = idx >> lgR;
+          const int r = idx & (R - 1);
+          const float* cp = sComp + c * p.cstride;
+          const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
+          const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
+          sP[idx] = make_float2(P.hi, P.lo);
+          if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
+          return P;
+        };
+        auto step_of = [&](int idx, ds P, int d) {
           // reduced step angle: exact integer removal from the high part, the
           // low part kept for the first-order correction
           const ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
@@ -409,15 +415,30 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
           for (int m = 1; m < Q; m <<= 1) sq = cmul(sq, sq);
           sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
+        };
+        const int n = ct * R, nt = blockDim.x;
+        int idx = threadIdx.x;
+        // (Gaussian families: one item at a time -- their main loop is already
+        // at the register limit and pairs measured slower there)
+        for (; !F::kGaussian && idx + nt < n; idx += 2 * nt) {
+          const ds P0 = phase_of(idx), P1 = phase_of(idx + nt);
+          for (int d = 0; d < p.ndf; d++) {
+            step_of(idx, P0, d);
+            step_of(idx + nt, P1, d);
+          }
         }
-        if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
+        for (; idx < n; idx += nt) {
+          const ds P0 = phase_of(idx);
+          for (int d = 0; d < p.ndf; d++) step_of(idx, P0, d);
+        }
       }
       // (component, block): spectral amplitudes A exp(e0 + e1 k + e2 k^2) for the
-      // block's K channels, stored as pairs (k, k + H) so one 64-bit load feeds
-      // both halves.  Two packed amplitude recurrences g <- g r, r <- r q start
-      // from exact exponentials at k = 0 and k = H (H steps each).
+      // block's K channels (point families with a spectrum).  Two packed
+      // amplitude recurrences g <- g r, r <- r q over the pairs (k, k + H) start
+      // from exact exponentials at k = 0 and k = H (H steps each); items are
+      // taken two at a time so their recurrences interleave.
       if constexpr (F::kTable) {
-        for (int idx = threadIdx.x; idx < ct * Bt; idx += blockDim.x) {
+        auto table_row = [&](int idx) {
           const int c = idx >> lgBt;
           const int b = idx & (Bt - 1);
           const float* cp = sComp + c * p.cstride;
@@ -458,7 +479,14 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
             GP = mul2(GP, RP);
             RP = mul2(RP, QQ);
           }
+        };
+        const int n = ct * Bt, nt = blockDim.x;
+        int idx = threadIdx.x;
+        for (; idx + nt < n; idx += 2 * nt) {
+          table_row(idx);
+          table_row(idx + nt);
         }
+        if (idx < n) table_row(idx);
       }
       __syncthreads();
 
