@@ -433,10 +433,10 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         }
       }
       // (component, block): spectral amplitudes A exp(e0 + e1 k + e2 k^2) for the
-      // block's K channels (point families with a spectrum).  Two packed
-      // amplitude recurrences g <- g r, r <- r q over the pairs (k, k + H) start
-      // from exact exponentials at k = 0 and k = H (H steps each); items are
-      // taken two at a time so their recurrences interleave.
+      // block's K channels (point families with a spectrum), by packed
+      // amplitude recurrences g <- g r, r <- r q started from exact
+      // exponentials; items are taken two at a time so their recurrences
+      // interleave.
       if constexpr (F::kTable) {
         auto table_row = [&](int idx) {
           const int c = idx >> lgBt;
@@ -463,21 +463,27 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
               }
             }
           }
-          const float fh = (float)H;
-          f2x GP = pk2(A * exp_fast(e0), A * exp_fast(e0 + fh * (e1 + fh * e2)));
-          f2x RP = pk2(exp_fast(e1 + e2), exp_fast(e1 + e2 * (2.0f * fh + 1.0f)));
+          // amplitude exp(E(k)) and ratio exp(D(k)) = A(k+1) / A(k) at channel k
+          auto E = [&](float k) { return A * exp_fast(__fmaf_rn(k, __fmaf_rn(k, e2, e1), e0)); };
+          auto D = [&](float k) { return exp_fast(__fmaf_rn(e2, 2.0f * k + 1.0f, e1)); };
+          const float fh = (float)H, fe = (float)QE;
+          // layout [component][block][entry e], entry e = {pair e, pair e + QE}
+          // with pair j = channels (j, j + H): one 128-bit load feeds a step of
+          // both chains.  Two packed recurrences, one per half of the entries,
+          // fill whole entries; the padded row of QE + 1 entries puts the
+          // 128-bit stores of consecutive threads on distinct banks.
+          f2x GA = pk2(E(0.f), E(fh)), RA = pk2(D(0.f), D(fh));
+          f2x GB = pk2(E(fe), E(fe + fh)), RB = pk2(D(fe), D(fe + fh));
           const float q = exp_fast(2.0f * e2);
           const f2x QQ = pk2(q, q);
-          // layout [component][block][entry e], entry e = {pair e, pair e + QE}:
-          // one 128-bit load feeds a step of both chains; the padded row of
-          // QE + 1 entries puts the 128-bit rows of consecutive threads on
-          // distinct banks
-          f2x* out = reinterpret_cast<f2x*>(sG) + (c * Bt + b) * (2 * TE);
+          ulonglong2* out = reinterpret_cast<ulonglong2*>(sG) + (c * Bt + b) * TE;
 #pragma unroll
-          for (int j = 0; j < H; j++) {
-            out[j < QE ? 2 * j : 2 * (j - QE) + 1] = GP;
-            GP = mul2(GP, RP);
-            RP = mul2(RP, QQ);
+          for (int e = 0; e < QE; e++) {
+            out[e] = make_ulonglong2(GA, GB);
+            GA = mul2(GA, RA);
+            RA = mul2(RA, QQ);
+            GB = mul2(GB, RB);
+            RB = mul2(RB, QQ);
           }
         };
         const int n = ct * Bt, nt = blockDim.x;

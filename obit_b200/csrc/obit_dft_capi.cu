@@ -328,11 +328,14 @@ int obit_dft_calc(GPUInfo* g) {
     }
   }
   // chunk i: upload, compute and download on stream i % nbuf, so that copies of
-  // one chunk overlap the kernel of another
+  // one chunk overlap the kernel of another.  Large buffers are cut into
+  // quarter-buffer chunks: only the first upload and the last download are not
+  // hidden behind a kernel, and they shrink with the chunk.
   std::string err;
+  const int step = rowsPerBuf >= 8192 ? (rowsPerBuf + 3) / 4 : rowsPerBuf;
   int chunk = 0;
-  for (int r0 = 0; r0 < nvis; r0 += rowsPerBuf, chunk++) {
-    const int nr = std::min(rowsPerBuf, nvis - r0);
+  for (int r0 = 0; r0 < nvis; r0 += step, chunk++) {
+    const int nr = std::min(step, nvis - r0);
     const int b = chunk % nbuf;
     const size_t bytes = sizeof(float) * (size_t)nr * lenvis;
     float* host = g->h_data + (size_t)r0 * lenvis;
