@@ -75,6 +75,26 @@ class ObitDFTErr(C.Structure):
     _fields_ = [("error", C.c_int), ("prtLv", C.c_int), ("message", C.c_char * 512)]
 
 
+class ObitDFTCCField(C.Structure):
+    _fields_ = [
+        ("nrow", C.c_int), ("flux", C.POINTER(C.c_float)), ("deltaX", C.POINTER(C.c_float)),
+        ("deltaY", C.POINTER(C.c_float)), ("deltaZ", C.POINTER(C.c_float)),
+        ("parms", C.POINTER(C.c_float)), ("nparms", C.c_int), ("status", C.POINTER(C.c_int)),
+        ("startComp", C.c_int), ("endComp", C.c_int), ("crvalRA", C.c_double),
+        ("crvalDec", C.c_double), ("rotation", C.c_float), ("do3D", C.c_int),
+        ("xPxOff", C.c_float), ("yPxOff", C.c_float), ("cdeltX", C.c_float), ("cdeltY", C.c_float),
+        ("xShift", C.c_float), ("yShift", C.c_float), ("ncpProjection", C.c_int),
+    ]
+
+
+class ObitDFTCCModel(C.Structure):
+    _fields_ = [
+        ("uvRA", C.c_double), ("uvDec", C.c_double), ("uvRotation", C.c_float),
+        ("factor", C.c_float), ("minFlux", C.c_float), ("minDFT", C.c_float), ("noNeg", C.c_int),
+        ("do3D", C.c_int),
+    ]
+
+
 class ObitDFTFacet(C.Structure):
     _fields_ = [
         ("visInfo", C.POINTER(GPUVisInfo)), ("modelInfo", C.POINTER(GPUModelInfo)),
@@ -118,6 +138,10 @@ SIGNATURES = {
     "obit_dft_batch_check": (C.c_int, [C.c_void_p]),
     "obit_dft_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
     "obit_dft_batch_destroy": (C.c_int, [C.c_void_p]),
+    "obit_dft_load_comps": (C.c_int, [C.POINTER(ObitDFTCCField), C.c_int, C.POINTER(ObitDFTCCModel),
+                                      C.POINTER(C.c_float), C.c_longlong, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_last_error": (C.c_char_p, []),
     "obit_dft_version": (C.c_int, []),

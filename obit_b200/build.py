@@ -25,7 +25,7 @@ OBJ = PKG / "_build"
 CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "abi_layout.cu", "obit_dft_capi.cu",
               "obit_dft_static.cu", "dft_batch.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
-CXX_SOURCES = ["dft_planner.cpp"]
+CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -81,7 +81,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         jobs.append(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", f"-I{INCLUDE}",
                      f"-I{_cuda_include()}", "-c", str(CSRC / s), "-o", str(OBJ / (s + ".o"))])
     for s in CXX_SOURCES:
-        jobs.append(["g++", "-O2", "-fPIC", "-std=c++17", "-Wall", f"-I{INCLUDE}",
+        # no floating-point contraction: the component loader rounds where the
+        # reference's single-precision code does
+        jobs.append(["g++", "-O2", "-fPIC", "-std=c++17", "-Wall", "-ffp-contract=off", f"-I{INCLUDE}",
                      f"-I{_cuda_include()}", "-c", str(CSRC / s), "-o", str(OBJ / (s + ".o"))])
     with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
         logs = list(ex.map(lambda c: _run(c, verbose), jobs))

@@ -27,8 +27,9 @@ and then runs the FP64 oracle's divide and the metric of
 ObitUVUtilVisCompare (src/ObitUVUtil.c:1350-1506, restated in vis_compare).
 
 Only this generator reads the reference tree; the committed fixture holds a
-row subset (every STRIDE-th record) of input and master plus the component
-table and frequencies, and the full-data RMS values measured here.
+row subset (every STRIDE-th record) of input and master, the component table,
+the CC rows and image / uv geometry it came from, the frequencies, and the
+full-data RMS values measured here.
 
 Run:  python tests/golden/make_uvsub_fixture.py [path/to/ObitSystem/Obit]
 """
@@ -148,14 +149,15 @@ def read_model(path: Path, ccver: int = 2):
 
 
 def shift_sin(ra, dec, rotate, xra, xdec):
-    """ObitSkyGeomShiftSIN: FP64 direction cosines, FP32 results."""
-    maprr = F32(rotate) * F32(DG2RAD)
+    """ObitSkyGeomShiftSIN: FP64 direction cosines, FP32 results.  (The
+    reference's DG2RAD macro expands unparenthesized: rotate * pi / 180.)"""
+    maprr = F32(float(F32(rotate)) * math.pi / 180.0)
     xx = math.cos(DG2RAD * xdec) * math.sin(DG2RAD * (xra - ra))
     yy = (math.sin(DG2RAD * xdec) * math.cos(DG2RAD * dec)
           - math.cos(DG2RAD * xdec) * math.sin(DG2RAD * dec) * math.cos(DG2RAD * (xra - ra)))
     xs = F32(math.cos(maprr) * xx + math.sin(maprr) * yy)
     ys = F32(-math.sin(maprr) * xx + math.cos(maprr) * yy)
-    dz = math.sqrt(1.0 - float(xs) * float(xs) - float(ys) * float(ys))
+    dz = math.sqrt(1.0 - float(xs * xs) - float(ys * ys))  # FP32 squares
     return np.array([2.0 * math.pi * float(xs), 2.0 * math.pi * float(ys),
                      2.0 * math.pi * (dz - 1.0)], dtype=np.float32)
 
@@ -174,7 +176,18 @@ def urot3d(ra, dec, xra, xdec, mrot, urot):
     r = DG2RAD * float(F32(urot))
     ruv = np.array([[math.cos(r), -math.sin(r), 0.0], [math.sin(r), math.cos(r), 0.0],
                     [0.0, 0.0, 1.0]])
-    return (rmap @ x @ ruv).astype(np.float32)
+    # t[j][i] = sum_k x[k][i] rm[j][k]; U[j][i] = sum_k ruv[k][i] t[j][k], in
+    # the reference's summation order
+    t = [[sum_ordered(x[k][i] * rmap[j][k] for k in range(3)) for i in range(3)] for j in range(3)]
+    u = [[sum_ordered(ruv[k][i] * t[j][k] for k in range(3)) for i in range(3)] for j in range(3)]
+    return np.array(u).astype(np.float32)
+
+
+def sum_ordered(terms):
+    acc = 0.0
+    for v in terms:
+        acc += v
+    return acc
 
 
 def load_comps(cc, img, uv_axes, factor, do3D_model, nfield):
@@ -254,7 +267,13 @@ def main():
                         comps=comps, freq_arr=freq_arr,
                         axes=np.array([axes["nstok"], axes["nchan"], axes["nif"]], np.int32),
                         ref_freq=np.float64(axes["ref_freq"]),
-                        crval_stokes=np.float64(axes["crval_stokes"]))
+                        crval_stokes=np.float64(axes["crval_stokes"]),
+                        # the CC rows and geometry the component table came from
+                        cc=cc, cc_factor=np.float32(0.5), cc_nfield=np.int32(2),
+                        im_geom=np.array([img["ra"], img["dec"], img["rot"], float(img["do3D"]),
+                                          img["xPxOff"], img["yPxOff"], img["cdelt"][0],
+                                          img["cdelt"][1]], np.float64),
+                        uv_geom=np.array([axes["ra"], axes["dec"], axes["uvrot"]], np.float64))
     (HERE / "uvsub_fixture.json").write_text(json.dumps(info, indent=1) + "\n")
     print(json.dumps(info, indent=1))
 
