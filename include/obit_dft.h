@@ -295,6 +295,13 @@ int obit_dft_batch_destroy(ObitDFTBatch *batch);
  * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */
 int obit_dft_check(GPUInfo *gpuInfo);
 
+/* Diagnostic, no counterpart in the reference: polls of a component-tile copy
+ * before a kernel gives up, sets the error flag and leaves its remaining
+ * records untouched (default 4194304; a negative value restores it).  0 makes
+ * every wait give up at once, which exercises the timeout path -- the call
+ * then reports OBIT_DFT_EKERNEL and the CUDA context stays usable. */
+int obit_dft_set_wait_limit(GPUInfo *gpuInfo, int polls);
+
 /* Last error message of the calling thread ("" if none). */
 const char *obit_dft_last_error(void);
 

@@ -143,6 +143,7 @@ SIGNATURES = {
                                       C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
+    "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),
     "obit_dft_version": (C.c_int, []),
     # host mirror of the GPU sky-model class

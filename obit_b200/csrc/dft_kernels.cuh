@@ -156,7 +156,7 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
   // zero-fill the tail of the tile
   for (int i = nc * p.cstride + threadIdx.x; i < p.ct * p.cstride; i += blockDim.x) sComp[i] = 0.0f;
   uint32_t done = 0;
-  for (int it = 0; it < (1 << 22) && !done; it++) {
+  for (int it = 0; it < p.waitPolls && !done; it++) {
     asm volatile(
         "{ .reg .pred P; mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2; selp.u32 %0, 1, 0, P; }"
         : "=r"(done)

@@ -236,6 +236,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   kp.ndf = (int)dfs.size();
   for (int i = 0; i < kp.ndf; i++) split_ds(dfs[i], &kp.df_hi[i], &kp.df_lo[i]);
   kp.cstride = comp_stride(M);
+  kp.waitPolls = kDefaultWaitPolls;
   kp.nterm = M.nterm;
   kp.nspec = M.nspec;
   const bool gauss = (M.kind == kGauss || M.kind == kGaussSpec || M.kind == kGaussTSpec);

@@ -17,6 +17,7 @@ constexpr int kMaxNTerm = 4;   // spectral terms supported (ObitSkyModel nSpecTe
 constexpr int kMaxDf = 8;      // distinct channel increments per launch
 constexpr int kMaxPol = 4;
 constexpr int kMaxBt = 32;     // blocks per tile (R >= 8)
+constexpr int kDefaultWaitPolls = 1 << 22;  // bulk-copy wait before the timeout path
 
 // Model families; numbering matches GPUModType (ObitCUDASkyModelInfoDef.h:44-52).
 enum ModelKind : int {
@@ -65,6 +66,7 @@ struct KParams {
   int nspec;           // planes (tabulated spectra)
   int rowBase;         // first row index of this launch within vis
   int* errFlag;        // set non-zero on an internal error (never traps)
+  int waitPolls;       // polls of a component-tile copy before the timeout path
 };
 
 // A batched launch over many facets (one KParams each, same tile shape and

@@ -52,6 +52,7 @@ struct State {
   std::vector<float*> ownBufs;     // used when the caller supplies none
   std::vector<cudaStream_t> ownStreams;
   int* d_err = nullptr;
+  int waitPolls = kDefaultWaitPolls;  // obit_dft_set_wait_limit
 };
 
 std::mutex g_mu;
@@ -106,6 +107,7 @@ int ensure_plan(GPUInfo* g, State* s) {
   free_plan(&s->plan);
   rc = build_plan(L, s->mc.model, A, s->tune, &s->plan, &err);
   if (rc) return fail(rc, err);
+  s->plan.kp.waitPolls = s->waitPolls;
   s->planValid = true;
   return OBIT_DFT_OK;
 }
@@ -236,6 +238,16 @@ int obit_dft_set_tile(GPUInfo* g, int blocksPerTile, int threadsPerCTA) {
   s->tune.Bt = blocksPerTile;
   s->tune.threads = th;
   s->planValid = false;
+  return OBIT_DFT_OK;
+}
+
+int obit_dft_set_wait_limit(GPUInfo* g, int polls) {
+  set_last_error("");
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  s->waitPolls = polls < 0 ? kDefaultWaitPolls : polls;
+  if (s->planValid) s->plan.kp.waitPolls = s->waitPolls;
   return OBIT_DFT_OK;
 }
 
