@@ -299,7 +299,9 @@ int obit_dft_check(GPUInfo *gpuInfo);
  * before a kernel gives up, sets the error flag and leaves its remaining
  * records untouched (default 4194304; a negative value restores it).  0 makes
  * every wait give up at once, which exercises the timeout path -- the call
- * then reports OBIT_DFT_EKERNEL and the CUDA context stays usable. */
+ * then reports OBIT_DFT_EKERNEL and the CUDA context stays usable.  A lowered
+ * limit runs a separate kernel instance, available for 32-channel
+ * point+spectrum plans. */
 int obit_dft_set_wait_limit(GPUInfo *gpuInfo, int polls);
 
 /* Last error message of the calling thread ("" if none). */

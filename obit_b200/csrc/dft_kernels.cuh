@@ -133,6 +133,10 @@ __device__ __forceinline__ void apply_tile(const KParams& p, const float2* stage
 // Every thread waits on the barrier with a bounded number of polls; the return
 // value is uniform across the CTA (false: the copy did not land, the error
 // flag is set and the caller must leave the kernel).
+// kProbe (the wait-limit diagnostic instance only) takes the first wait's poll
+// count from p.waitPolls; every other instance keeps it a constant, which the
+// hot loops' register allocation is sensitive to.
+template <bool kProbe = false>
 __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int c0, uint64_t* bar,
                                             uint32_t& phase) {
   const int nc = min(p.ct, p.ncomp - c0);
@@ -156,7 +160,8 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
   // zero-fill the tail of the tile
   for (int i = nc * p.cstride + threadIdx.x; i < p.ct * p.cstride; i += blockDim.x) sComp[i] = 0.0f;
   uint32_t done = 0;
-  for (int it = 0; it < p.waitPolls && !done; it++) {
+  const int polls = kProbe ? p.waitPolls : kDefaultWaitPolls;
+  for (int it = 0; it < polls && !done; it++) {
     asm volatile(
         "{ .reg .pred P; mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2; selp.u32 %0, 1, 0, P; }"
         : "=r"(done)
@@ -337,7 +342,7 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // its bulk-copy mbarrier with the running parity in phase.  Returns false (the
 // error flag set, uniformly across the CTA) when a component copy did not land;
 // the caller must then leave the kernel.
-template <int K, int MODE>
+template <int K, int MODE, bool kProbe = false>
 __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* smem, uint64_t* bar,
                                            uint32_t& phase) {
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
@@ -388,7 +393,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // previous tile's readers are done with shared memory
-      if (!stage_comps(p, sComp, c0, bar, phase)) return false;
+      if (!stage_comps<kProbe>(p, sComp, c0, bar, phase)) return false;
       __syncthreads();
 
       // (row, component): phase turns, steps, Gaussian form.  Items are taken
@@ -589,7 +594,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   return true;
 }
 
-template <int K, int MODE>
+template <int K, int MODE, bool kProbe = false>
 __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
     dft_recur_kernel(const __grid_constant__ KParams p) {
   extern __shared__ __align__(16) float smem[];
@@ -598,7 +603,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
   uint32_t phase = 0;
   const int nItems = ((p.nvis + p.R - 1) / p.R) * p.nBlockTiles;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x)
-    if (!recur_item<K, MODE>(p, item, smem, &bar, phase)) return;
+    if (!recur_item<K, MODE, kProbe>(p, item, smem, &bar, phase)) return;
   inval_bar(&bar);
 }
 

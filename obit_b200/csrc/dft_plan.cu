@@ -40,7 +40,12 @@ KernelFn pick_plain(int mode) {
   return nullptr;
 }
 
-KernelFn pick_kernel(int flavor, int K, int mode) {
+// The wait-limit diagnostic runs its own instance (32 channels, point +
+// spectrum) so that no production instance reads the limit at run time.
+KernelFn pick_kernel(int flavor, int K, int mode, bool probe = false) {
+  if (probe)
+    return (flavor == kFlavorRecur && K == 32 && mode == kPointSpec) ? dft_recur_kernel<32, kPointSpec, true>
+                                                                     : nullptr;
   if (flavor == kFlavorRecur) {
     switch (K) {
       case 2: return pick_recur<2>(mode);
@@ -96,9 +101,11 @@ int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* 
   const int K = plan->tune.K;
   const int threads = plan->threads;
   const int nblocks = kp.nblocks;
-  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind);
+  const bool probe = kp.waitPolls != kDefaultWaitPolls;
+  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind, probe);
   if (!fn) {
-    *err = "no kernel for this flavor and channel count";
+    *err = probe ? "the wait-limit diagnostic runs 32-channel point+spectrum plans only"
+                 : "no kernel for this flavor and channel count";
     return 3;
   }
   if (int rc = raise_smem_limit((const void*)fn, plan->smemBytes, err)) return rc;
@@ -157,7 +164,12 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   kp.errFlag = d_err;
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);
-  KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind);
+  KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind,
+                            plan.kp.waitPolls != kDefaultWaitPolls);
+  if (!fn) {
+    *err = "no kernel for this plan";
+    return 3;
+  }
   // an error left by an earlier, unrelated runtime call would otherwise be
   // reported as this launch's
   cudaError_t ce = cudaGetLastError();

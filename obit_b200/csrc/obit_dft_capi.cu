@@ -105,9 +105,10 @@ int ensure_plan(GPUInfo* g, State* s) {
   if (!rc) rc = apply_from_info(s->mc, s->pr, L, &A, &err);
   if (rc) return fail(rc, err);
   free_plan(&s->plan);
-  rc = build_plan(L, s->mc.model, A, s->tune, &s->plan, &err);
+  rc = plan_layout(L, s->mc.model, A, s->tune, &s->plan, &err);
+  s->plan.kp.waitPolls = s->waitPolls;  // chooses the diagnostic instance when lowered
+  if (!rc) rc = finalize_plan(&s->plan, nullptr, 0, &err);
   if (rc) return fail(rc, err);
-  s->plan.kp.waitPolls = s->waitPolls;
   s->planValid = true;
   return OBIT_DFT_OK;
 }
@@ -247,7 +248,7 @@ int obit_dft_set_wait_limit(GPUInfo* g, int polls) {
   int rc = ensure_state(g, &s);
   if (rc) return rc;
   s->waitPolls = polls < 0 ? kDefaultWaitPolls : polls;
-  if (s->planValid) s->plan.kp.waitPolls = s->waitPolls;
+  s->planValid = false;  // re-planned (and re-finalized) at the next calc
   return OBIT_DFT_OK;
 }
 
