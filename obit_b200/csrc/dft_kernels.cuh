@@ -50,6 +50,11 @@ struct Fields {
   static constexpr int kSpecOff = (MODE == kPointSpec) ? 4 : 7;   // first spectral coefficient
   static constexpr int kAlphaOff = (MODE == kPointTSpec) ? 4 : 7; // TSpec spectral index
   static constexpr int kTabOff = (MODE == kPointTSpec) ? 5 : 8;   // TSpec first plane flux
+  // Packed chains per component: point models (unit amplitude, no per-channel
+  // factor) run one chain of K/2 steps over the pairs (j, j + K/2), which
+  // halves the chain starts of each (row, component, block); the others run
+  // two chains of K/4 steps, keeping their amplitude recurrences short.
+  static constexpr int kChains = (MODE == kPoint) ? 1 : 2;
 };
 
 // exp(x) as one MUFU.EX2 of x log2(e); flushes results below ~1e-38 to zero.
@@ -276,7 +281,13 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
     z0.x *= A;
     z0.y *= A;
   }
-  if constexpr (Q > 0) {
+  if constexpr (F::kChains == 1 || Q == 0) {
+    // one chain over (j, j + H): st.zw holds s^H
+    const float2 zh = cmul(z0, make_float2(st.z, st.w));
+    x.ZRa = pk2(z0.x, zh.x);
+    x.ZIa = pk2(z0.y, zh.y);
+    x.ZRb = x.ZIb = 0ull;
+  } else {
     const float2 sq = make_float2(st.z, st.w);
     const float2 zq = cmul(z0, sq);
     const float2 zh = cmul(zq, sq);
@@ -285,11 +296,6 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
     x.ZIa = pk2(z0.y, zh.y);
     x.ZRb = pk2(zq.x, z3.x);
     x.ZIb = pk2(zq.y, z3.y);
-  } else {
-    const float2 zh = cmul(z0, make_float2(st.x, st.y));
-    x.ZRa = pk2(z0.x, zh.x);
-    x.ZIa = pk2(z0.y, zh.y);
-    x.ZRb = x.ZIb = 0ull;
   }
   x.SR = pk2(st.x, st.x);
   x.SI = pk2(st.y, st.y);
@@ -415,10 +421,12 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           // low part kept for the first-order correction
           const ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
           const float2 s = phasor_accurate(ds{__fsub_rn(t.hi, rintf(t.hi)), t.lo});
-          // s^Q, Q = K/4: offset between the two packed chains of a block
+          // s^Q (Q = K/4), the offset between the two packed chains of a
+          // block, or s^H (H = K/2) for one-chain models
+          constexpr int SP = (F::kChains == 1 || Q == 0) ? H : Q;
           float2 sq = s;
 #pragma unroll
-          for (int m = 1; m < Q; m <<= 1) sq = cmul(sq, sq);
+          for (int m = 1; m < SP; m <<= 1) sq = cmul(sq, sq);
           sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
         };
         const int n = ct * R, nt = blockDim.x;
@@ -547,6 +555,14 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
                               (c + 1) * R + tr, sComp, p.cstride, f0, bd, df, p.nterm);
           const ulonglong2* Gx = table(c);
           const ulonglong2* Gy = table(c + 1);
+          if constexpr (F::kChains == 1) {
+#pragma unroll
+            for (int jj = 0; jj < H; jj++) {
+              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, 0ull, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
+              chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, 0ull, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
+            }
+            continue;
+          }
 #pragma unroll
           for (int jj = 0; jj < QE; jj++) {
             const ulonglong2 gx = entry(Gx, jj), gy = entry(Gy, jj);
