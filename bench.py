@@ -37,10 +37,10 @@ sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_EVAL = 10.0  # complex rotate (6) + accumulate (4), algorithmic
 # DRAM bytes (read + write) per record of the config-2 layout, from one ncu
-# capture of dft_recur_kernel<32, 1> at 10,080 records (499.93 MB read + 444.28
+# capture of dft_recur_kernel<32, 1> at 10,080 records (500.15 MB read + 446.61
 # MB written); traffic grows in proportion to records, so a launch's traffic is
 # this figure times its records.
-NCU_DRAM_BYTES_PER_RECORD = (499.93e6 + 444.28e6) / 10080
+NCU_DRAM_BYTES_PER_RECORD = (500.15e6 + 446.61e6) / 10080
 
 
 def parse():
