@@ -187,3 +187,22 @@ def test_128_thread_ctas(Bt):
     uv, sky = small(U.MOD_POINT_SPEC, nrow=70, nchan=64, nif=3, ncomp=90)
     mx, _ = model_error(uv, sky, Bt=Bt, threads=128)
     assert mx < TOL_REL
+
+
+def test_host_buffer_path_pipelines_large_buffers():
+    """40,003 records through obit_dft_calc in one call: four stream buffers of
+    10,001 records, each cut into quarter-buffer chunks with a short last one
+    (the pipelined host-buffer path), subtract with flags."""
+    uv, sky = small(U.MOD_POINT_SPEC, nrow=40003, nchan=8, nif=2, nstok=2, ncomp=40, seed=71,
+                    flag_frac=0.05)
+    mx, _ = model_error(uv, sky)
+    assert mx < TOL_REL
+    p = SkyModelParams(op=OP_SUB)
+    got = run_gpu(uv, sky, p).vis
+    want = oracle.apply_fp64(uv, sky, p)
+    _, l1 = oracle.model_fp64(uv, sky, p)
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    b = want[:, uv.nrparm:].reshape(a.shape)
+    d = np.abs((a[..., :2, 0] - b[..., :2, 0]) + 1j * (a[..., :2, 1] - b[..., :2, 1]))
+    assert np.nanmax(d / l1[..., None]) < TOL_REL + 1e-6
+    assert np.array_equal(a[..., 2], b[..., 2])
