@@ -182,7 +182,8 @@ int obit_dft_set_poln(GPUInfo *gpuInfo, int cpuRules, float stokFactor, int doFl
 int obit_dft_set_kernel(GPUInfo *gpuInfo, int flavor, int chanPerThread, int compsPerTile);
 
 /* CTA tile shape: channel blocks per tile (1, 2, 4, ..., 32; 0 = planner's
- * choice) and threads per CTA (128 or 256; 0 = 256).  Rows per tile are
+ * choice) and threads per CTA (128 or 256; 0 = planner's choice: 256, or 128
+ * when the records have at most two channel blocks).  Rows per tile are
  * threads / blocks (at least 8). */
 int obit_dft_set_tile(GPUInfo *gpuInfo, int blocksPerTile, int threadsPerCTA);
 

@@ -23,6 +23,11 @@
 //   (row, component, channel)   two packed recurrences z <- z * s over the block's
 //                               halves k and k + K/2 (one f32x2 complex multiply
 //                               advances both) and the packed accumulate.
+//                               Point models (constant amplitude) factor channel
+//                               k = 8a + b instead: G_b = A z0 s^b by a short
+//                               packed chain, H_a = s^(8a) from the (row,
+//                               component) level, and one packed complex
+//                               multiply-accumulate G_b H_a per pair of channels.
 // Component partial sums are plain FP32 within a tile and folded into a
 // compensated (Kahan) total at each tile boundary.
 #pragma once
@@ -354,6 +359,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
   constexpr int H = K / 2;
   using F = Fields<MODE>;
+  constexpr bool kFact = point_factored(MODE, K);
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
@@ -361,8 +367,10 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   BlockDesc* sBlk = reinterpret_cast<BlockDesc*>(sUVW + ((R * 3 + 3) & ~3));
   float2* sP = reinterpret_cast<float2*>(sBlk + Bt);
   float4* sS = reinterpret_cast<float4*>(sP + ct * R);
-  float* sQ = reinterpret_cast<float*>(sS + p.ndf * ct * R);
+  float2* sT = reinterpret_cast<float2*>(sS + p.ndf * ct * R);
+  float* sQ = reinterpret_cast<float*>(sT + (kFact ? p.ndf * ct * R : 0));
   float* sG = sQ + (F::kGaussian ? ct * R : 0);
+  f2x* sCmp = reinterpret_cast<f2x*>(sG + (F::kTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
   float2* stage = reinterpret_cast<float2*>(smem);
 
   // R and Bt are powers of two (R * Bt == CTA size)
@@ -386,6 +394,10 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
     const int nblkTile = min(Bt, p.nblocks - blk0);
     __syncthreads();  // the previous item's epilogue is done with the stage
 
+    if constexpr (kFact) {  // this thread's compensation terms start at zero
+#pragma unroll
+      for (int j = 0; j < 2 * H; j++) sCmp[j * blockDim.x + threadIdx.x] = 0ull;
+    }
     load_uvw(p, sUVW, row0);
     for (int i = threadIdx.x; i < Bt; i += blockDim.x) sBlk[i] = p.blocks[blk0 + min(i, nblkTile - 1)];
     __syncthreads();
@@ -422,12 +434,14 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           const ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
           const float2 s = phasor_accurate(ds{__fsub_rn(t.hi, rintf(t.hi)), t.lo});
           // s^Q (Q = K/4), the offset between the two packed chains of a
-          // block, or s^H (H = K/2) for one-chain models
-          constexpr int SP = (F::kChains == 1 || Q == 0) ? H : Q;
+          // block, or s^H (H = K/2) for one-chain models; factored point
+          // models: s^4 and s^8
+          constexpr int SP = kFact ? 4 : (F::kChains == 1 || Q == 0) ? H : Q;
           float2 sq = s;
 #pragma unroll
           for (int m = 1; m < SP; m <<= 1) sq = cmul(sq, sq);
           sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
+          if constexpr (kFact) sT[d * ct * R + idx] = cmul(sq, sq);
         };
         const int n = ct * R, nt = blockDim.x;
         int idx = threadIdx.x;
@@ -513,7 +527,69 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
       for (int j = 0; j < H; j++) AR[j] = AI[j] = 0ull;
 
-      if (mine) {
+      if (kFact && mine) {
+        // Factored point model: pair m = 4a + b holds channels (8a + b, 8a + b + 4).
+        // G pairs (G_b, G_b+4) = A z0 (s^b, s^(b+4)) by a packed chain of three
+        // steps; H_a = s^(8a) from the (row, component) prepass; then one packed
+        // complex multiply-accumulate per pair of evaluations (a = 0: add).
+        const int nc = min(ct, p.ncomp - c0);
+        const float4* sSd = sS + bd.dfc * ct * R;
+        const float2* sTd = sT + bd.dfc * ct * R;
+        // anchor A exp(2 pi i P f0) of component c, one component ahead of
+        // the multiply-accumulates so that its latency (shared loads,
+        // split-FP32 product, MUFU) overlaps them; the tile is zero-filled to
+        // ct components, so the look-ahead index is clamped to the tile
+        auto anchor = [&](int c, float2& g, float4& st, float2& s8) {
+          const int i = c * R + tr;
+          const float2 Pp = sP[i];
+          st = sSd[i];
+          s8 = sTd[i];
+          g = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
+          const float A = sComp[c * p.cstride];
+          g.x *= A;
+          g.y *= A;
+        };
+        float2 gn, s8n;
+        float4 stn;
+        anchor(0, gn, stn, s8n);
+        for (int c = 0; c < nc; c++) {
+          const float2 g0 = gn, s8 = s8n;
+          const float4 st = stn;
+          anchor(min(c + 1, ct - 1), gn, stn, s8n);
+          const float2 g4 = cmul(g0, make_float2(st.z, st.w));
+          f2x GR[4], GI[4];
+          GR[0] = pk2(g0.x, g4.x);
+          GI[0] = pk2(g0.y, g4.y);
+          const f2x SR = pk2(st.x, st.x), SI = pk2(st.y, st.y), NSI = pk2(-st.y, -st.y);
+#pragma unroll
+          for (int b = 1; b < 4; b++) {
+            const f2x t1 = mul2(GI[b - 1], NSI);
+            const f2x t2 = mul2(GI[b - 1], SR);
+            GR[b] = fma2(GR[b - 1], SR, t1);
+            GI[b] = fma2(GR[b - 1], SI, t2);
+          }
+#pragma unroll
+          for (int b = 0; b < 4; b++) {
+            AR[b] = add2(AR[b], GR[b]);
+            AI[b] = add2(AI[b], GI[b]);
+          }
+          float2 h = s8;
+#pragma unroll
+          for (int a = 1; a < K / 8; a++) {
+            if (a > 1) h = cmul(h, s8);
+            const f2x HR = pk2(h.x, h.x), HI = pk2(h.y, h.y), NHI = pk2(-h.y, -h.y);
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+              const int m = 4 * a + b;
+              AR[m] = fma2(GR[b], HR, AR[m]);
+              AR[m] = fma2(GI[b], NHI, AR[m]);
+              AI[m] = fma2(GR[b], HI, AI[m]);
+              AI[m] = fma2(GI[b], HR, AI[m]);
+            }
+          }
+        }
+      }
+      if (!kFact && mine) {
         const int nc = min(ct, p.ncomp - c0);
         const float df = bd.df;
         const float4* sSd = sS + bd.dfc * ct * R;
@@ -578,6 +654,24 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         }
       }
       // compensated fold of this tile's partial sums
+      if constexpr (kFact) {  // compensation terms in shared memory
+        f2x* cmp = sCmp + threadIdx.x;
+        const int nt = blockDim.x;
+#pragma unroll
+        for (int j = 0; j < H; j++) {
+          f2x c = cmp[(2 * j) * nt];
+          f2x y = sub2(AR[j], c);
+          f2x s = add2(TR[j], y);
+          cmp[(2 * j) * nt] = sub2(sub2(s, TR[j]), y);
+          TR[j] = s;
+          c = cmp[(2 * j + 1) * nt];
+          y = sub2(AI[j], c);
+          s = add2(TI[j], y);
+          cmp[(2 * j + 1) * nt] = sub2(sub2(s, TI[j]), y);
+          TI[j] = s;
+        }
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < H; j++) {
         f2x y = sub2(AR[j], CR[j]);
@@ -600,8 +694,11 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         float ra, rb, ia, ib;
         up2(TR[j], ra, rb);
         up2(TI[j], ia, ib);
-        out[j] = make_float2(ra, ia);
-        out[j + H] = make_float2(rb, ib);
+        // pair j: channels (j, j + H), or (8a + b, 8a + b + 4) for j = 4a + b
+        const int k1 = kFact ? 8 * (j >> 2) + (j & 3) : j;
+        const int k2 = kFact ? k1 + 4 : j + H;
+        out[k1] = make_float2(ra, ia);
+        out[k2] = make_float2(rb, ib);
       }
     }
     __syncthreads();

@@ -46,7 +46,7 @@ struct TuneDesc {
   int K = 0;    // channels per thread; 0 = chosen by the planner
   int ct = 128;  // components per shared-memory tile (shrunk to fit shared memory)
   int Bt = 0;   // blocks per tile (power of two); 0 = chosen by the planner
-  int threads = 256;  // CTA size, 128 or 256
+  int threads = 0;  // CTA size, 128 or 256; 0 = chosen by the planner
 };
 
 // A compiled plan: block table on the device plus the fixed kernel fields.

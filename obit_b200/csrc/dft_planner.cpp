@@ -212,8 +212,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   // Tile shape R x Bt = threads (128 or 256), R a power of two >= 8 (warp lanes
   // are rows): the fewest idle blocks, then the most blocks sharing each row's
   // phase work.
-  const int threads = (T.threads == 128) ? 128 : kThreads;
-  {
+  auto pick_bt = [&](int threads) {
     int bestBt = 1;
     long best = 0;
     bool have = false;
@@ -228,7 +227,16 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
         bestBt = bt;
       }
     }
-    kp.Bt = bestBt;
+    return bestBt;
+  };
+  int threads = (T.threads == 128) ? 128 : kThreads;
+  kp.Bt = pick_bt(threads);
+  // Rows with at most two channel blocks: a 256-thread tile would span 128 rows,
+  // and its per-(row, component) shared arrays would cut the component tile;
+  // two 128-thread CTAs per SM keep the tile and overlap each other's barriers.
+  if (T.threads == 0 && T.flavor == kFlavorRecur && threads / kp.Bt >= 128) {
+    threads = 128;
+    kp.Bt = pick_bt(threads);
   }
   kp.R = threads / kp.Bt;
   plan->threads = threads;
@@ -243,6 +251,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   // spectral amplitude table: point families with a spectrum (Gaussian
   // families fold the spectrum into their per-row amplitude recurrence)
   const bool table = (M.kind == kPointSpec || M.kind == kPointTSpec);
+  const bool factored = (T.flavor == kFlavorRecur) && point_factored(M.kind, K);
   // shrink the component tile until the CTAs that the register budget lets
   // share an SM also fit its shared memory (32-channel recurrences run one
   // 256-thread CTA per SM)
@@ -252,7 +261,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
                                : (threads == 128 ? 52 * 1024 : 110 * 1024);
   auto need = [&](int c) {
     size_t mainf = (T.flavor == kFlavorRecur)
-                       ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table)
+                       ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored)
                        : (size_t)c * kp.cstride + (size_t)kp.R * 3;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };

@@ -78,24 +78,34 @@ struct BatchParams {
   int* counter;           // device work counter, zero at launch
 };
 
+// Point models (no per-channel amplitude factor) with K a multiple of 8 take
+// the factored recurrence: channel k = 8a + b of a block gets
+// G_b * H_a, G_b = A z0 s^b and H_a = s^(8a), so each evaluation is one
+// packed complex multiply-accumulate.
+OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == kPoint && K >= 8 && K % 8 == 0; }
+
 //--------------------------------------------------------------------------
 // Shared memory per CTA of the recurrence kernel (dynamic):
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
 //   uvw    : R * 3 floats (padded to a multiple of 4)
 //   blk    : Bt BlockDesc (this tile's channel blocks)
 //   P      : ct * R float2            (phase turns, split-FP32)
-//   S      : ndf * ct * R float4      (step s and s^(K/4))
+//   S      : ndf * ct * R float4      (step s and s^(K/4); s and s^4 when factored)
+//   T      : ndf * ct * R float2      (s^8, factored point models)
 //   Q      : ct * R floats            (Gaussian form, Gaussian models)
 //   G      : ct * Bt * 4 * (max(K/4, 1) + 1) floats (spectral amplitudes, point
 //            families with a spectrum: 16-byte entries, one padding entry per row)
+//   Cmp    : 2 * K * R * Bt floats    (Kahan compensation of the totals, factored
+//            point models: K/2 re and K/2 im pairs per thread, thread-minor)
 // The model stage of the epilogue (R * Bt * K float2) reuses the same space.
 //--------------------------------------------------------------------------
 OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf, bool gauss,
-                                       bool table) {
+                                       bool table, bool factored = false) {
   size_t n = (size_t)ct * cstride + (size_t)((R * 3 + 3) & ~3) +
              (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
   if (gauss) n += (size_t)ct * R;
   if (table) n += (size_t)ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1);
+  if (factored) n += 2 * (size_t)ndf * ct * R + 2 * (size_t)K * R * Bt;
   return n;
 }
 OBIT_HD inline size_t smem_floats_stage(int R, int Bt, int K) { return (size_t)R * Bt * K * 2; }

@@ -233,11 +233,10 @@ int obit_dft_set_tile(GPUInfo* g, int blocksPerTile, int threadsPerCTA) {
     return fail(OBIT_DFT_EBADARG, "blocks per tile must be 0 or a power of two up to 32");
   if (threadsPerCTA != 0 && threadsPerCTA != 128 && threadsPerCTA != 256)
     return fail(OBIT_DFT_EBADARG, "threads per CTA must be 128 or 256");
-  const int th = threadsPerCTA ? threadsPerCTA : 256;
-  if (blocksPerTile && th / blocksPerTile < 8)
+  if (blocksPerTile && (threadsPerCTA ? threadsPerCTA : 256) / blocksPerTile < 8)
     return fail(OBIT_DFT_EBADARG, "a tile needs at least 8 rows (threads / blocks)");
   s->tune.Bt = blocksPerTile;
-  s->tune.threads = th;
+  s->tune.threads = threadsPerCTA;
   s->planValid = false;
   return OBIT_DFT_OK;
 }
