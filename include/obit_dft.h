@@ -159,6 +159,20 @@ int obit_dft_set_mod(GPUInfo *gpuInfo);
 int obit_dft_calc(GPUInfo *gpuInfo);
 int obit_dft_shutdown(GPUInfo *gpuInfo);
 
+/* FP64 component positions (no reference counterpart; the reference's device
+ * table holds FP32 X, Y, Z, which at 1e7-radian phases -- VLBI baselines, a
+ * field far from the phase centre -- limit the phase itself to about a radian).
+ * xyz: X, Y, Z of each component in FP64, in the units of fields 1-3 of the
+ * component table (ObitSkyModel.c:1965-1982), at least as many as the model
+ * set by the last SetMod.  Fields 1-3 of the library's device copy become the
+ * nearest floats and the remainders a side table, so the split-FP32 phase
+ * carries the FP64 positions; the plain kernel adds them in FP64.  NULL drops
+ * the side table; the next SetMod drops it too.  The multi-facet batch and
+ * obit_dft_calc_noalloc take FP32 positions only.  The void form records
+ * failures for obit_dft_last_error like the four calls above. */
+int obit_dft_set_mod_d(GPUInfo *gpuInfo, const double *xyz, int ncomp);
+void ObitCUDASkyModelDFTSetModD(GPUInfo *gpuInfo, const double *xyz, int ncomp);
+
 /* FP64 frequency side table (no reference counterpart; the reference passes
  * only FP32 freqScale).  freqArr: nchan*nIF channel frequencies in Hz indexed
  * like freqScale (ObitUVDesc.freqArr, ObitUVDesc.c:506-617); uvRefFreq: the

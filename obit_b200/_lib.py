@@ -114,6 +114,7 @@ SIGNATURES = {
     "ObitCUDASkyModelDFTSetMod": (None, [_GPUINFO_P]),
     "ObitCUDASkyModelDFTCalc": (None, [_GPUINFO_P]),
     "ObitCUDASkyModelDFTShutdown": (None, [_GPUINFO_P]),
+    "ObitCUDASkyModelDFTSetModD": (None, [_GPUINFO_P, C.POINTER(C.c_double), C.c_int]),
     # level 2: status-returning API
     "obit_dft_init": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_mod": (C.c_int, [_GPUINFO_P]),
@@ -122,6 +123,7 @@ SIGNATURES = {
     "obit_dft_set_freq": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_double), C.c_int, C.c_double,
                                     C.c_double, C.POINTER(C.c_double), C.c_int]),
     "obit_dft_set_poln": (C.c_int, [_GPUINFO_P, C.c_int, C.c_float, C.c_int]),
+    "obit_dft_set_mod_d": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_double), C.c_int]),
     "obit_dft_set_kernel": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int, C.c_int]),
     "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),

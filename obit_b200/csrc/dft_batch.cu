@@ -392,56 +392,75 @@ extern "C" int obit_dft_batch_autotune(ObitDFTBatch* b, void* stream, int* best)
   CUDA_TRY(cudaSetDevice(b->device));
   cudaStream_t st = (cudaStream_t)stream;
   std::string err;
-  // row sample: about 1e11 evaluations in all, at least one 64-row tile per facet
+  // Row samples of the facets (at least one 64-row tile each), copied into
+  // scratch so the candidates leave the records alone: every candidate is timed
+  // on a sample of about 1e11 evaluations, then the three fastest again, twice
+  // each, on one four times larger, where the choice between near-equal shapes
+  // is no longer decided by timing noise and sample-sized tails.
   long long total = 0;
   for (const Facet& f : b->facets) total += (long long)f.nvis * f.evalsPerRow;
-  const double frac = total > 0 ? std::min(1.0, 1.0e11 / (double)total) : 1.0;
-  std::vector<Facet> sample(b->facets.size());
-  std::vector<size_t> off(b->facets.size());
-  size_t floats = 0;
-  for (size_t i = 0; i < b->facets.size(); i++) {
-    const Facet& f = b->facets[i];
-    Facet& s = sample[i];
-    s.mc = f.mc;
-    s.L = f.L;
-    s.A = f.A;
-    s.compOff = f.compOff;
-    s.evalsPerRow = f.evalsPerRow;
-    s.nvis = (int)std::min<long long>(f.nvis, std::max<long long>(64, (long long)std::ceil(f.nvis * frac)));
-    off[i] = floats;
-    floats += round_up((size_t)s.nvis * f.L.lrec, 64);
-  }
-  float* scratch = nullptr;
-  CUDA_TRY(cudaMalloc(&scratch, sizeof(float) * std::max<size_t>(64, floats)));
-  for (size_t i = 0; i < sample.size(); i++) {
-    sample[i].d_vis = scratch + off[i];
-    if (sample[i].nvis > 0) {
-      cudaError_t ce = cudaMemcpyAsync(sample[i].d_vis, b->facets[i].d_vis,
-                                       sizeof(float) * (size_t)sample[i].nvis * b->facets[i].L.lrec,
-                                       cudaMemcpyDeviceToDevice, st);
-      if (ce != cudaSuccess) {
-        cudaFree(scratch);
-        return fail(OBIT_DFT_ECUDA, std::string("sample copy: ") + cudaGetErrorString(ce));
+  std::vector<float*> scratches;
+  auto make_sample = [&](double evals, std::vector<Facet>* sample) -> int {
+    const double frac = total > 0 ? std::min(1.0, evals / (double)total) : 1.0;
+    sample->assign(b->facets.size(), Facet());
+    std::vector<size_t> off(b->facets.size());
+    size_t floats = 0;
+    for (size_t i = 0; i < b->facets.size(); i++) {
+      const Facet& f = b->facets[i];
+      Facet& s = (*sample)[i];
+      s.mc = f.mc;
+      s.L = f.L;
+      s.A = f.A;
+      s.compOff = f.compOff;
+      s.evalsPerRow = f.evalsPerRow;
+      s.nvis = (int)std::min<long long>(f.nvis, std::max<long long>(64, (long long)std::ceil(f.nvis * frac)));
+      off[i] = floats;
+      floats += round_up((size_t)s.nvis * f.L.lrec, 64);
+    }
+    float* scratch = nullptr;
+    cudaError_t ce = cudaMalloc(&scratch, sizeof(float) * std::max<size_t>(64, floats));
+    if (ce != cudaSuccess) return fail(OBIT_DFT_ECUDA, std::string("sample buffer: ") + cudaGetErrorString(ce));
+    scratches.push_back(scratch);
+    for (size_t i = 0; i < sample->size(); i++) {
+      Facet& s = (*sample)[i];
+      s.d_vis = scratch + off[i];
+      if (s.nvis > 0) {
+        ce = cudaMemcpyAsync(s.d_vis, b->facets[i].d_vis, sizeof(float) * (size_t)s.nvis * b->facets[i].L.lrec,
+                             cudaMemcpyDeviceToDevice, st);
+        if (ce != cudaSuccess) return fail(OBIT_DFT_ECUDA, std::string("sample copy: ") + cudaGetErrorString(ce));
       }
     }
+    return OBIT_DFT_OK;
+  };
+  auto free_samples = [&]() {
+    cudaStreamSynchronize(st);
+    for (float* p : scratches) cudaFree(p);
+    scratches.clear();
+  };
+  std::vector<Facet> small, large;
+  int rcAll = make_sample(1.0e11, &small);
+  if (!rcAll) rcAll = make_sample(4.0e11, &large);
+  if (rcAll) {
+    free_samples();
+    return rcAll;
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   int tried = 0;
-  int rcAll = 0;
   for (Group& g : b->groups) {
     if (g.order.empty()) continue;
-    struct Cand { int K, threads, Bt, ct; };
+    struct Cand { int K, threads, Bt, ct; double rate; };
     std::vector<Cand> cands;
     for (int K : {16, 32})
       for (int threads : {256, 128})
         for (int Bt = 1; Bt <= kMaxBt && threads / Bt >= 8; Bt *= 2)
           for (int ct : {64, 128})
-            if (Bt >= 4) cands.push_back({K, threads, Bt, ct});
-    double bestRate = -1.0;
-    TuneDesc bestT = g.tune;
-    for (const Cand& c : cands) {
+            if (Bt >= 4) cands.push_back({K, threads, Bt, ct, -1.0});
+    // evaluations per millisecond of the best of `reps` timed launches (after
+    // one warm-up) of a candidate on a sample; 0 if the shape does not plan,
+    // -1 on a launch failure
+    auto time_cand = [&](const Cand& c, std::vector<Facet>& sample, int reps, TuneDesc* chosen) {
       Group t;
       t.kind = g.kind;
       t.order = g.order;
@@ -451,31 +470,52 @@ extern "C" int obit_dft_batch_autotune(ObitDFTBatch* b, void* stream, int* best)
       t.tune.ct = c.ct;
       if (build_group(t, sample, b->d_comps, b->d_err, &err) || t.items <= 0) {
         free_group(t);
-        continue;  // shape not plannable for these facets
+        return 0.0;
       }
-      float ms = 0.f;
       bool ok = launch_group(t, st, &err) == 0;  // warm-up
-      ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
-      ok = ok && launch_group(t, st, &err) == 0;
-      ok = ok && cudaEventRecord(e1, st) == cudaSuccess;
-      ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
-      ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
-      if (ok && ms > 0.f) {
-        tried++;
-        const double rate = (double)t.evals / ms;
-        if (rate > bestRate) {
-          bestRate = rate;
-          bestT = t.tune;
-          bestT.K = t.K;
-          bestT.Bt = t.Bt;
-          bestT.ct = t.ct;
-          bestT.threads = t.threads;
-        }
+      float best = 0.f;
+      for (int r = 0; r < reps && ok; r++) {
+        float ms = 0.f;
+        ok = ok && cudaEventRecord(e0, st) == cudaSuccess;
+        ok = ok && launch_group(t, st, &err) == 0;
+        ok = ok && cudaEventRecord(e1, st) == cudaSuccess;
+        ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+        ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+        if (ok && ms > 0.f && (best == 0.f || ms < best)) best = ms;
+      }
+      double rate = (ok && best > 0.f) ? (double)t.evals / best : (ok ? 0.0 : -1.0);
+      if (chosen) {
+        *chosen = t.tune;
+        chosen->K = t.K;
+        chosen->Bt = t.Bt;
+        chosen->ct = t.ct;
+        chosen->threads = t.threads;
       }
       free_group(t);
-      if (!ok) {
+      return rate;
+    };
+    for (Cand& c : cands) {
+      c.rate = time_cand(c, small, 1, nullptr);
+      if (c.rate < 0) {
         rcAll = fail(OBIT_DFT_ECUDA, "autotune launch failed: " + err);
         break;
+      }
+      if (c.rate > 0) tried++;
+    }
+    if (rcAll) break;
+    std::sort(cands.begin(), cands.end(), [](const Cand& a, const Cand& c) { return a.rate > c.rate; });
+    double bestRate = -1.0;
+    TuneDesc bestT = g.tune;
+    for (size_t i = 0; i < cands.size() && i < 3 && cands[i].rate > 0; i++) {
+      TuneDesc t;
+      const double rate = time_cand(cands[i], large, 2, &t);
+      if (rate < 0) {
+        rcAll = fail(OBIT_DFT_ECUDA, "autotune launch failed: " + err);
+        break;
+      }
+      if (rate > bestRate) {
+        bestRate = rate;
+        bestT = t;
       }
     }
     if (rcAll) break;
@@ -486,8 +526,7 @@ extern "C" int obit_dft_batch_autotune(ObitDFTBatch* b, void* stream, int* best)
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaStreamSynchronize(st);
-  cudaFree(scratch);
+  free_samples();
   if (rcAll) return rcAll;
   drop_graph(b);
   int rc = ensure_built(b);

@@ -153,6 +153,9 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
   const uint32_t bytes = (uint32_t)nc * p.cstride * 4u;
   const float* src = p.comps + (size_t)c0 * p.cstride;
   const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
+  // low parts of the FP64 positions follow the tile (ct x 4 floats)
+  float* sLo = sComp + p.ct * p.cstride;
+  const uint32_t bytesLo = p.compsLo ? (uint32_t)nc * 16u : 0u;
   // Bulk copies need 16-byte aligned addresses and sizes; cstride is a multiple
   // of 4 floats and the table base is 256-byte aligned, so this always holds.
   if (threadIdx.x == 0) {
@@ -160,15 +163,24 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
     // order earlier generic-proxy accesses of this shared memory before the
     // async-proxy write of the copy
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_s), "r"(bytes)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_s),
+                 "r"(bytes + bytesLo)
                  : "memory");
     asm volatile(
         "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_s),
         "l"(src), "r"(bytes), "r"(bar_s)
         : "memory");
+    if (bytesLo) {
+      const uint32_t lo_s = (uint32_t)__cvta_generic_to_shared(sLo);
+      asm volatile(
+          "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(lo_s),
+          "l"(p.compsLo + (size_t)c0 * 4), "r"(bytesLo), "r"(bar_s)
+          : "memory");
+    }
   }
-  // zero-fill the tail of the tile
+  // zero-fill the tail of the tile (and all of the low parts without FP64 positions)
   for (int i = nc * p.cstride + threadIdx.x; i < p.ct * p.cstride; i += blockDim.x) sComp[i] = 0.0f;
+  for (int i = (p.compsLo ? nc * 4 : 0) + threadIdx.x; i < p.ct * 4; i += blockDim.x) sLo[i] = 0.0f;
   uint32_t done = 0;
   const int polls = kProbe ? p.waitPolls : kDefaultWaitPolls;
   for (int it = 0; it < polls && !done; it++) {
@@ -363,7 +375,8 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
-  float* sUVW = sComp + ct * p.cstride;
+  const float* sLo = sComp + ct * p.cstride;  // low parts of X, Y, Z (zero without FP64 positions)
+  float* sUVW = sComp + ct * p.cstride + 4 * ct;
   BlockDesc* sBlk = reinterpret_cast<BlockDesc*>(sUVW + ((R * 3 + 3) & ~3));
   float2* sP = reinterpret_cast<float2*>(sBlk + Bt);
   float4* sS = reinterpret_cast<float4*>(sP + ct * R);
@@ -423,7 +436,9 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           const int r = idx & (R - 1);
           const float* cp = sComp + c * p.cstride;
           const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-          const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
+          const float* lo = sLo + 4 * c;
+          const ds P = ds_mul(ds_dot3_lo(cp[1], lo[0], u, cp[2], lo[1], v, cp[3], lo[2], w),
+                              ds{kInv2PiHi, kInv2PiLo});
           sP[idx] = make_float2(P.hi, P.lo);
           if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
           return P;
@@ -781,7 +796,7 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
   __shared__ __align__(8) uint64_t bar;
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
-  float* sUVW = sComp + ct * p.cstride;
+  float* sUVW = sComp + ct * p.cstride + 4 * ct;  // after the tile and its low parts
   float2* stage = reinterpret_cast<float2*>(smem);
   init_bar(&bar);
   uint32_t phase = 0;
@@ -819,8 +834,14 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
         const double f0 = (double)bd.f0_hi + (double)bd.f0_lo;
         for (int c = 0; c < nc; c++) {
           const float* cp = sComp + c * p.cstride;
-          const double Pt = ((double)cp[1] * u + (double)cp[2] * v + (double)cp[3] * w) *
-                            0.15915494309189535;
+          double Pt = (double)cp[1] * u + (double)cp[2] * v + (double)cp[3] * w;
+          if (p.compsLo) {  // FP64 positions: the low parts' share of the phase
+            // (addressed from the kernel parameters, so nothing stays live in
+            // registers across the channel loop)
+            const float* lo = sComp + p.ct * p.cstride + 4 * c;
+            Pt += (double)lo[0] * u + (double)lo[1] * v + (double)lo[2] * w;
+          }
+          Pt *= 0.15915494309189535;
           float A = cp[0];
           float Qg = 0.f, al = 0.f;
           if constexpr (F::kTSpec) {

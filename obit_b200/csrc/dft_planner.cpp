@@ -257,12 +257,14 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   // 256-thread CTA per SM)
   int ct = (T.ct + 1) & ~1;  // even: the recurrence kernel takes components in pairs
   const bool oneCta = (T.flavor == kFlavorRecur && K >= 32);
-  const size_t budget = oneCta ? (threads == 128 ? 100 * 1024 : 200 * 1024)
+  // (one 256-thread or two 128-thread CTAs per SM: 228 KB of shared memory,
+  // less 1 KB reserved per CTA)
+  const size_t budget = oneCta ? (threads == 128 ? 110 * 1024 : 200 * 1024)
                                : (threads == 128 ? 52 * 1024 : 110 * 1024);
   auto need = [&](int c) {
     size_t mainf = (T.flavor == kFlavorRecur)
                        ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored)
-                       : (size_t)c * kp.cstride + (size_t)kp.R * 3;
+                       : (size_t)c * kp.cstride + 4 * (size_t)c + (size_t)kp.R * 3;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
   while (ct > 8 && need(ct) > budget) ct /= 2;

@@ -62,6 +62,8 @@ struct KParams {
   int ndf;
   float df_hi[kMaxDf], df_lo[kMaxDf];
   const float* comps;  // ncomp records of cstride floats (reference field order)
+  const float* compsLo;  // optional ncomp x 4 floats: low parts of X, Y, Z (FP64
+                         // positions; fields 1-3 of comps hold the high parts)
   int ncomp, cstride, ct, nterm;
   int nspec;           // planes (tabulated spectra)
   int rowBase;         // first row index of this launch within vis
@@ -87,6 +89,7 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 //--------------------------------------------------------------------------
 // Shared memory per CTA of the recurrence kernel (dynamic):
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
+//   lo     : ct * 4 floats (low parts of X, Y, Z; zero without FP64 positions)
 //   uvw    : R * 3 floats (padded to a multiple of 4)
 //   blk    : Bt BlockDesc (this tile's channel blocks)
 //   P      : ct * R float2            (phase turns, split-FP32)
@@ -101,7 +104,7 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 //--------------------------------------------------------------------------
 OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf, bool gauss,
                                        bool table, bool factored = false) {
-  size_t n = (size_t)ct * cstride + (size_t)((R * 3 + 3) & ~3) +
+  size_t n = (size_t)ct * cstride + 4 * (size_t)ct + (size_t)((R * 3 + 3) & ~3) +
              (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
   if (gauss) n += (size_t)ct * R;
   if (table) n += (size_t)ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1);

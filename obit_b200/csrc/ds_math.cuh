@@ -60,6 +60,22 @@ __device__ __forceinline__ ds ds_dot3(float x, float u, float y, float v, float 
   return fast_two_sum(t.hi, lo);
 }
 
+// (x + xl) u + (y + yl) v + (z + zl) w for coefficients given as float pairs
+// (x = nearest float of an FP64 value, xl = the float of the remainder): the
+// products of the low parts, at most 2^-24 of the leading terms, enter the
+// low word of the result.
+__device__ __forceinline__ ds ds_dot3_lo(float x, float xl, float u, float y, float yl, float v,
+                                         float z, float zl, float w) {
+  ds p1 = two_prod(x, u);
+  ds p2 = two_prod(y, v);
+  ds p3 = two_prod(z, w);
+  ds s = two_sum(p1.hi, p2.hi);
+  ds t = two_sum(s.hi, p3.hi);
+  float lo = __fadd_rn(__fadd_rn(__fadd_rn(p1.lo, p2.lo), __fadd_rn(p3.lo, s.lo)), t.lo);
+  lo = __fmaf_rn(xl, u, __fmaf_rn(yl, v, __fmaf_rn(zl, w, lo)));
+  return fast_two_sum(t.hi, lo);
+}
+
 // Fractional turns of the product (a.hi + a.lo) * (b.hi + b.lo) as one float in
 // [-0.5, 0.5] (up to rounding): the exact high product and its error term, the
 // cross terms, then the nearest integer removed from the high part.  Absolute

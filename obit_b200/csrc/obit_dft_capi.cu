@@ -44,6 +44,9 @@ struct State {
   float* d_comps = nullptr;
   size_t compBytes = 0;
   bool haveModel = false;
+  float* d_lo = nullptr;  // low parts of FP64 positions (obit_dft_set_mod_d)
+  size_t loBytes = 0;
+  bool haveLo = false;
   // plan
   Plan plan;
   bool planValid = false;
@@ -90,6 +93,7 @@ void release_state(State* s) {
   cudaSetDevice(s->device);
   free_plan(&s->plan);
   if (s->d_comps) cudaFree(s->d_comps);
+  if (s->d_lo) cudaFree(s->d_lo);
   if (s->d_err) cudaFree(s->d_err);
   for (float* b : s->ownBufs) cudaFree(b);
   for (cudaStream_t st : s->ownStreams) cudaStreamDestroy(st);
@@ -107,6 +111,7 @@ int ensure_plan(GPUInfo* g, State* s) {
   free_plan(&s->plan);
   rc = plan_layout(L, s->mc.model, A, s->tune, &s->plan, &err);
   s->plan.kp.waitPolls = s->waitPolls;  // chooses the diagnostic instance when lowered
+  s->plan.kp.compsLo = s->haveLo ? s->d_lo : nullptr;
   if (!rc) rc = finalize_plan(&s->plan, nullptr, 0, &err);
   if (rc) return fail(rc, err);
   s->planValid = true;
@@ -165,6 +170,53 @@ int obit_dft_set_mod(GPUInfo* g) {
   CUDA_TRY(cudaStreamSynchronize(0));
   s->mc = mc;
   s->haveModel = true;
+  s->haveLo = false;  // FP64 positions belong to the previous model
+  s->planValid = false;
+  return OBIT_DFT_OK;
+}
+
+int obit_dft_set_mod_d(GPUInfo* g, const double* xyz, int ncomp) {
+  set_last_error("");
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  if (!xyz) {  // back to the FP32 fields as they now stand
+    s->haveLo = false;
+    s->planValid = false;
+    return OBIT_DFT_OK;
+  }
+  if (!s->haveModel) return fail(OBIT_DFT_EBADARG, "no model set (call SetMod first)");
+  const ModelDesc& md = s->mc.model;
+  if (ncomp < md.ncomp)
+    return fail(OBIT_DFT_EBADARG, "FP64 positions for " + std::to_string(ncomp) + " components, the model has " +
+                                      std::to_string(md.ncomp));
+  // X, Y, Z = hi + lo: hi the nearest float (it replaces fields 1-3 of the
+  // device table), lo the float of the remainder (a side table of 4 floats per
+  // component, staged beside each component tile)
+  std::vector<float> hi(3 * (size_t)md.ncomp), lo(4 * (size_t)md.ncomp, 0.0f);
+  for (int i = 0; i < md.ncomp; i++) {
+    for (int k = 0; k < 3; k++) {
+      const double x = xyz[3 * (size_t)i + k];
+      if (!std::isfinite(x)) return fail(OBIT_DFT_EBADARG, "non-finite FP64 position");
+      const float h = (float)x;
+      hi[3 * (size_t)i + k] = h;
+      lo[4 * (size_t)i + k] = (float)(x - (double)h);
+    }
+  }
+  if (md.ncomp > 0) {
+    const size_t bytes = lo.size() * sizeof(float);
+    if (bytes > s->loBytes) {
+      if (s->d_lo) cudaFree(s->d_lo);
+      s->d_lo = nullptr;
+      s->loBytes = 0;
+      CUDA_TRY(cudaMalloc(&s->d_lo, bytes));
+      s->loBytes = bytes;
+    }
+    CUDA_TRY(cudaMemcpy(s->d_lo, lo.data(), bytes, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy2D(s->d_comps + 1, sizeof(float) * comp_stride(md), hi.data(), 3 * sizeof(float),
+                          3 * sizeof(float), (size_t)md.ncomp, cudaMemcpyHostToDevice));
+  }
+  s->haveLo = true;
   s->planValid = false;
   return OBIT_DFT_OK;
 }
@@ -388,6 +440,10 @@ void ObitCUDASkyModelDFTInit(GPUInfo* gpuInfo) {
 
 void ObitCUDASkyModelDFTSetMod(GPUInfo* gpuInfo) {
   report("ObitCUDASkyModelDFTSetMod", obit_dft_set_mod(gpuInfo));
+}
+
+void ObitCUDASkyModelDFTSetModD(GPUInfo* gpuInfo, const double* xyz, int ncomp) {
+  report("ObitCUDASkyModelDFTSetModD", obit_dft_set_mod_d(gpuInfo, xyz, ncomp));
 }
 
 void ObitCUDASkyModelDFTCalc(GPUInfo* gpuInfo) {

@@ -164,6 +164,16 @@ class GPUSkyModel:
         if blocks_per_tile or threads:
             _lib.check(self._lib.obit_dft_set_tile(self.gpuinfo, blocks_per_tile, threads))
 
+    def set_positions_fp64(self, xyz) -> None:
+        """FP64 X, Y, Z per component (ncomp x 3, the units of table fields 1-3)
+        for the phase of the model set by the last DFTSetMod; None drops them."""
+        if xyz is None:
+            _lib.check(self._lib.obit_dft_set_mod_d(self.gpuinfo, None, 0))
+            return
+        a = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        _lib.check(self._lib.obit_dft_set_mod_d(self.gpuinfo, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                                a.shape[0]))
+
     def plan_info(self) -> dict:
         """The kernel plan the next call uses (built on demand)."""
         arr = (C.c_int * 8)()

@@ -117,6 +117,7 @@ class SkyComps:
     refFreq: float = 0.0     # reference frequency of polynomial spectra, Hz
     specFreq: np.ndarray | None = None   # coarse-plane frequencies (TSpec), Hz
     specIndex: np.ndarray | None = None  # plane per (chan, IF) (TSpec)
+    xyz: np.ndarray | None = None        # FP64 X, Y, Z per component (ncomp, 3), if known
 
     @property
     def ncomp(self) -> int:
@@ -271,8 +272,10 @@ def make_comps(modType: int, n: int, rng: np.random.Generator, radius_deg: float
             cols.append(S * (f / ref_freq) ** a)
     comps = np.stack(cols, axis=1).astype(np.float32)
     # order by decreasing flux, as merged CC tables are (ObitTableCCUtil.c:1238-1361)
-    comps = comps[np.argsort(-np.abs(comps[:, 0]), kind="stable")]
-    return SkyComps(modType, np.ascontiguousarray(comps),
+    order = np.argsort(-np.abs(comps[:, 0]), kind="stable")
+    comps = comps[order]
+    xyz = np.stack([X, Y, Z], axis=1)[order]
+    return SkyComps(modType, np.ascontiguousarray(comps), xyz=np.ascontiguousarray(xyz),
                     nterm=nterm if modType in (MOD_POINT_SPEC, MOD_GAUSS_SPEC) else 0,
                     refFreq=ref_freq, specFreq=None if spec_freq is None else np.asarray(spec_freq, np.float64),
                     specIndex=None if spec_index is None else np.asarray(spec_index, np.int32))

@@ -32,6 +32,7 @@ class OracleJob(C.Structure):
         ("stokFactor", C.c_float), ("polFact", C.c_float * 4),
         ("fscale", C.POINTER(C.c_double)), ("fscale32", C.POINTER(C.c_float)),
         ("lnspec", C.POINTER(C.c_double)), ("specIndex", C.POINTER(C.c_int)),
+        ("xyz", C.POINTER(C.c_double)),
     ]
 
 
@@ -80,7 +81,7 @@ def _p(a, t):
 class Job:
     """An OracleJob plus the arrays it points into."""
 
-    def __init__(self, uv, sky, params=None, exact: bool = True):
+    def __init__(self, uv, sky, params=None, exact: bool = True, xyz=None):
         from obit_b200.skymodel import OP_DIV, OP_REPL, SkyModelParams
         p = params or SkyModelParams()
         j = OracleJob()
@@ -130,6 +131,11 @@ class Job:
             j.specIndex = _p(self.specIndex, C.c_int)
         if self.lnspec is not None:
             j.lnspec = _p(self.lnspec, C.c_double)
+        self.xyz = None
+        if xyz is not None:  # FP64 positions in place of the table's FP32 X, Y, Z
+            self.xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+            assert self.xyz.shape[0] >= j.ncomp
+            j.xyz = _p(self.xyz, C.c_double)
         self.job = j
         self.uv = uv
 
@@ -138,11 +144,12 @@ def nthreads_default() -> int:
     return max(1, len(os.sched_getaffinity(0)))
 
 
-def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None):
+def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None):
     """FP64 component sum and L1 norm per (row, IF, channel):
     returns (model complex128 (nvis, nif, nchan), l1 float64 (nvis, nif, nchan));
-    unselected entries are NaN."""
-    jb = Job(uv, sky, params, exact)
+    unselected entries are NaN.  xyz: optional (ncomp, 3) FP64 positions used
+    for the phase instead of the table's FP32 fields 1-3."""
+    jb = Job(uv, sky, params, exact, xyz)
     nfreq = uv.nchan * uv.nif
     model = np.full((uv.nvis, nfreq, 2), np.nan)
     l1 = np.full((uv.nvis, nfreq), np.nan)
@@ -156,9 +163,9 @@ def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = 
     return m, l1.reshape(uv.nvis, uv.nif, uv.nchan)
 
 
-def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None):
+def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None):
     """FP64 oracle applied to a copy of uv.vis; returns the new float32 records."""
-    jb = Job(uv, sky, params, exact)
+    jb = Job(uv, sky, params, exact, xyz)
     out = np.ascontiguousarray(uv.vis, dtype=np.float32).copy()
     rc = lib_a().oracle_apply_fp64(C.byref(jb.job), _p(out, C.c_float), nthreads or nthreads_default())
     if rc:

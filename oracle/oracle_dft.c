@@ -87,7 +87,9 @@ static void comp_sum(const OracleJob *j, const float *rec, int ifq, double *sr,
         break;
     }
     if (expo != 0.0) amp *= exp(expo);
-    const double ph = (double)c[1] * u + (double)c[2] * v + (double)c[3] * w;
+    const double *x = j->xyz ? j->xyz + 3 * (size_t)ic : NULL;
+    const double ph = x ? x[0] * u + x[1] * v + x[2] * w
+                        : (double)c[1] * u + (double)c[2] * v + (double)c[3] * w;
     accr += amp * cos(ph);
     acci += amp * sin(ph);
     accl += fabs(amp);

@@ -59,6 +59,9 @@ typedef struct OracleJob {
   const float *fscale32;  /* the FP32 desc->fscale, used by restatement B */
   const double *lnspec;   /* Spec: ln(nu/nu_model_ref); TSpec: ln(nu/nu_plane) */
   const int *specIndex;   /* TSpec: coarse plane per (channel, IF) */
+  /* optional FP64 X, Y, Z per component (3 doubles each) used for the phase in
+   * place of the FP32 fields 1-3 of the table (the FP64 oracle only) */
+  const double *xyz;
 } OracleJob;
 
 /* (A) FP64 model: for every row and selected (channel, IF) writes the raw
