@@ -76,6 +76,16 @@ int obit_dft_load_comps(const ObitDFTCCField *fields, int nfield, const ObitDFTC
                         float *table, long long capacity, int *nrowOut, int *ncomp, int *lcomp,
                         int *modType, int *nterm);
 
+/* The same, plus FP64 positions (no reference counterpart): when xyz and
+ * table are both given, xyz (3 doubles per table row) receives X,
+ * Y, Z of each component row written, computed with every step of the
+ * geometry above (field shift, rotation, 3-D re-projection) in FP64, for
+ * obit_dft_set_mod_d.  The table itself is the one obit_dft_load_comps
+ * writes. */
+int obit_dft_load_comps_d(const ObitDFTCCField *fields, int nfield, const ObitDFTCCModel *model,
+                          float *table, long long capacity, int *nrowOut, int *ncomp, int *lcomp,
+                          int *modType, int *nterm, double *xyz);
+
 #ifdef __cplusplus
 }
 #endif

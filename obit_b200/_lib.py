@@ -144,6 +144,10 @@ SIGNATURES = {
                                       C.POINTER(C.c_float), C.c_longlong, C.POINTER(C.c_int),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int)]),
+    "obit_dft_load_comps_d": (C.c_int, [C.POINTER(ObitDFTCCField), C.c_int, C.POINTER(ObitDFTCCModel),
+                                        C.POINTER(C.c_float), C.c_longlong, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),

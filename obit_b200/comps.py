@@ -83,10 +83,12 @@ def load_comps(fields: list[CCField], model: CCModel, ref_freq: float = 0.0):
     _lib.check(lib.obit_dft_load_comps(arr, len(fields), C.byref(m), None, 0, C.byref(nrow),
                                        C.byref(ncomp), C.byref(lcomp), C.byref(mtype), C.byref(nterm)))
     table = np.zeros((max(1, nrow.value), lcomp.value), np.float32)
-    _lib.check(lib.obit_dft_load_comps(arr, len(fields), C.byref(m),
-                                       table.ctypes.data_as(C.POINTER(C.c_float)), table.size,
-                                       C.byref(nrow), C.byref(ncomp), C.byref(lcomp), C.byref(mtype),
-                                       C.byref(nterm)))
+    xyz = np.zeros((table.shape[0], 3), np.float64)
+    _lib.check(lib.obit_dft_load_comps_d(arr, len(fields), C.byref(m),
+                                         table.ctypes.data_as(C.POINTER(C.c_float)), table.size,
+                                         C.byref(nrow), C.byref(ncomp), C.byref(lcomp), C.byref(mtype),
+                                         C.byref(nterm), xyz.ctypes.data_as(C.POINTER(C.c_double))))
     comps = np.ascontiguousarray(table[:ncomp.value])
-    sky = SkyComps(mtype.value, comps, nterm=nterm.value, refFreq=ref_freq)
+    sky = SkyComps(mtype.value, comps, nterm=nterm.value, refFreq=ref_freq,
+                   xyz=np.ascontiguousarray(xyz[:ncomp.value]))
     return sky, nrow.value

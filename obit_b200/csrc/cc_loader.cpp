@@ -57,10 +57,26 @@ void shift_sin(double ra, double dec, float rotate, double xra, double xdec, flo
   dxyzc[2] = (float)(2.0 * kPi * (dz - 1.0));
 }
 
+// The same shift terms with no single-precision rounding (FP64 positions).
+void shift_sin_d(double ra, double dec, float rotate, double xra, double xdec, double dxyzc[3]) {
+  const double maprr = (double)rotate * kPi / 180.0;
+  const double d2r = kPi / 180.0;
+  const double xxshft = std::cos(d2r * xdec) * std::sin(d2r * (xra - ra));
+  const double yyshft = std::sin(d2r * xdec) * std::cos(d2r * dec) -
+                        std::cos(d2r * xdec) * std::sin(d2r * dec) * std::cos(d2r * (xra - ra));
+  const double xshift = std::cos(maprr) * xxshft + std::sin(maprr) * yyshft;
+  const double yshift = -std::sin(maprr) * xxshft + std::cos(maprr) * yyshft;
+  const double dz = std::sqrt(1.0 - xshift * xshift - yshift * yshift);
+  dxyzc[0] = 2.0 * kPi * xshift;
+  dxyzc[1] = 2.0 * kPi * yshift;
+  dxyzc[2] = 2.0 * kPi * (dz - 1.0);
+}
+
 // ObitUVDescShift3DMatrix, 3-D image branch (ObitUVDesc.c:913-978): the uv
 // re-projection matrix R(map +) X R(uv -), FP64 products in the reference's
 // summation order, FP32 result.
-void urot3d(double ra, double dec, double xra, double xdec, float mrot, float urot, float U[3][3]) {
+template <typename T>
+void urot3d(double ra, double dec, double xra, double xdec, float mrot, float urot, T U[3][3]) {
   const double d2r = kPi / 180.0;
   const double sa = std::sin(d2r * (xra - ra)), ca = std::cos(d2r * (xra - ra));
   const double sd = std::sin(d2r * xdec), cd = std::cos(d2r * xdec);
@@ -96,7 +112,7 @@ void urot3d(double ra, double dec, double xra, double xdec, float mrot, float ur
     for (int j = 0; j < 3; j++) {
       double s = 0.0;
       for (int k = 0; k < 3; k++) s += rm[k][i] * t[j][k];
-      U[j][i] = (float)s;
+      U[j][i] = (T)s;
     }
 }
 
@@ -112,6 +128,13 @@ int field_type(const ObitDFTCCField& f, int start) {
 extern "C" int obit_dft_load_comps(const ObitDFTCCField* fields, int nfield, const ObitDFTCCModel* model,
                                    float* table, long long capacity, int* nrowOut, int* ncompOut,
                                    int* lcompOut, int* modTypeOut, int* ntermOut) {
+  return obit_dft_load_comps_d(fields, nfield, model, table, capacity, nrowOut, ncompOut, lcompOut,
+                               modTypeOut, ntermOut, nullptr);
+}
+
+extern "C" int obit_dft_load_comps_d(const ObitDFTCCField* fields, int nfield, const ObitDFTCCModel* model,
+                                     float* table, long long capacity, int* nrowOut, int* ncompOut,
+                                     int* lcompOut, int* modTypeOut, int* ntermOut, double* xyzOut) {
   set_last_error("");
   if (nfield < 0 || (nfield > 0 && !fields) || !model || !nrowOut || !lcompOut)
     return fail(OBIT_DFT_EBADARG, "NULL or negative argument");
@@ -220,6 +243,23 @@ extern "C" int obit_dft_load_comps(const ObitDFTCCField* fields, int nfield, con
     const float zzoff = dxyzc[2];
     float U[3][3];
     if (do3Dmul) urot3d(model->uvRA, model->uvDec, f.crvalRA, f.crvalDec, maprot, uvrot, U);
+    // FP64 positions: the same geometry with every step in double
+    double Ud[3][3], dxyzd[3], xxoffd = 0.0, yyoffd = 0.0, zzoffd = 0.0, ssd = 0.0, ccd = 1.0;
+    double xpoffd = 0.0, ypoffd = 0.0;
+    const double konstd = kPi / 180.0 * 2.0 * kPi;
+    if (xyzOut) {
+      ssd = std::sin(kPi / 180.0 * ((double)uvrot - (double)maprot));
+      ccd = std::cos(kPi / 180.0 * ((double)uvrot - (double)maprot));
+      shift_sin_d(model->uvRA, model->uvDec, maprot, f.crvalRA, f.crvalDec, dxyzd);
+      xxoffd = dxyzd[0] * ccd + dxyzd[1] * ssd;
+      yyoffd = dxyzd[1] * ccd - dxyzd[0] * ssd;
+      zzoffd = dxyzd[2];
+      if (!model->do3D) {
+        xpoffd = (double)f.xPxOff * (double)f.cdeltX;
+        ypoffd = (double)f.yPxOff * (double)f.cdeltY;
+      }
+      if (do3Dmul) urot3d(model->uvRA, model->uvDec, f.crvalRA, f.crvalDec, maprot, uvrot, Ud);
+    }
     // Gaussian terms from the first row's FWHM and PA (ObitSkyModel.c:1938-1947)
     float gp1 = 0.f, gp2 = 0.f, gp3 = 0.f;
     if (is_gauss(ftype)) {
@@ -252,6 +292,21 @@ extern "C" int obit_dft_load_comps(const ObitDFTCCField* fields, int nfield, con
       row[1] = xyz[0] + xxoff;
       row[2] = xyz[1] + yyoff;
       row[3] = xyz[2] + zzoff;
+      if (xyzOut) {
+        const double q0 = ((double)e.dx + xpoffd) * konstd;
+        const double q1 = ((double)e.dy + ypoffd) * konstd;
+        const double q2 = f.deltaZ ? (double)e.dz * konstd : 0.0;
+        double* o = xyzOut + 3 * (size_t)ncomp;
+        if (do3Dmul) {
+          o[0] = q0 * Ud[0][0] + q1 * Ud[1][0] + xxoffd;
+          o[1] = q0 * Ud[0][1] + q1 * Ud[1][1] + yyoffd;
+          o[2] = q0 * Ud[0][2] + q1 * Ud[1][2] + zzoffd;
+        } else {
+          o[0] = ccd * q0 + ssd * q1 + xxoffd;
+          o[1] = ccd * q1 - ssd * q0 + yyoffd;
+          o[2] = q2 + zzoffd;
+        }
+      }
       // type-specific terms, mixed types zero what a field lacks (ObitSkyModel.c:1990-2083)
       const int g0 = 4, s0 = is_gauss(maxType) ? 7 : 4;
       if (is_gauss(maxType) && is_gauss(ftype)) {

@@ -158,3 +158,23 @@ def test_unsupported_geometry_and_types_are_errors():
                 parms=parms)
     with pytest.raises(_lib.DFTError):
         load_comps([g], CCModel(0.0, 0.0))
+
+
+def test_fp64_positions_follow_the_table():
+    """obit_dft_load_comps_d: the same table, plus X, Y, Z with every step of
+    the geometry in FP64 -- at the phase centre exactly 2 pi dx (rad) in
+    double; for the UVSub field (0.5 deg off, 10 deg rotation, 3-D) within the
+    FP32 table's rounding of it, and not equal to it."""
+    f = CCField(np.array([1.0, 2.0], np.float32), np.array([1e-3, -2e-3], np.float32),
+                np.array([5e-4, 0.0], np.float32), 150.0, -30.0)
+    sky, _ = load_comps([f], CCModel(150.0, -30.0))
+    konst = math.pi / 180.0 * 2.0 * math.pi
+    assert np.array_equal(sky.xyz[:, 0], np.float32([-2e-3, 1e-3]).astype(np.float64) * konst)
+    assert np.array_equal(sky.xyz[:, 1], np.float32([0.0, 5e-4]).astype(np.float64) * konst)
+    assert np.all(sky.xyz[:, 2] == 0.0)
+
+    fields, model, _ = _uvsub_fields()
+    sky, _ = load_comps(fields, model)
+    d = np.abs(sky.xyz - sky.comps[:, 1:4].astype(np.float64))
+    assert np.max(d) < 1e-6 * np.max(np.abs(sky.xyz))
+    assert np.max(d) > 0.0
