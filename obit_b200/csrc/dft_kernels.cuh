@@ -146,16 +146,17 @@ __device__ __forceinline__ void apply_tile(const KParams& p, const float2* stage
 // kProbe (the wait-limit diagnostic instance only) takes the first wait's poll
 // count from p.waitPolls; every other instance keeps it a constant, which the
 // hot loops' register allocation is sensitive to.
-template <bool kProbe = false>
+// kLo (FP64 positions) instances also bring the tile's low parts of X, Y, Z
+// (4 floats per component) into sLo on the same mbarrier; the other instances
+// never touch them.
+template <bool kProbe = false, bool kLo = false>
 __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int c0, uint64_t* bar,
-                                            uint32_t& phase) {
+                                            uint32_t& phase, float* sLo = nullptr) {
   const int nc = min(p.ct, p.ncomp - c0);
   const uint32_t bytes = (uint32_t)nc * p.cstride * 4u;
   const float* src = p.comps + (size_t)c0 * p.cstride;
   const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
-  // low parts of the FP64 positions follow the tile (ct x 4 floats)
-  float* sLo = sComp + p.ct * p.cstride;
-  const uint32_t bytesLo = p.compsLo ? (uint32_t)nc * 16u : 0u;
+  const uint32_t bytesLo = kLo ? (uint32_t)nc * 16u : 0u;
   // Bulk copies need 16-byte aligned addresses and sizes; cstride is a multiple
   // of 4 floats and the table base is 256-byte aligned, so this always holds.
   if (threadIdx.x == 0) {
@@ -170,7 +171,7 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
         "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_s),
         "l"(src), "r"(bytes), "r"(bar_s)
         : "memory");
-    if (bytesLo) {
+    if (kLo && bytesLo) {
       const uint32_t lo_s = (uint32_t)__cvta_generic_to_shared(sLo);
       asm volatile(
           "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(lo_s),
@@ -178,9 +179,10 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
           : "memory");
     }
   }
-  // zero-fill the tail of the tile (and all of the low parts without FP64 positions)
+  // zero-fill the tail of the tile (and of its low parts)
   for (int i = nc * p.cstride + threadIdx.x; i < p.ct * p.cstride; i += blockDim.x) sComp[i] = 0.0f;
-  for (int i = (p.compsLo ? nc * 4 : 0) + threadIdx.x; i < p.ct * 4; i += blockDim.x) sLo[i] = 0.0f;
+  if constexpr (kLo)
+    for (int i = nc * 4 + threadIdx.x; i < p.ct * 4; i += blockDim.x) sLo[i] = 0.0f;
   uint32_t done = 0;
   const int polls = kProbe ? p.waitPolls : kDefaultWaitPolls;
   for (int it = 0; it < polls && !done; it++) {
@@ -365,7 +367,7 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // its bulk-copy mbarrier with the running parity in phase.  Returns false (the
 // error flag set, uniformly across the CTA) when a component copy did not land;
 // the caller must then leave the kernel.
-template <int K, int MODE, bool kProbe = false>
+template <int K, int MODE, bool kProbe = false, bool kLo = false>
 __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* smem, uint64_t* bar,
                                            uint32_t& phase) {
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
@@ -375,8 +377,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
-  const float* sLo = sComp + ct * p.cstride;  // low parts of X, Y, Z (zero without FP64 positions)
-  float* sUVW = sComp + ct * p.cstride + 4 * ct;
+  float* sUVW = sComp + ct * p.cstride;
   BlockDesc* sBlk = reinterpret_cast<BlockDesc*>(sUVW + ((R * 3 + 3) & ~3));
   float2* sP = reinterpret_cast<float2*>(sBlk + Bt);
   float4* sS = reinterpret_cast<float4*>(sP + ct * R);
@@ -384,6 +385,8 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   float* sQ = reinterpret_cast<float*>(sT + (kFact ? p.ndf * ct * R : 0));
   float* sG = sQ + (F::kGaussian ? ct * R : 0);
   f2x* sCmp = reinterpret_cast<f2x*>(sG + (F::kTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
+  // low parts of X, Y, Z (kLo instances), after everything else
+  float* sLo = reinterpret_cast<float*>(sCmp) + (kFact ? 2 * K * R * Bt : 0);
   float2* stage = reinterpret_cast<float2*>(smem);
 
   // R and Bt are powers of two (R * Bt == CTA size)
@@ -424,7 +427,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // previous tile's readers are done with shared memory
-      if (!stage_comps<kProbe>(p, sComp, c0, bar, phase)) return false;
+      if (!stage_comps<kProbe, kLo>(p, sComp, c0, bar, phase, sLo)) return false;
       __syncthreads();
 
       // (row, component): phase turns, steps, Gaussian form.  Items are taken
@@ -436,9 +439,13 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           const int r = idx & (R - 1);
           const float* cp = sComp + c * p.cstride;
           const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-          const float* lo = sLo + 4 * c;
-          const ds P = ds_mul(ds_dot3_lo(cp[1], lo[0], u, cp[2], lo[1], v, cp[3], lo[2], w),
-                              ds{kInv2PiHi, kInv2PiLo});
+          ds P;
+          if constexpr (kLo) {  // FP64 positions
+            const float* lo = sLo + 4 * c;
+            P = ds_mul(ds_dot3_lo(cp[1], lo[0], u, cp[2], lo[1], v, cp[3], lo[2], w), ds{kInv2PiHi, kInv2PiLo});
+          } else {
+            P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
+          }
           sP[idx] = make_float2(P.hi, P.lo);
           if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
           return P;
@@ -722,7 +729,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   return true;
 }
 
-template <int K, int MODE, bool kProbe = false>
+template <int K, int MODE, bool kProbe = false, bool kLo = false>
 __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
     dft_recur_kernel(const __grid_constant__ KParams p) {
   extern __shared__ __align__(16) float smem[];
@@ -731,7 +738,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
   uint32_t phase = 0;
   const int nItems = ((p.nvis + p.R - 1) / p.R) * p.nBlockTiles;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x)
-    if (!recur_item<K, MODE, kProbe>(p, item, smem, &bar, phase)) return;
+    if (!recur_item<K, MODE, kProbe, kLo>(p, item, smem, &bar, phase)) return;
   inval_bar(&bar);
 }
 
@@ -789,14 +796,15 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
 // component), FP32 accumulation.  Same tiling, component staging and epilogue;
 // every channel of the block evaluated independently.
 //--------------------------------------------------------------------------
-template <int K, int MODE>
+template <int K, int MODE, bool kLo = false>
 __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p) {
   using F = Fields<MODE>;
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) uint64_t bar;
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
-  float* sUVW = sComp + ct * p.cstride + 4 * ct;  // after the tile and its low parts
+  float* sUVW = sComp + ct * p.cstride;
+  float* sLo = sUVW + ((R * 3 + 3) & ~3);  // low parts of X, Y, Z (kLo instances)
   float2* stage = reinterpret_cast<float2*>(smem);
   init_bar(&bar);
   uint32_t phase = 0;
@@ -822,7 +830,7 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
     }
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();
-      if (!stage_comps(p, sComp, c0, &bar, phase)) return;
+      if (!stage_comps<false, kLo>(p, sComp, c0, &bar, phase, sLo)) return;
       __syncthreads();
       float2 acc[K];
 #pragma unroll
@@ -835,10 +843,8 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
         for (int c = 0; c < nc; c++) {
           const float* cp = sComp + c * p.cstride;
           double Pt = (double)cp[1] * u + (double)cp[2] * v + (double)cp[3] * w;
-          if (p.compsLo) {  // FP64 positions: the low parts' share of the phase
-            // (addressed from the kernel parameters, so nothing stays live in
-            // registers across the channel loop)
-            const float* lo = sComp + p.ct * p.cstride + 4 * c;
+          if constexpr (kLo) {  // FP64 positions: the low parts' share of the phase
+            const float* lo = sLo + 4 * c;
             Pt += (double)lo[0] * u + (double)lo[1] * v + (double)lo[2] * w;
           }
           Pt *= 0.15915494309189535;

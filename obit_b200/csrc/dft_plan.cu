@@ -14,56 +14,63 @@ namespace {
 
 using KernelFn = void (*)(const KParams);
 
-template <int K>
+template <int K, bool kLo>
 KernelFn pick_recur(int mode) {
   switch (mode) {
-    case kPoint: return dft_recur_kernel<K, kPoint>;
-    case kPointSpec: return dft_recur_kernel<K, kPointSpec>;
-    case kPointTSpec: return dft_recur_kernel<K, kPointTSpec>;
-    case kGauss: return dft_recur_kernel<K, kGauss>;
-    case kGaussSpec: return dft_recur_kernel<K, kGaussSpec>;
-    case kGaussTSpec: return dft_recur_kernel<K, kGaussTSpec>;
+    case kPoint: return dft_recur_kernel<K, kPoint, false, kLo>;
+    case kPointSpec: return dft_recur_kernel<K, kPointSpec, false, kLo>;
+    case kPointTSpec: return dft_recur_kernel<K, kPointTSpec, false, kLo>;
+    case kGauss: return dft_recur_kernel<K, kGauss, false, kLo>;
+    case kGaussSpec: return dft_recur_kernel<K, kGaussSpec, false, kLo>;
+    case kGaussTSpec: return dft_recur_kernel<K, kGaussTSpec, false, kLo>;
   }
   return nullptr;
 }
 
-template <int K>
+template <int K, bool kLo>
 KernelFn pick_plain(int mode) {
   switch (mode) {
-    case kPoint: return dft_plain_kernel<K, kPoint>;
-    case kPointSpec: return dft_plain_kernel<K, kPointSpec>;
-    case kPointTSpec: return dft_plain_kernel<K, kPointTSpec>;
-    case kGauss: return dft_plain_kernel<K, kGauss>;
-    case kGaussSpec: return dft_plain_kernel<K, kGaussSpec>;
-    case kGaussTSpec: return dft_plain_kernel<K, kGaussTSpec>;
+    case kPoint: return dft_plain_kernel<K, kPoint, kLo>;
+    case kPointSpec: return dft_plain_kernel<K, kPointSpec, kLo>;
+    case kPointTSpec: return dft_plain_kernel<K, kPointTSpec, kLo>;
+    case kGauss: return dft_plain_kernel<K, kGauss, kLo>;
+    case kGaussSpec: return dft_plain_kernel<K, kGaussSpec, kLo>;
+    case kGaussTSpec: return dft_plain_kernel<K, kGaussTSpec, kLo>;
+  }
+  return nullptr;
+}
+
+template <bool kLo>
+KernelFn pick_flavor(int flavor, int K, int mode) {
+  if (flavor == kFlavorRecur) {
+    switch (K) {
+      case 2: return pick_recur<2, kLo>(mode);
+      case 4: return pick_recur<4, kLo>(mode);
+      case 8: return pick_recur<8, kLo>(mode);
+      case 16: return pick_recur<16, kLo>(mode);
+      case 32: return pick_recur<32, kLo>(mode);
+    }
+  } else if (flavor == kFlavorPlain) {
+    switch (K) {
+      case 1: return pick_plain<1, kLo>(mode);
+      case 2: return pick_plain<2, kLo>(mode);
+      case 4: return pick_plain<4, kLo>(mode);
+      case 8: return pick_plain<8, kLo>(mode);
+      case 16: return pick_plain<16, kLo>(mode);
+    }
   }
   return nullptr;
 }
 
 // The wait-limit diagnostic runs its own instance (32 channels, point +
-// spectrum) so that no production instance reads the limit at run time.
-KernelFn pick_kernel(int flavor, int K, int mode, bool probe = false) {
+// spectrum) so that no production instance reads the limit at run time; FP64
+// positions (lo) select the instances that stage and add the low parts.
+KernelFn pick_kernel(int flavor, int K, int mode, bool probe, bool lo) {
   if (probe)
-    return (flavor == kFlavorRecur && K == 32 && mode == kPointSpec) ? dft_recur_kernel<32, kPointSpec, true>
-                                                                     : nullptr;
-  if (flavor == kFlavorRecur) {
-    switch (K) {
-      case 2: return pick_recur<2>(mode);
-      case 4: return pick_recur<4>(mode);
-      case 8: return pick_recur<8>(mode);
-      case 16: return pick_recur<16>(mode);
-      case 32: return pick_recur<32>(mode);
-    }
-  } else if (flavor == kFlavorPlain) {
-    switch (K) {
-      case 1: return pick_plain<1>(mode);
-      case 2: return pick_plain<2>(mode);
-      case 4: return pick_plain<4>(mode);
-      case 8: return pick_plain<8>(mode);
-      case 16: return pick_plain<16>(mode);
-    }
-  }
-  return nullptr;
+    return (flavor == kFlavorRecur && K == 32 && mode == kPointSpec && !lo)
+               ? dft_recur_kernel<32, kPointSpec, true>
+               : nullptr;
+  return lo ? pick_flavor<true>(flavor, K, mode) : pick_flavor<false>(flavor, K, mode);
 }
 
 }  // namespace
@@ -102,9 +109,9 @@ int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* 
   const int threads = plan->threads;
   const int nblocks = kp.nblocks;
   const bool probe = kp.waitPolls != kDefaultWaitPolls;
-  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind, probe);
+  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind, probe, kp.compsLo != nullptr);
   if (!fn) {
-    *err = probe ? "the wait-limit diagnostic runs 32-channel point+spectrum plans only"
+    *err = probe ? "the wait-limit diagnostic runs 32-channel point+spectrum plans without FP64 positions only"
                  : "no kernel for this flavor and channel count";
     return 3;
   }
@@ -165,7 +172,7 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);
   KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind,
-                            plan.kp.waitPolls != kDefaultWaitPolls);
+                            plan.kp.waitPolls != kDefaultWaitPolls, plan.kp.compsLo != nullptr);
   if (!fn) {
     *err = "no kernel for this plan";
     return 3;

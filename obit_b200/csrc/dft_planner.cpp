@@ -264,7 +264,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   auto need = [&](int c) {
     size_t mainf = (T.flavor == kFlavorRecur)
                        ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored)
-                       : (size_t)c * kp.cstride + 4 * (size_t)c + (size_t)kp.R * 3;
+                       : (size_t)c * kp.cstride + (size_t)((kp.R * 3 + 3) & ~3) + 4 * (size_t)c;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
   while (ct > 8 && need(ct) > budget) ct /= 2;

@@ -89,7 +89,6 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 //--------------------------------------------------------------------------
 // Shared memory per CTA of the recurrence kernel (dynamic):
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
-//   lo     : ct * 4 floats (low parts of X, Y, Z; zero without FP64 positions)
 //   uvw    : R * 3 floats (padded to a multiple of 4)
 //   blk    : Bt BlockDesc (this tile's channel blocks)
 //   P      : ct * R float2            (phase turns, split-FP32)
@@ -100,6 +99,8 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 //            families with a spectrum: 16-byte entries, one padding entry per row)
 //   Cmp    : 2 * K * R * Bt floats    (Kahan compensation of the totals, factored
 //            point models: K/2 re and K/2 im pairs per thread, thread-minor)
+//   lo     : ct * 4 floats            (low parts of X, Y, Z: instances for FP64
+//            positions; reserved in every plan so that one plan serves both)
 // The model stage of the epilogue (R * Bt * K float2) reuses the same space.
 //--------------------------------------------------------------------------
 OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf, bool gauss,
