@@ -36,11 +36,19 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_EVAL = 10.0  # complex rotate (6) + accumulate (4), algorithmic
-# DRAM bytes (read + write) per record of the config-2 layout, from one ncu
-# capture of dft_recur_kernel<32, 1> at 10,080 records (500.15 MB read + 446.61
-# MB written); traffic grows in proportion to records, so a launch's traffic is
-# this figure times its records.
-NCU_DRAM_BYTES_PER_RECORD = (500.15e6 + 446.61e6) / 10080
+# DRAM bytes (read + write) per record of a workload's records, each from one ncu
+# capture of the recurrence kernel on a smaller case of the same layout; traffic
+# grows in proportion to records, so a launch's traffic is the figure times its
+# records.
+#   config2: dft_recur_kernel<32, 1> at 10,080 records (500.15 MB read + 446.61 MB written)
+#   config4: dft_recur_kernel<32, 0> at 23,808 records (296.35 MB read + 240.85 MB written)
+#   config5: dft_recur_batch_kernel<32, 0> over the 96-facet draw at 189,029 records
+#            (rows x 0.001; 3,668.0 MB read + 3,567.0 MB written)
+NCU_DRAM_BYTES_PER_RECORD = {
+    "config2": ((500.15e6 + 446.61e6) / 10080, "10,080-record capture"),
+    "config4": ((296.35e6 + 240.85e6) / 23808, "23,808-record capture"),
+    "config5": ((3668.0e6 + 3567.0e6) / 189029, "189,029-record capture of the same facet draw"),
+}
 
 
 def parse():
@@ -462,7 +470,10 @@ def run_config5(args):
                    "launch": f"1 CUDA graph launch per step ({info['launches']} persistent kernel(s), "
                              f"grid {info['grid']})"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": NCU_DRAM_BYTES_PER_RECORD["config5"][0] * sum(f.nvis for f in facets),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record ("
+                                       + NCU_DRAM_BYTES_PER_RECORD["config5"][1] + ") x records per launch",
                      "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)"},
         "comparators": comp,
         "cpu_baseline": None, "e2e": None,
@@ -616,10 +627,11 @@ def main():
                        if flush is not None else "CUDA events around all steps"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": NCU_DRAM_BYTES_PER_RECORD * rows
-                         if (args.flavor == "recur" and g.name == "config2") else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record "
-                                           "(10,080-record capture) x records per launch",
+                         "traffic": NCU_DRAM_BYTES_PER_RECORD[g.name][0] * rows
+                         if (args.flavor == "recur" and g.name in NCU_DRAM_BYTES_PER_RECORD) else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record ("
+                                           + NCU_DRAM_BYTES_PER_RECORD.get(g.name, (0, "no capture"))[1]
+                                           + ") x records per launch",
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
                          "flops_per_eval": FLOPS_PER_EVAL},
             "cpu_baseline": cpu,

@@ -90,3 +90,25 @@ def test_side_table_must_cover_the_model():
         gm.DFTShutdown()
     finally:
         gm.close()
+
+
+ALL_TYPES = [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC, U.MOD_GAUSS, U.MOD_GAUSS_SPEC,
+             U.MOD_GAUSS_TSPEC]
+
+
+@pytest.mark.parametrize("flavor", [OBIT_DFT_RECUR, OBIT_DFT_PLAIN])
+@pytest.mark.parametrize("mt,nterm", [(m, 1) for m in ALL_TYPES] + [(U.MOD_POINT_SPEC, 2)])
+def test_fp64_position_instances_of_every_family(mt, nterm, flavor):
+    """Every model family (and the 16-channel blocks of two spectral terms)
+    through the FP64-position kernel instances: 300 km baselines at 1.4 GHz,
+    components within 3 deg, subtract with flags."""
+    from helpers import small
+    uv, sky = small(mt, nrow=40, nchan=40, nif=2, nstok=2, ncomp=160, seed=31 + mt, max_bl=3e5,
+                    radius_deg=3.0, nterm=nterm, flag_frac=0.05)
+    p = SkyModelParams(op=OP_SUB)
+    _, l1 = oracle.model_fp64(uv, sky, p, xyz=sky.xyz)
+    want = oracle.apply_fp64(uv, sky, p, xyz=sky.xyz)
+    got = _run(uv, sky, p, flavor, xyz=sky.xyz)
+    assert _err(got, want, l1, uv) < TOL_REL
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    assert np.array_equal(a[..., 2], uv.vis_view()[..., 2])  # weights untouched by subtract
