@@ -90,6 +90,9 @@ int layout_from_info(const GPUVisInfo* v, const ModelCfg& mc, const FreqSide& fs
   if (L->lrec <= 0 || L->nchan <= 0 || L->nstok <= 0)
     return bad(err, OBIT_DFT_EBADARG,
                "record length, channel and polarization counts must be positive");
+  if (L->chanb < 0 || L->chane < L->chanb || L->chane >= L->nchan || L->ifb < 0 || L->ife < L->ifb ||
+      L->ife >= L->nif || L->stokb < 0 || L->stoke < L->stokb || L->stoke >= L->nstok)
+    return bad(err, OBIT_DFT_EBADARG, "channel, IF or polarization selection outside the data");
   const int nfreq = L->nchan * L->nif;
   // every selected product must lie inside the record
   const long long lastOff = (long long)L->nrparm + (long long)L->ife * L->incif +
