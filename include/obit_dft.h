@@ -173,6 +173,42 @@ int obit_dft_shutdown(GPUInfo *gpuInfo);
 int obit_dft_set_mod_d(GPUInfo *gpuInfo, const double *xyz, int ncomp);
 void ObitCUDASkyModelDFTSetModD(GPUInfo *gpuInfo, const double *xyz, int ncomp);
 
+/* Beam-corrected DFT, Stokes I sky, linear feeds (the model of
+ * ObitCUDABeamModel's beam*Kernel family, ObitCUDABeamModel.cu:139-1226, with
+ * the Jones product of cudaJonesCor1_Lin_I, CUDALinCorSum.h:104-134).  No
+ * level-2 counterpart of this shape: the reference's ObitCUDABeamModelDFT*
+ * calls take a GPUBeamInfo of device beam-image interpolators
+ * (ObitCUDABeamModelInfoDef.h:148-275) and fill the Jones table from them on
+ * the GPU; here the caller passes the Jones table itself.  For a record of
+ * baseline (a1, a2) -- from BASELINE = 256 a1 + a2 (+ subarray fraction) or
+ * ANTENNA1 / ANTENNA2, as GetAnts (ObitCUDABeamModel.cu:82-99) -- and a
+ * (channel, IF) of Jones plane jc, component c contributes its DFT term times
+ *   XX: P(0,0) + P(1,1)   XY: P(1,3) + P(0,2)   YX: P(2,0) + P(3,1)   YY: P(2,2) + P(3,3),
+ * P(i, j) = J1[i] conj(J2[j]), J1 = jones[type(a1)][c][jc], J2 = jones[type(a2)][c][jc].
+ * The records' first correlations XX, YY (, XY, YX with four) are modelled;
+ * each one with positive weight (any, when replacing) is subtracted from,
+ * divided into (weight unchanged) or replaced by its model times stokFact of
+ * its position, independently of the others; every selected channel of every
+ * selected IF is processed.  Once set, obit_dft_calc and obit_dft_calc_device
+ * apply the beam-corrected model; NULL returns to the plain sky model; the
+ * multi-facet batch and obit_dft_calc_noalloc do not take a beam.  A record
+ * whose antennas fall outside antType is left untouched and the call reports
+ * OBIT_DFT_EKERNEL (code 3). */
+typedef struct ObitDFTBeam {
+  int numAnt;            /* antennas: records number them 1..numAnt */
+  int numAntType;        /* antenna types */
+  int numJChan;          /* Jones planes */
+  const int *antType;    /* host [numAnt]: type of each antenna, 0..numAntType-1 */
+  const int *jchan;      /* host [nchan*nIF]: Jones plane of each (channel, IF), freqScale order */
+  int ilocb;             /* BASELINE random parameter offset, or -1 */
+  int iloca1, iloca2;    /* ANTENNA1 / ANTENNA2 offsets when ilocb < 0 */
+  int stokType;          /* Stokes of the sky model: 1 = I (the only one supported) */
+  const float *jones;    /* device, 16-byte aligned: [numAntType][jonesComps][numJChan] 2x2
+                            complex matrices of 8 floats (XX, XY, YX, YY as re, im) */
+  int jonesComps;        /* components per type in jones, at least the model's */
+} ObitDFTBeam;
+int obit_dft_set_beam(GPUInfo *gpuInfo, const ObitDFTBeam *beam);
+
 /* FP64 frequency side table (no reference counterpart; the reference passes
  * only FP32 freqScale).  freqArr: nchan*nIF channel frequencies in Hz indexed
  * like freqScale (ObitUVDesc.freqArr, ObitUVDesc.c:506-617); uvRefFreq: the

@@ -105,6 +105,15 @@ class ObitDFTFacet(C.Structure):
     ]
 
 
+class ObitDFTBeam(C.Structure):
+    _fields_ = [
+        ("numAnt", C.c_int), ("numAntType", C.c_int), ("numJChan", C.c_int),
+        ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
+        ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int), ("stokType", C.c_int),
+        ("jones", C.c_void_p), ("jonesComps", C.c_int),
+    ]
+
+
 # ---- exported symbols, with C signatures ------------------------------------
 
 _GPUINFO_P = C.POINTER(GPUInfo)
@@ -124,6 +133,7 @@ SIGNATURES = {
                                     C.c_double, C.POINTER(C.c_double), C.c_int]),
     "obit_dft_set_poln": (C.c_int, [_GPUINFO_P, C.c_int, C.c_float, C.c_int]),
     "obit_dft_set_mod_d": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_double), C.c_int]),
+    "obit_dft_set_beam": (C.c_int, [_GPUINFO_P, C.POINTER(ObitDFTBeam)]),
     "obit_dft_set_kernel": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int, C.c_int]),
     "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),

@@ -17,6 +17,7 @@
 
 #include "obit_dft.h"
 #include "abi_internal.h"
+#include "dft_beam.h"
 #include "dft_plan.h"
 
 namespace {
@@ -34,6 +35,29 @@ int fail(int code, const std::string& msg) {
     if (_e != cudaSuccess)                                                          \
       return fail(OBIT_DFT_ECUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
   } while (0)
+
+// Beam-corrected DFT (obit_dft_set_beam): the caller's description, its
+// per-antenna and per-(channel, IF) tables on the device, and the launch
+// parameters built with the plan.
+struct BeamState {
+  bool on = false;
+  int numAnt = 0, numAntType = 0, numJChan = 0, ilocb = -1, iloca1 = -1, iloca2 = -1;
+  int jonesComps = 0;
+  const float* jones = nullptr;
+  int* d_antType = nullptr;
+  int* d_jchan = nullptr;
+  double* d_fscale = nullptr;
+  double* d_lnspec = nullptr;
+  int* d_plane = nullptr;
+  BeamKParams kp{};
+};
+
+void free_beam_tables(BeamState& b) {
+  for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane}) if (q) cudaFree(q);
+  b.d_fscale = nullptr;
+  b.d_lnspec = nullptr;
+  b.d_plane = nullptr;
+}
 
 struct State {
   int device = 0;
@@ -56,6 +80,7 @@ struct State {
   std::vector<cudaStream_t> ownStreams;
   int* d_err = nullptr;
   int waitPolls = kDefaultWaitPolls;  // obit_dft_set_wait_limit
+  BeamState beam;
 };
 
 std::mutex g_mu;
@@ -95,6 +120,9 @@ void release_state(State* s) {
   if (s->d_comps) cudaFree(s->d_comps);
   if (s->d_lo) cudaFree(s->d_lo);
   if (s->d_err) cudaFree(s->d_err);
+  free_beam_tables(s->beam);
+  if (s->beam.d_antType) cudaFree(s->beam.d_antType);
+  if (s->beam.d_jchan) cudaFree(s->beam.d_jchan);
   for (float* b : s->ownBufs) cudaFree(b);
   for (cudaStream_t st : s->ownStreams) cudaStreamDestroy(st);
 }
@@ -114,6 +142,66 @@ int ensure_plan(GPUInfo* g, State* s) {
   s->plan.kp.compsLo = s->haveLo ? s->d_lo : nullptr;
   if (!rc) rc = finalize_plan(&s->plan, nullptr, 0, &err);
   if (rc) return fail(rc, err);
+  if (s->beam.on) {  // launch parameters and per-(channel, IF) tables of the beam kernel
+    BeamState& b = s->beam;
+    if (b.jonesComps < s->mc.model.ncomp)
+      return fail(OBIT_DFT_EBADARG, "the Jones table holds fewer components than the model");
+    free_beam_tables(b);
+    const int nfreq = L.nchan * L.nif;
+    auto upload = [&](const void* h, size_t bytes, void** d) -> int {
+      CUDA_TRY(cudaMalloc(d, std::max<size_t>(bytes, 8)));
+      CUDA_TRY(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+      return OBIT_DFT_OK;
+    };
+    if ((rc = upload(L.fscale.data(), sizeof(double) * nfreq, (void**)&b.d_fscale))) return rc;
+    if ((int)L.lnspec.size() >= nfreq &&
+        (rc = upload(L.lnspec.data(), sizeof(double) * nfreq, (void**)&b.d_lnspec)))
+      return rc;
+    if ((int)L.specIndex.size() >= nfreq &&
+        (rc = upload(L.specIndex.data(), sizeof(int) * nfreq, (void**)&b.d_plane)))
+      return rc;
+    BeamKParams& k = b.kp;
+    k = BeamKParams{};
+    k.lrec = L.lrec;
+    k.nrparm = L.nrparm;
+    k.ilocu = L.ilocu;
+    k.ilocv = L.ilocv;
+    k.ilocw = L.ilocw;
+    k.ilocb = b.ilocb;
+    k.iloca1 = b.iloca1;
+    k.iloca2 = b.iloca2;
+    k.incs = L.incs;
+    k.incf = L.incf;
+    k.incif = L.incif;
+    k.ncorr = L.nstok >= 4 ? 4 : std::min(2, L.nstok);
+    if ((long long)L.nrparm + (long long)L.ife * L.incif + (long long)L.chane * L.incf +
+            (long long)(k.ncorr - 1) * L.incs + 2 >= L.lrec)
+      return fail(OBIT_DFT_EBADARG, "modelled correlations extend past the record");
+    k.op = A.op;
+    for (int q = 0; q < 4; q++) k.polFact[q] = s->mc.stokFact[q];
+    k.chanb = L.chanb;
+    k.nchanSel = L.chane - L.chanb + 1;
+    k.ifb = L.ifb;
+    k.nifSel = L.ife - L.ifb + 1;
+    k.kincf = L.kincf;
+    k.kincif = L.kincif;
+    k.fscale = b.d_fscale;
+    k.lnspec = b.d_lnspec;
+    k.plane = b.d_plane;
+    k.jchan = b.d_jchan;
+    k.antType = b.d_antType;
+    k.numAnt = b.numAnt;
+    k.numJChan = b.numJChan;
+    k.jones = b.jones;
+    k.jonesComps = b.jonesComps;
+    k.comps = s->d_comps;
+    k.ncomp = s->mc.model.ncomp;
+    k.cstride = comp_stride(s->mc.model);
+    k.ct = 128;
+    k.nterm = s->mc.model.nterm;
+    k.mode = s->mc.model.kind;
+    k.errFlag = s->d_err;
+  }
   s->planValid = true;
   return OBIT_DFT_OK;
 }
@@ -221,6 +309,56 @@ int obit_dft_set_mod_d(GPUInfo* g, const double* xyz, int ncomp) {
   return OBIT_DFT_OK;
 }
 
+int obit_dft_set_beam(GPUInfo* g, const ObitDFTBeam* beam) {
+  set_last_error("");
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  BeamState& b = s->beam;
+  if (!beam) {
+    b.on = false;
+    s->planValid = false;
+    return OBIT_DFT_OK;
+  }
+  const GPUVisInfo* v = g->h_visInfo;
+  if (!v) return fail(OBIT_DFT_EBADARG, "GPUInfo.h_visInfo is NULL (call Init first)");
+  if (beam->stokType != 1) return fail(OBIT_DFT_EUNSUPPORTED, "only Stokes I beam models are supported");
+  if (beam->numAnt < 1 || beam->numAntType < 1 || beam->numJChan < 1 || !beam->antType || !beam->jchan ||
+      !beam->jones || beam->jonesComps < 1)
+    return fail(OBIT_DFT_EBADARG, "incomplete beam description");
+  if (((uintptr_t)beam->jones & 15u) != 0) return fail(OBIT_DFT_EBADARG, "Jones table not 16-byte aligned");
+  const int nrparm = v->nrparm;
+  if (beam->ilocb >= 0 ? beam->ilocb >= nrparm
+                       : (beam->iloca1 < 0 || beam->iloca1 >= nrparm || beam->iloca2 < 0 || beam->iloca2 >= nrparm))
+    return fail(OBIT_DFT_EBADARG, "antenna random parameters outside the record's random parameters");
+  for (int i = 0; i < beam->numAnt; i++)
+    if (beam->antType[i] < 0 || beam->antType[i] >= beam->numAntType)
+      return fail(OBIT_DFT_EBADARG, "antenna type outside 0..numAntType-1");
+  const int nfreq = v->nchan * std::max(1, v->nIF);
+  for (int i = 0; i < nfreq; i++)
+    if (beam->jchan[i] < 0 || beam->jchan[i] >= beam->numJChan)
+      return fail(OBIT_DFT_EBADARG, "Jones plane outside 0..numJChan-1");
+  if (b.d_antType) cudaFree(b.d_antType);
+  if (b.d_jchan) cudaFree(b.d_jchan);
+  b.d_antType = nullptr;
+  b.d_jchan = nullptr;
+  CUDA_TRY(cudaMalloc(&b.d_antType, sizeof(int) * beam->numAnt));
+  CUDA_TRY(cudaMemcpy(b.d_antType, beam->antType, sizeof(int) * beam->numAnt, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMalloc(&b.d_jchan, sizeof(int) * nfreq));
+  CUDA_TRY(cudaMemcpy(b.d_jchan, beam->jchan, sizeof(int) * nfreq, cudaMemcpyHostToDevice));
+  b.numAnt = beam->numAnt;
+  b.numAntType = beam->numAntType;
+  b.numJChan = beam->numJChan;
+  b.ilocb = beam->ilocb;
+  b.iloca1 = beam->iloca1;
+  b.iloca2 = beam->iloca2;
+  b.jones = beam->jones;
+  b.jonesComps = beam->jonesComps;
+  b.on = true;
+  s->planValid = false;
+  return OBIT_DFT_OK;
+}
+
 int obit_dft_set_freq(GPUInfo* g, const double* freqArr, int nfreq, double uvRefFreq,
                       double modelRefFreq, const double* specFreq, int nSpec) {
   set_last_error("");
@@ -313,7 +451,14 @@ int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
   rc = ensure_plan(g, s);
   if (rc) return rc;
   std::string err;
-  rc = launch_plan(s->plan, d_vis, 0, nvis, s->d_comps, s->d_err, (cudaStream_t)stream, &err);
+  if (s->beam.on) {
+    BeamKParams k = s->beam.kp;
+    k.vis = d_vis;
+    k.nvis = nvis;
+    rc = launch_beam(k, (cudaStream_t)stream, &err);
+  } else {
+    rc = launch_plan(s->plan, d_vis, 0, nvis, s->d_comps, s->d_err, (cudaStream_t)stream, &err);
+  }
   if (rc) return fail(rc, err);
   return OBIT_DFT_OK;
 }
@@ -404,7 +549,14 @@ int obit_dft_calc(GPUInfo* g) {
     const size_t bytes = sizeof(float) * (size_t)nr * lenvis;
     float* host = g->h_data + (size_t)r0 * lenvis;
     CUDA_TRY(cudaMemcpyAsync(bufs[b], host, bytes, cudaMemcpyHostToDevice, streams[b]));
-    rc = launch_plan(s->plan, bufs[b], 0, nr, s->d_comps, s->d_err, streams[b], &err);
+    if (s->beam.on) {
+      BeamKParams k = s->beam.kp;
+      k.vis = bufs[b];
+      k.nvis = nr;
+      rc = launch_beam(k, streams[b], &err);
+    } else {
+      rc = launch_plan(s->plan, bufs[b], 0, nr, s->d_comps, s->d_err, streams[b], &err);
+    }
     if (rc) return fail(rc, err);
     CUDA_TRY(cudaMemcpyAsync(host, bufs[b], bytes, cudaMemcpyDeviceToHost, streams[b]));
   }

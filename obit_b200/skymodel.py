@@ -174,6 +174,16 @@ class GPUSkyModel:
         _lib.check(self._lib.obit_dft_set_mod_d(self.gpuinfo, a.ctypes.data_as(C.POINTER(C.c_double)),
                                                 a.shape[0]))
 
+    def set_beam(self, beam, d_jones: int = 0) -> None:
+        """Beam-corrected model (obit_b200.beam.Beam, Jones table at device
+        address d_jones) for the following calls; None returns to the plain
+        sky model."""
+        if beam is None:
+            _lib.check(self._lib.obit_dft_set_beam(self.gpuinfo, None))
+            return
+        self._beam_desc = beam.descriptor(d_jones)
+        _lib.check(self._lib.obit_dft_set_beam(self.gpuinfo, C.byref(self._beam_desc)))
+
     def plan_info(self) -> dict:
         """The kernel plan the next call uses (built on demand)."""
         arr = (C.c_int * 8)()

@@ -173,6 +173,48 @@ def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = 
     return out
 
 
+class OracleBeam(C.Structure):
+    _fields_ = [
+        ("numAnt", C.c_int), ("numAntType", C.c_int), ("numJChan", C.c_int),
+        ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
+        ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int),
+        ("jones", C.POINTER(C.c_float)),
+    ]
+
+
+def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None):
+    """FP64 beam-corrected model (oracle_beam.c) applied to a copy of uv.vis:
+    returns (records, l1 of shape (nvis, nif, nchan, 4) over the model
+    correlations XX, XY, YX, YY).  beam: obit_b200.beam.Beam (host Jones
+    table); the first min(2, nstok) correlations, or all four, are modelled."""
+    jb = Job(uv, sky, params, exact=True)
+    jb.job.startPoln = 0
+    jb.job.numberPoln = 4 if uv.nstok >= 4 else min(2, uv.nstok)
+    for i in range(4):
+        jb.job.polFact[i] = 1.0
+    at = np.ascontiguousarray(beam.antType, dtype=np.int32)
+    jc = np.ascontiguousarray(beam.jchan, dtype=np.int32)
+    jo = np.ascontiguousarray(beam.jones, dtype=np.float32)
+    assert jo.shape[1] >= sky.ncomp
+    ob = OracleBeam(len(at), jo.shape[0], jo.shape[2], _p(at, C.c_int), _p(jc, C.c_int), beam.ilocb,
+                    beam.iloca1, beam.iloca2, _p(jo, C.c_float))
+    # the oracle indexes the table with the model's component count
+    if jo.shape[1] != sky.ncomp:
+        jo = np.ascontiguousarray(jo[:, :sky.ncomp])
+        ob.jones = _p(jo, C.c_float)
+    out = np.ascontiguousarray(uv.vis, dtype=np.float32).copy()
+    l1 = np.full((uv.nvis, uv.nchan * uv.nif, 4), np.nan)
+    lib = lib_a()
+    lib.oracle_beam_apply.restype = C.c_int
+    lib.oracle_beam_apply.argtypes = [C.POINTER(OracleJob), C.POINTER(OracleBeam), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_double), C.c_int]
+    rc = lib.oracle_beam_apply(C.byref(jb.job), C.byref(ob), _p(out, C.c_float), _p(l1, C.c_double),
+                               nthreads or nthreads_default())
+    if rc:
+        raise ValueError(f"oracle_beam_apply returned {rc}")
+    return out, l1.reshape(uv.nvis, uv.nif, uv.nchan, 4)
+
+
 def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):
     """Reference-faithful CPU restatement (FP32 phase, reference sin/cos)
     applied to a copy of uv.vis; returns the new float32 records."""

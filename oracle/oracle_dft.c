@@ -42,6 +42,48 @@ typedef struct {
 
 static int type_ok(int t) { return t >= ORACLE_POINT && t <= ORACLE_GAUSS_TSPEC; }
 
+void oracle_comp_term(const OracleJob *j, int ic, double u, double v, double w, double L, int plane,
+                      double *amp_out, double *ph_out) {
+  const float *c = j->comps + (size_t)ic * j->lcomp;
+  double amp, expo = 0.0;
+  switch (j->modType) {
+    case ORACLE_POINT:
+      amp = c[0];
+      break;
+    case ORACLE_POINT_SPEC: {
+      double p = L;
+      for (int t = 0; t < j->nterm; t++) { expo += (double)c[4 + t] * p; p *= L; }
+      amp = c[0];
+      break;
+    }
+    case ORACLE_POINT_TSPEC:
+      amp = c[5 + plane];
+      expo = (double)c[4] * L;
+      break;
+    case ORACLE_GAUSS:
+      amp = c[0];
+      expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v;
+      break;
+    case ORACLE_GAUSS_SPEC: {
+      double p = L;
+      expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v;
+      for (int t = 0; t < j->nterm; t++) { expo += (double)c[7 + t] * p; p *= L; }
+      amp = c[0];
+      break;
+    }
+    default: /* ORACLE_GAUSS_TSPEC */
+      amp = c[8 + plane];
+      expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v +
+             (double)c[7] * L;
+      break;
+  }
+  if (expo != 0.0) amp *= exp(expo);
+  const double *x = j->xyz ? j->xyz + 3 * (size_t)ic : NULL;
+  *ph_out = x ? x[0] * u + x[1] * v + x[2] * w
+              : (double)c[1] * u + (double)c[2] * v + (double)c[3] * w;
+  *amp_out = amp;
+}
+
 /* Raw component sum for one record at one (channel, IF) table index. */
 static void comp_sum(const OracleJob *j, const float *rec, int ifq, double *sr,
                      double *si, double *l1) {
@@ -52,44 +94,9 @@ static void comp_sum(const OracleJob *j, const float *rec, int ifq, double *sr,
   const double L = j->lnspec ? j->lnspec[ifq] : 0.0;
   const int plane = j->specIndex ? j->specIndex[ifq] : 0;
   double accr = 0.0, acci = 0.0, accl = 0.0;
-  const float *c = j->comps;
-  for (int ic = 0; ic < j->ncomp; ic++, c += j->lcomp) {
-    double amp, expo = 0.0;
-    switch (j->modType) {
-      case ORACLE_POINT:
-        amp = c[0];
-        break;
-      case ORACLE_POINT_SPEC: {
-        double p = L;
-        for (int t = 0; t < j->nterm; t++) { expo += (double)c[4 + t] * p; p *= L; }
-        amp = c[0];
-        break;
-      }
-      case ORACLE_POINT_TSPEC:
-        amp = c[5 + plane];
-        expo = (double)c[4] * L;
-        break;
-      case ORACLE_GAUSS:
-        amp = c[0];
-        expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v;
-        break;
-      case ORACLE_GAUSS_SPEC: {
-        double p = L;
-        expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v;
-        for (int t = 0; t < j->nterm; t++) { expo += (double)c[7 + t] * p; p *= L; }
-        amp = c[0];
-        break;
-      }
-      default: /* ORACLE_GAUSS_TSPEC */
-        amp = c[8 + plane];
-        expo = (double)c[4] * u * u + (double)c[5] * v * v + (double)c[6] * u * v +
-               (double)c[7] * L;
-        break;
-    }
-    if (expo != 0.0) amp *= exp(expo);
-    const double *x = j->xyz ? j->xyz + 3 * (size_t)ic : NULL;
-    const double ph = x ? x[0] * u + x[1] * v + x[2] * w
-                        : (double)c[1] * u + (double)c[2] * v + (double)c[3] * w;
+  for (int ic = 0; ic < j->ncomp; ic++) {
+    double amp, ph;
+    oracle_comp_term(j, ic, u, v, w, L, plane, &amp, &ph);
     accr += amp * cos(ph);
     acci += amp * sin(ph);
     accl += fabs(amp);

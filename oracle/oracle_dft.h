@@ -64,6 +64,13 @@ typedef struct OracleJob {
   const double *xyz;
 } OracleJob;
 
+/* One component's FP64 amplitude (flux x spectrum x taper) and phase
+ * X u + Y v + Z w at scaled (u, v, w), for the log-frequency term L and the
+ * coarse plane of the (channel, IF) (the per-component step of the model
+ * functions below). */
+void oracle_comp_term(const OracleJob *job, int ic, double u, double v, double w, double L,
+                      int plane, double *amp, double *phase);
+
 /* (A) FP64 model: for every row and selected (channel, IF) writes the raw
  * complex component sum S = sum_c amp_c exp(i phase_c) (no flip, no
  * polarization factor) to model[(row*nfreq + ifq)*2 + {0,1}] and the L1 norm
@@ -80,6 +87,26 @@ int oracle_apply_fp64(const OracleJob *job, float *vis, int nthreads);
 
 /* (B) reference-faithful restatement; in oracle/_ref/libobit_refcpu.so only. */
 int refcpu_apply(const OracleJob *job, float *vis, int nthreads);
+
+/* Beam-corrected DFT (oracle_beam.c): antenna types, the Jones plane of each
+ * (channel, IF) and the Jones table of ObitCUDABeamModel (GPUBeamAntInfo,
+ * ObitSystem/Obit/include/ObitCUDABeamModelInfoDef.h:178-205). */
+typedef struct OracleBeam {
+  int numAnt, numAntType, numJChan;
+  const int *antType;   /* [numAnt] type of each antenna (0-rel) */
+  const int *jchan;     /* [nchan*nif] Jones plane per (channel, IF) table index */
+  int ilocb;            /* BASELINE offset in the record, or -1 */
+  int iloca1, iloca2;   /* ANTENNA1 / ANTENNA2 offsets when ilocb < 0 */
+  const float *jones;   /* [numAntType][ncomp][numJChan][8]: XX, XY, YX, YY complex */
+} OracleBeam;
+
+/* Applies the beam-corrected FP64 model (Stokes I, linear feeds) to the
+ * records in place: job->numberPoln correlations from the first (XX, YY, XY,
+ * YX), the job's channel / IF selection and operation.  l1 (may be NULL)
+ * receives per (row, table index, model correlation XX/XY/YX/YY) the sum over
+ * components of |amp| |coefficient|.  Returns 0, or < 0 for a bad job. */
+int oracle_beam_apply(const OracleJob *job, const OracleBeam *beam, float *vis, double *l1,
+                      int nthreads);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,124 @@
+"""Beam-corrected DFT (obit_dft_set_beam) on a B200 against the FP64 beam
+oracle: random Jones matrices per antenna type, component and Jones plane,
+2 or 4 correlations, subtract / replace / divide with flags, every model
+family; unit Jones matrices reproduce the plain sky model; a record whose
+antennas fall outside the table is reported and left untouched."""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import TOL_REL, run_gpu
+from obit_b200 import _lib
+from obit_b200 import uvdata as U
+from obit_b200.skymodel import OP_DIV, OP_REPL, OP_SUB, GPUSkyModel, SkyModelParams
+from test_beam_oracle_cpu import beam_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_beam(uv, sky, p, beam, torch, jones=None):
+    out = uv.copy()
+    d_jones = torch.from_numpy(np.ascontiguousarray(jones if jones is not None else beam.jones)).cuda()
+    gm = GPUSkyModel("beam")
+    try:
+        gm.DFTInit(sky, out, SkyModelParams(**{**p.__dict__, "nVisPIO": uv.nvis}))
+        gm.set_beam(beam, d_jones.data_ptr())
+        gm.DFTSetMod(sky)
+        gm.DFTCalc(out)
+        gm.DFTShutdown()
+    finally:
+        gm.close()
+    return out.vis
+
+
+def _check(uv, got, want, l1, op):
+    shape = uv.vis_view().shape
+    a = got[:, uv.nrparm:].reshape(shape)
+    b = want[:, uv.nrparm:].reshape(shape)
+    ncorr = 4 if uv.nstok >= 4 else min(2, uv.nstok)
+    model_of = [0, 3, 1, 2]
+    assert np.array_equal(a[..., ncorr:, :], uv.vis_view()[..., ncorr:, :])
+    assert np.array_equal(a[..., 2], uv.vis_view()[..., 2])  # weights are never changed
+    for p_ in range(ncorr):
+        L = l1[..., model_of[p_]]
+        if op == OP_DIV:
+            sel = b[..., p_, 2] > 0
+            g = 1.0 / (a[..., p_, 0] + 1j * a[..., p_, 1])
+            w = 1.0 / (b[..., p_, 0] + 1j * b[..., p_, 1])
+            rel = np.where(sel, np.abs(g - w) / np.maximum(L, 1e-30), 0)
+            assert np.nanmax(rel) < 2 * TOL_REL
+        else:
+            d = np.abs((a[..., p_, 0] - b[..., p_, 0]) + 1j * (a[..., p_, 1] - b[..., p_, 1]))
+            assert np.nanmax(d / np.maximum(L, 1e-30)) < TOL_REL + 1e-6
+
+
+@pytest.mark.parametrize("nstok", [2, 4])
+@pytest.mark.parametrize("op", [OP_SUB, OP_REPL, OP_DIV])
+def test_beam_matches_oracle(op, nstok):
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=nstok, nrow=70, nchan=24, nif=2, ncomp=150, seed=3 + op,
+                              flag_frac=0.1)
+    if op == OP_DIV:
+        c = uv.vis_view()
+        c[..., 0] = 1.0
+        c[..., 1] = 0.0
+    p = SkyModelParams(op=op)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, op)
+
+
+@pytest.mark.parametrize("mt", [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC, U.MOD_GAUSS,
+                                U.MOD_GAUSS_SPEC, U.MOD_GAUSS_TSPEC])
+def test_beam_every_family(mt):
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(mt=mt, nstok=4, nrow=40, nchan=20, nif=2, ncomp=90, seed=11 + mt)
+    p = SkyModelParams(op=OP_SUB)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
+
+
+def test_unit_jones_reproduce_the_sky_model():
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=2, nrow=50, nchan=32, nif=2, ncomp=120, unit=True)
+    p = SkyModelParams(op=OP_REPL)
+    got = _run_beam(uv, sky, p, beam, torch)
+    plain = run_gpu(uv, sky, SkyModelParams(op=OP_REPL)).vis
+    _, l1 = oracle.model_fp64(uv, sky, p)
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :2]
+    b = plain[:, uv.nrparm:].reshape(a.shape[:-1] + (3,))[..., :2]
+    d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1]))
+    assert np.max(d / l1[..., None]) < 2 * TOL_REL
+
+
+def test_antenna_outside_the_table_is_reported():
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=2, nrow=20, nchan=8, nif=1, ncomp=30)
+    uv.vis[5, 3] = 256.0 * 1 + 40  # antenna 40 of 12
+    p = SkyModelParams(op=OP_SUB)
+    with pytest.raises(_lib.DFTError) as e:
+        _run_beam(uv, sky, p, beam, torch)
+    assert e.value.code == 4 or "code 3" in str(e.value)
+
+
+def test_beam_description_is_validated():
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=2, nrow=10, nchan=8, nif=1, ncomp=20)
+    d_jones = torch.from_numpy(beam.jones).cuda()
+    out = uv.copy()
+    gm = GPUSkyModel("beam-bad")
+    try:
+        gm.DFTInit(sky, out, SkyModelParams(op=OP_SUB, nVisPIO=uv.nvis))
+        bad_type = beam.antType.copy()
+        bad_type[3] = 7
+        from obit_b200.beam import Beam
+        for b, msg in ((Beam(bad_type, beam.jchan, beam.jones), "antenna type"),
+                       (Beam(beam.antType, beam.jchan + 5, beam.jones), "Jones plane"),
+                       (Beam(beam.antType, beam.jchan, beam.jones, stokType=2), "Stokes I")):
+            with pytest.raises(_lib.DFTError) as e:
+                gm.set_beam(b, d_jones.data_ptr())
+            assert msg in str(e.value)
+        gm.DFTShutdown()
+    finally:
+        gm.close()
