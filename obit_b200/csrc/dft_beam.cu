@@ -1,11 +1,15 @@
 // Beam-corrected DFT kernel (Stokes I, linear feeds).  One thread per (record,
-// selected channel-IF); the CTA stages component tiles in shared memory; per
-// component the phase is formed in FP64 and range-reduced (MUFU sin/cos of the
-// fractional turn), the amplitude carries the model family's spectrum and
-// taper, and the coefficients of the baseline's Jones pair,
+// selected channel-IF).  Per component tile the CTA stages the components and
+// computes, once for the whole tile, the coefficients of every antenna-type
+// pair at every Jones plane,
 //   XX: P(0,0) + P(1,1)   XY: P(1,3) + P(0,2)   YX: P(2,0) + P(3,1)   YY: P(2,2) + P(3,3)
 // with P(i, j) = J1[i] conj(J2[j]) (cudaJonesCor1_Lin_I, CUDALinCorSum.h:104-134),
-// multiply it into four FP32 sums folded per tile into compensated totals.
+// in shared memory: a thread then reads its baseline's coefficients with two
+// 16-byte loads, where the reference recomputes the Jones products for every
+// evaluation.  Per component the phase is formed in FP64 and range-reduced
+// (MUFU sin/cos of the fractional turn), the amplitude carries the model
+// family's spectrum and taper, and the four products go into FP32 sums folded
+// per tile into compensated totals.
 // Records hold XX, YY, XY, YX; each modelled correlation with positive weight
 // (any, when replacing) is subtracted from, divided into or replaced by its
 // model, independently of the others.
@@ -13,6 +17,7 @@
 
 #include "dft_beam.h"
 #include "dft_kernels.cuh"
+#include "dft_plan.h"
 
 namespace obit {
 
@@ -79,9 +84,11 @@ __global__ void __launch_bounds__(256) dft_beam_kernel(const __grid_constant__ B
       if (!any) active = false;
     }
   }
-  const size_t tstride = (size_t)p.jonesComps * p.numJChan * 8;
-  const float* J1b = p.jones + (size_t)t1 * tstride + (size_t)jc * 8;
-  const float* J2b = p.jones + (size_t)t2 * tstride + (size_t)jc * 8;
+  // coefficients of the tile: [type pair][component][plane] x 8 floats
+  float* sC = sComp + p.ct * p.cstride;
+  const int crow = p.numJChan * 8;
+  const float* Cb = sC + (size_t)(t1 * p.numAntType + t2) * p.ct * crow + jc * 8;
+  const int npair = p.numAntType * p.numAntType;
   float totR[4], totI[4], cmpR[4], cmpI[4];
 #pragma unroll
   for (int q = 0; q < 4; q++) totR[q] = totI[q] = cmpR[q] = cmpI[q] = 0.0f;
@@ -91,6 +98,32 @@ __global__ void __launch_bounds__(256) dft_beam_kernel(const __grid_constant__ B
     __syncthreads();  // the previous tile's readers are done
     const float* src = p.comps + (size_t)c0 * p.cstride;
     for (int i = threadIdx.x; i < nc * p.cstride; i += blockDim.x) sComp[i] = src[i];
+    for (int i = threadIdx.x; i < npair * nc * p.numJChan; i += blockDim.x) {
+      const int pr = i / (nc * p.numJChan);
+      const int rem = i - pr * nc * p.numJChan;
+      const int c = rem / p.numJChan, j = rem - c * p.numJChan;
+      const int ta = pr / p.numAntType, tb = pr - ta * p.numAntType;
+      const float* J1 = p.jones + (((size_t)ta * p.jonesComps + c0 + c) * p.numJChan + j) * 8;
+      const float* J2 = p.jones + (((size_t)tb * p.jonesComps + c0 + c) * p.numJChan + j) * 8;
+      const float4 a0 = __ldg(reinterpret_cast<const float4*>(J1));
+      const float4 a1 = __ldg(reinterpret_cast<const float4*>(J1 + 4));
+      const float4 b0 = __ldg(reinterpret_cast<const float4*>(J2));
+      const float4 b1 = __ldg(reinterpret_cast<const float4*>(J2 + 4));
+      const float J1r[4] = {a0.x, a0.z, a1.x, a1.z}, J1i[4] = {a0.y, a0.w, a1.y, a1.w};
+      const float J2r[4] = {b0.x, b0.z, b1.x, b1.z}, J2i[4] = {b0.y, b0.w, b1.y, b1.w};
+      float cr[4] = {0.f, 0.f, 0.f, 0.f}, ci[4] = {0.f, 0.f, 0.f, 0.f};
+      pconj(J1r[0], J1i[0], J2r[0], J2i[0], cr[0], ci[0]);  // XX
+      pconj(J1r[1], J1i[1], J2r[1], J2i[1], cr[0], ci[0]);
+      pconj(J1r[1], J1i[1], J2r[3], J2i[3], cr[1], ci[1]);  // XY
+      pconj(J1r[0], J1i[0], J2r[2], J2i[2], cr[1], ci[1]);
+      pconj(J1r[2], J1i[2], J2r[0], J2i[0], cr[2], ci[2]);  // YX
+      pconj(J1r[3], J1i[3], J2r[1], J2i[1], cr[2], ci[2]);
+      pconj(J1r[2], J1i[2], J2r[2], J2i[2], cr[3], ci[3]);  // YY
+      pconj(J1r[3], J1i[3], J2r[3], J2i[3], cr[3], ci[3]);
+      float4* d = reinterpret_cast<float4*>(sC + ((size_t)pr * p.ct + c) * crow + j * 8);
+      d[0] = make_float4(cr[0], ci[0], cr[1], ci[1]);
+      d[1] = make_float4(cr[2], ci[2], cr[3], ci[3]);
+    }
     __syncthreads();
     if (!active) continue;
     float accR[4] = {0.f, 0.f, 0.f, 0.f}, accI[4] = {0.f, 0.f, 0.f, 0.f};
@@ -116,23 +149,10 @@ __global__ void __launch_bounds__(256) dft_beam_kernel(const __grid_constant__ B
       float sn, cs;
       __sincosf(6.283185307179586f * rr, &sn, &cs);
       const float vr = A * cs, vi = A * sn;
-      // Jones pair of this component at the channel's plane: (XX, XY, YX, YY)
-      const size_t jo = (size_t)(c0 + c) * p.numJChan * 8;
-      const float4 a0 = __ldg(reinterpret_cast<const float4*>(J1b + jo));
-      const float4 a1 = __ldg(reinterpret_cast<const float4*>(J1b + jo + 4));
-      const float4 b0 = __ldg(reinterpret_cast<const float4*>(J2b + jo));
-      const float4 b1 = __ldg(reinterpret_cast<const float4*>(J2b + jo + 4));
-      const float J1r[4] = {a0.x, a0.z, a1.x, a1.z}, J1i[4] = {a0.y, a0.w, a1.y, a1.w};
-      const float J2r[4] = {b0.x, b0.z, b1.x, b1.z}, J2i[4] = {b0.y, b0.w, b1.y, b1.w};
-      float cr[4] = {0.f, 0.f, 0.f, 0.f}, ci[4] = {0.f, 0.f, 0.f, 0.f};
-      pconj(J1r[0], J1i[0], J2r[0], J2i[0], cr[0], ci[0]);  // XX
-      pconj(J1r[1], J1i[1], J2r[1], J2i[1], cr[0], ci[0]);
-      pconj(J1r[1], J1i[1], J2r[3], J2i[3], cr[1], ci[1]);  // XY
-      pconj(J1r[0], J1i[0], J2r[2], J2i[2], cr[1], ci[1]);
-      pconj(J1r[2], J1i[2], J2r[0], J2i[0], cr[2], ci[2]);  // YX
-      pconj(J1r[3], J1i[3], J2r[1], J2i[1], cr[2], ci[2]);
-      pconj(J1r[2], J1i[2], J2r[2], J2i[2], cr[3], ci[3]);  // YY
-      pconj(J1r[3], J1i[3], J2r[3], J2i[3], cr[3], ci[3]);
+      // the baseline's coefficients for this component at the channel's plane
+      const float4 k0 = *reinterpret_cast<const float4*>(Cb + (size_t)c * crow);
+      const float4 k1 = *reinterpret_cast<const float4*>(Cb + (size_t)c * crow + 4);
+      const float cr[4] = {k0.x, k0.z, k1.x, k1.z}, ci[4] = {k0.y, k0.w, k1.y, k1.w};
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         accR[q] = __fmaf_rn(cr[q], vr, __fmaf_rn(-ci[q], vi, accR[q]));
@@ -197,8 +217,10 @@ int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err) {
     *err = std::string("error pending before the beam kernel launch: ") + cudaGetErrorString(ce);
     return 2;
   }
+  const size_t smem = beam_smem_bytes(kp);
+  if (int rc = raise_smem_limit((const void*)fn, smem, err)) return rc;
   const long long grid = (nitems + 255) / 256;
-  fn<<<(unsigned)grid, 256, beam_smem_bytes(kp), stream>>>(kp);
+  fn<<<(unsigned)grid, 256, smem, stream>>>(kp);
   ce = cudaGetLastError();
   if (ce != cudaSuccess) {
     *err = std::string("beam kernel launch: ") + cudaGetErrorString(ce);

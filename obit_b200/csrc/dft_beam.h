@@ -22,7 +22,7 @@ struct BeamKParams {
   const int* plane;              // device or null: tabulated-spectrum plane per table index
   const int* jchan;              // device: Jones plane per table index
   const int* antType;            // device: antenna type per antenna (0-rel)
-  int numAnt, numJChan;
+  int numAnt, numAntType, numJChan;
   const float* jones;            // device: [type][component][plane] x 8 floats (XX, XY, YX, YY)
   int jonesComps;                // components per type in the Jones table (>= ncomp)
   const float* comps;            // device: ncomp records of cstride floats
@@ -30,8 +30,11 @@ struct BeamKParams {
   int* errFlag;                  // set to 3 for a record whose antennas are outside the table
 };
 
-// Shared memory of one launch (component tile).
-inline size_t beam_smem_bytes(const BeamKParams& p) { return sizeof(float) * (size_t)p.ct * p.cstride; }
+// Shared memory of one launch: the component tile and its Jones coefficients
+// for every (type, type) pair and plane, 8 floats each.
+inline size_t beam_smem_bytes(const BeamKParams& p) {
+  return sizeof(float) * ((size_t)p.ct * p.cstride + (size_t)p.numAntType * p.numAntType * p.ct * p.numJChan * 8);
+}
 
 // One launch over all records of kp (stream-ordered, asynchronous).
 int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);

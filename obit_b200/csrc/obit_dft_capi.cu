@@ -191,13 +191,18 @@ int ensure_plan(GPUInfo* g, State* s) {
     k.jchan = b.d_jchan;
     k.antType = b.d_antType;
     k.numAnt = b.numAnt;
+    k.numAntType = b.numAntType;
     k.numJChan = b.numJChan;
     k.jones = b.jones;
     k.jonesComps = b.jonesComps;
     k.comps = s->d_comps;
     k.ncomp = s->mc.model.ncomp;
     k.cstride = comp_stride(s->mc.model);
-    k.ct = 128;
+    // component tile: 128, or fewer so that the tile's coefficients (every
+    // type pair and plane) stay within 96 KB of shared memory
+    const size_t perComp =
+        sizeof(float) * ((size_t)k.cstride + (size_t)b.numAntType * b.numAntType * b.numJChan * 8);
+    k.ct = (int)std::max<size_t>(1, std::min<size_t>(128, (96 * 1024) / perComp));
     k.nterm = s->mc.model.nterm;
     k.mode = s->mc.model.kind;
     k.errFlag = s->d_err;

@@ -122,3 +122,16 @@ def test_beam_description_is_validated():
         gm.DFTShutdown()
     finally:
         gm.close()
+
+
+def test_beam_nonuniform_channels_take_the_direct_form():
+    """Irregular channel frequencies: the per-evaluation form (FP64 phase per
+    channel) instead of the recurrence, against the same oracle."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=4, nrow=40, nchan=24, nif=2, ncomp=100, seed=19, flag_frac=0.1)
+    rng = np.random.default_rng(3)
+    uv.freqArr = np.sort(uv.freqArr + rng.uniform(-3e5, 3e5, uv.freqArr.shape))
+    p = SkyModelParams(op=OP_SUB)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
