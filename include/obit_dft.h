@@ -173,9 +173,9 @@ int obit_dft_shutdown(GPUInfo *gpuInfo);
 int obit_dft_set_mod_d(GPUInfo *gpuInfo, const double *xyz, int ncomp);
 void ObitCUDASkyModelDFTSetModD(GPUInfo *gpuInfo, const double *xyz, int ncomp);
 
-/* Beam-corrected DFT, Stokes I sky, linear feeds (the model of
+/* Beam-corrected DFT, linear feeds, Stokes I, Q, U or V sky (the model of
  * ObitCUDABeamModel's beam*Kernel family, ObitCUDABeamModel.cu:139-1226, with
- * the Jones product of cudaJonesCor1_Lin_I, CUDALinCorSum.h:104-134).  No
+ * the Jones products of cudaJonesCor1_Lin_{I,Q,U,V}, CUDALinCorSum.h:104-455).  No
  * level-2 counterpart of this shape: the reference's ObitCUDABeamModelDFT*
  * calls take a GPUBeamInfo of device beam-image interpolators
  * (ObitCUDABeamModelInfoDef.h:148-275) and fill the Jones table from them on
@@ -184,7 +184,12 @@ void ObitCUDASkyModelDFTSetModD(GPUInfo *gpuInfo, const double *xyz, int ncomp);
  * ANTENNA1 / ANTENNA2, as GetAnts (ObitCUDABeamModel.cu:82-99) -- and a
  * (channel, IF) of Jones plane jc, component c contributes its DFT term times
  *   XX: P(0,0) + P(1,1)   XY: P(1,3) + P(0,2)   YX: P(2,0) + P(3,1)   YY: P(2,2) + P(3,3),
- * P(i, j) = J1[i] conj(J2[j]), J1 = jones[type(a1)][c][jc], J2 = jones[type(a2)][c][jc].
+ * P(i, j) = J1[i] conj(J2[j]), J1 = jones[type(a1)][c][jc], J2 = jones[type(a2)][c][jc],
+ * for Stokes I; Q and U combine D = P00 - P11 (XY: P02 - P13, YX: P20 - P31, YY:
+ * P22 - P33) and S = P10 + P01 (P12 + P03, P30 + P21, P32 + P23) as c2p D - s2p S
+ * and c2p S + s2p D with c2p, s2p = cos, sin of twice the parallactic angle; V is
+ * i (P01 - P13), i (P03 - P12), i (P21 - P30), i (P23 - P32) -- the combinations
+ * the reference's GPU kernels and its CPU ObitSkyModelVMBeamJonesCorSum use.
  * The records' first correlations XX, YY (, XY, YX with four) are modelled;
  * each one with positive weight (any, when replacing) is subtracted from,
  * divided into (weight unchanged) or replaced by its model times stokFact of
@@ -202,10 +207,11 @@ typedef struct ObitDFTBeam {
   const int *jchan;      /* host [nchan*nIF]: Jones plane of each (channel, IF), freqScale order */
   int ilocb;             /* BASELINE random parameter offset, or -1 */
   int iloca1, iloca2;    /* ANTENNA1 / ANTENNA2 offsets when ilocb < 0 */
-  int stokType;          /* Stokes of the sky model: 1 = I (the only one supported) */
+  int stokType;          /* Stokes of the sky model: 1 I, 2 Q, 3 U, 4 V */
   const float *jones;    /* device, 16-byte aligned: [numAntType][jonesComps][numJChan] 2x2
                             complex matrices of 8 floats (XX, XY, YX, YY as re, im) */
   int jonesComps;        /* components per type in jones, at least the model's */
+  float parAng;          /* parallactic angle, radians (Stokes Q and U) */
 } ObitDFTBeam;
 int obit_dft_set_beam(GPUInfo *gpuInfo, const ObitDFTBeam *beam);
 

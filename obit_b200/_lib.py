@@ -110,7 +110,7 @@ class ObitDFTBeam(C.Structure):
         ("numAnt", C.c_int), ("numAntType", C.c_int), ("numJChan", C.c_int),
         ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
         ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int), ("stokType", C.c_int),
-        ("jones", C.c_void_p), ("jonesComps", C.c_int),
+        ("jones", C.c_void_p), ("jonesComps", C.c_int), ("parAng", C.c_float),
     ]
 
 

@@ -1,7 +1,7 @@
 """Beam-corrected DFT description (obit_dft_set_beam): antenna types, the
 Jones plane of each (channel, IF) and the Jones table of ObitCUDABeamModel
-(GPUBeamAntInfo, ObitCUDABeamModelInfoDef.h:178-205) for a Stokes I sky and
-linear feeds."""
+(GPUBeamAntInfo, ObitCUDABeamModelInfoDef.h:178-205) for linear feeds and a
+Stokes I, Q, U or V sky."""
 from __future__ import annotations
 
 import ctypes as C
@@ -20,7 +20,8 @@ class Beam:
     ilocb: int = 3               # BASELINE random parameter, or -1 for ANTENNA1 / ANTENNA2
     iloca1: int = -1
     iloca2: int = -1
-    stokType: int = 1
+    stokType: int = 1            # 1 I, 2 Q, 3 U, 4 V
+    parAng: float = 0.0          # parallactic angle, radians (Q, U)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -43,7 +44,7 @@ class Beam:
         return _lib.ObitDFTBeam(self.numAnt, self.numAntType, self.numJChan,
                                 at.ctypes.data_as(C.POINTER(C.c_int)), jc.ctypes.data_as(C.POINTER(C.c_int)),
                                 self.ilocb, self.iloca1, self.iloca2, self.stokType, C.c_void_p(d_jones),
-                                int(self.jones.shape[1]))
+                                int(self.jones.shape[1]), float(self.parAng))
 
 
 def baseline_codes(nant: int, nrow: int) -> np.ndarray:

@@ -1,10 +1,7 @@
-// Beam-corrected DFT kernel (Stokes I, linear feeds).  One thread per (record,
-// selected channel-IF).  Per component tile the CTA stages the components and
-// computes, once for the whole tile, the coefficients of every antenna-type
-// pair at every Jones plane,
-//   XX: P(0,0) + P(1,1)   XY: P(1,3) + P(0,2)   YX: P(2,0) + P(3,1)   YY: P(2,2) + P(3,3)
-// with P(i, j) = J1[i] conj(J2[j]) (cudaJonesCor1_Lin_I, CUDALinCorSum.h:104-134),
-// in shared memory: a thread then reads its baseline's coefficients with two
+// Beam-corrected DFT kernel (linear feeds; Stokes I, Q, U or V sky).  One
+// thread per (record, selected channel-IF).  Per component tile the CTA stages
+// the components and computes, once for the whole tile, the coefficients of
+// every antenna-type pair at every Jones plane (beam_coeffs) in shared memory: a thread then reads its baseline's coefficients with two
 // 16-byte loads, where the reference recomputes the Jones products for every
 // evaluation.  Per component the phase is formed in FP64 and range-reduced
 // (MUFU sin/cos of the fractional turn), the amplitude carries the model
@@ -42,6 +39,63 @@ __device__ __forceinline__ void beam_ants(const BeamKParams& p, const float* rec
 __device__ __forceinline__ void pconj(float ar, float ai, float br, float bi, float& re, float& im) {
   re = __fmaf_rn(ar, br, __fmaf_rn(ai, bi, re));
   im = __fmaf_rn(ai, br, __fmaf_rn(-ar, bi, im));
+}
+
+// Coefficients of the model correlations XX, XY, YX, YY from P(i, j) =
+// J1[i] conj(J2[j]) for the sky's Stokes, as cudaJonesCor1_Lin_{I,Q,U,V}
+// (CUDALinCorSum.h:104-455) and ObitSkyModelVMBeamJonesCorSum
+// (ObitSkyModelVMBeam.c:1117-1240) form them:
+//   I: XX P00+P11  XY P13+P02  YX P20+P31  YY P22+P33
+//   Q: c2p D - s2p S,  U: c2p S + s2p D, with per correlation
+//      XX D = P00-P11 S = P10+P01   XY D = P02-P13 S = P12+P03
+//      YX D = P20-P31 S = P30+P21   YY D = P22-P33 S = P32+P23
+//   V: i (P01-P13), i (P03-P12), i (P21-P30), i (P23-P32)
+__device__ __forceinline__ void beam_coeffs(const BeamKParams& p, const float* J1r, const float* J1i,
+                                            const float* J2r, const float* J2i, float* cr, float* ci) {
+  auto P = [&](int x, int y, float& re, float& im) {
+    re = 0.f;
+    im = 0.f;
+    pconj(J1r[x], J1i[x], J2r[y], J2i[y], re, im);
+  };
+  float r0, i0, r1, i1;
+  if (p.stokType == 1) {
+    const int a[4][4] = {{0, 0, 1, 1}, {1, 3, 0, 2}, {2, 0, 3, 1}, {2, 2, 3, 3}};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      P(a[q][0], a[q][1], r0, i0);
+      P(a[q][2], a[q][3], r1, i1);
+      cr[q] = r0 + r1;
+      ci[q] = i0 + i1;
+    }
+  } else if (p.stokType == 4) {
+    const int a[4][4] = {{0, 1, 1, 3}, {0, 3, 1, 2}, {2, 1, 3, 0}, {2, 3, 3, 2}};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      P(a[q][0], a[q][1], r0, i0);
+      P(a[q][2], a[q][3], r1, i1);
+      cr[q] = -(i0 - i1);
+      ci[q] = r0 - r1;
+    }
+  } else {  // Q or U: D = first pair difference, S = second pair sum
+    const int d[4][4] = {{0, 0, 1, 1}, {0, 2, 1, 3}, {2, 0, 3, 1}, {2, 2, 3, 3}};
+    const int sm[4][4] = {{1, 0, 0, 1}, {1, 2, 0, 3}, {3, 0, 2, 1}, {3, 2, 2, 3}};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      P(d[q][0], d[q][1], r0, i0);
+      P(d[q][2], d[q][3], r1, i1);
+      const float Dr = r0 - r1, Di = i0 - i1;
+      P(sm[q][0], sm[q][1], r0, i0);
+      P(sm[q][2], sm[q][3], r1, i1);
+      const float Sr = r0 + r1, Si = i0 + i1;
+      if (p.stokType == 2) {
+        cr[q] = p.c2p * Dr - p.s2p * Sr;
+        ci[q] = p.c2p * Di - p.s2p * Si;
+      } else {
+        cr[q] = p.c2p * Sr + p.s2p * Dr;
+        ci[q] = p.c2p * Si + p.s2p * Di;
+      }
+    }
+  }
 }
 
 template <int MODE>
@@ -111,15 +165,8 @@ __global__ void __launch_bounds__(256) dft_beam_kernel(const __grid_constant__ B
       const float4 b1 = __ldg(reinterpret_cast<const float4*>(J2 + 4));
       const float J1r[4] = {a0.x, a0.z, a1.x, a1.z}, J1i[4] = {a0.y, a0.w, a1.y, a1.w};
       const float J2r[4] = {b0.x, b0.z, b1.x, b1.z}, J2i[4] = {b0.y, b0.w, b1.y, b1.w};
-      float cr[4] = {0.f, 0.f, 0.f, 0.f}, ci[4] = {0.f, 0.f, 0.f, 0.f};
-      pconj(J1r[0], J1i[0], J2r[0], J2i[0], cr[0], ci[0]);  // XX
-      pconj(J1r[1], J1i[1], J2r[1], J2i[1], cr[0], ci[0]);
-      pconj(J1r[1], J1i[1], J2r[3], J2i[3], cr[1], ci[1]);  // XY
-      pconj(J1r[0], J1i[0], J2r[2], J2i[2], cr[1], ci[1]);
-      pconj(J1r[2], J1i[2], J2r[0], J2i[0], cr[2], ci[2]);  // YX
-      pconj(J1r[3], J1i[3], J2r[1], J2i[1], cr[2], ci[2]);
-      pconj(J1r[2], J1i[2], J2r[2], J2i[2], cr[3], ci[3]);  // YY
-      pconj(J1r[3], J1i[3], J2r[3], J2i[3], cr[3], ci[3]);
+      float cr[4], ci[4];
+      beam_coeffs(p, J1r, J1i, J2r, J2i, cr, ci);
       float4* d = reinterpret_cast<float4*>(sC + ((size_t)pr * p.ct + c) * crow + j * 8);
       d[0] = make_float4(cr[0], ci[0], cr[1], ci[1]);
       d[1] = make_float4(cr[2], ci[2], cr[3], ci[3]);

@@ -28,6 +28,8 @@ struct BeamKParams {
   const float* comps;            // device: ncomp records of cstride floats
   int ncomp, cstride, ct, nterm, mode;
   int* errFlag;                  // set to 3 for a record whose antennas are outside the table
+  int stokType;                  // sky Stokes: 1 I, 2 Q, 3 U, 4 V
+  float c2p, s2p;                // cos, sin of twice the parallactic angle (Q, U)
 };
 
 // Shared memory of one launch: the component tile and its Jones coefficients

@@ -42,7 +42,8 @@ int fail(int code, const std::string& msg) {
 struct BeamState {
   bool on = false;
   int numAnt = 0, numAntType = 0, numJChan = 0, ilocb = -1, iloca1 = -1, iloca2 = -1;
-  int jonesComps = 0;
+  int jonesComps = 0, stokType = 1;
+  float c2p = 1.f, s2p = 0.f;
   const float* jones = nullptr;
   int* d_antType = nullptr;
   int* d_jchan = nullptr;
@@ -206,6 +207,9 @@ int ensure_plan(GPUInfo* g, State* s) {
     k.nterm = s->mc.model.nterm;
     k.mode = s->mc.model.kind;
     k.errFlag = s->d_err;
+    k.stokType = b.stokType;
+    k.c2p = b.c2p;
+    k.s2p = b.s2p;
   }
   s->planValid = true;
   return OBIT_DFT_OK;
@@ -327,7 +331,8 @@ int obit_dft_set_beam(GPUInfo* g, const ObitDFTBeam* beam) {
   }
   const GPUVisInfo* v = g->h_visInfo;
   if (!v) return fail(OBIT_DFT_EBADARG, "GPUInfo.h_visInfo is NULL (call Init first)");
-  if (beam->stokType != 1) return fail(OBIT_DFT_EUNSUPPORTED, "only Stokes I beam models are supported");
+  if (beam->stokType < 1 || beam->stokType > 4)
+    return fail(OBIT_DFT_EUNSUPPORTED, "Stokes type must be 1..4 (I, Q, U, V)");
   if (beam->numAnt < 1 || beam->numAntType < 1 || beam->numJChan < 1 || !beam->antType || !beam->jchan ||
       !beam->jones || beam->jonesComps < 1)
     return fail(OBIT_DFT_EBADARG, "incomplete beam description");
@@ -359,6 +364,9 @@ int obit_dft_set_beam(GPUInfo* g, const ObitDFTBeam* beam) {
   b.iloca2 = beam->iloca2;
   b.jones = beam->jones;
   b.jonesComps = beam->jonesComps;
+  b.stokType = beam->stokType;
+  b.c2p = (float)std::cos(2.0 * (double)beam->parAng);
+  b.s2p = (float)std::sin(2.0 * (double)beam->parAng);
   b.on = true;
   s->planValid = false;
   return OBIT_DFT_OK;

@@ -178,7 +178,7 @@ class OracleBeam(C.Structure):
         ("numAnt", C.c_int), ("numAntType", C.c_int), ("numJChan", C.c_int),
         ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
         ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int),
-        ("jones", C.POINTER(C.c_float)),
+        ("jones", C.POINTER(C.c_float)), ("stokType", C.c_int), ("c2p", C.c_double), ("s2p", C.c_double),
     ]
 
 
@@ -196,8 +196,11 @@ def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None):
     jc = np.ascontiguousarray(beam.jchan, dtype=np.int32)
     jo = np.ascontiguousarray(beam.jones, dtype=np.float32)
     assert jo.shape[1] >= sky.ncomp
+    # the parallactic terms as the library forms them (FP64 sin/cos, rounded to float)
+    c2p = float(np.float32(np.cos(2.0 * float(beam.parAng))))
+    s2p = float(np.float32(np.sin(2.0 * float(beam.parAng))))
     ob = OracleBeam(len(at), jo.shape[0], jo.shape[2], _p(at, C.c_int), _p(jc, C.c_int), beam.ilocb,
-                    beam.iloca1, beam.iloca2, _p(jo, C.c_float))
+                    beam.iloca1, beam.iloca2, _p(jo, C.c_float), int(beam.stokType), c2p, s2p)
     # the oracle indexes the table with the model's component count
     if jo.shape[1] != sky.ncomp:
         jo = np.ascontiguousarray(jo[:, :sky.ncomp])

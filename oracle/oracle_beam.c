@@ -1,13 +1,13 @@
 /* Test infrastructure (never linked into the product): FP64 oracle of the
  * beam-corrected DFT, the model of ObitCUDABeamModel's beam*Kernel family
- * (ObitSystem/Obit/src/ObitCUDABeamModel.cu:139-1226) for a Stokes I sky and
- * linear feeds.
+ * (ObitSystem/Obit/src/ObitCUDABeamModel.cu:139-1226) for linear feeds and a
+ * Stokes I, Q, U or V sky.
  *
  * For a record of baseline (a1, a2) with antenna types t1, t2 and a (channel,
  * IF) whose Jones plane is jc, each component contributes v = amp e^{i phase}
  * (amplitude and phase as in the DFT oracle, oracle_comp_term) times the
- * coefficients of cudaJonesCor1_Lin_I (ObitSystem/Obit/include/CUDALinCorSum.h:104-134),
- * with J1 = Jones[t1][c][jc], J2 = Jones[t2][c][jc] and P(i, j) = J1[i] conj(J2[j]):
+ * coefficients of its Stokes (beam_coeffs below) with J1 = Jones[t1][c][jc],
+ * J2 = Jones[t2][c][jc] and P(i, j) = J1[i] conj(J2[j]); for Stokes I
  *   XX: P(0,0) + P(1,1)   XY: P(1,3) + P(0,2)   YX: P(2,0) + P(3,1)   YY: P(2,2) + P(3,3)
  * Antenna numbers come from the BASELINE random parameter (256 a1 + a2, plus a
  * subarray fraction) or from ANTENNA1/ANTENNA2, as GetAnts does
@@ -45,6 +45,56 @@ static int beam_ants(const OracleBeam *b, const float *rec, int *a1, int *a2) {
   return *a1 >= 0 && *a1 < b->numAnt && *a2 >= 0 && *a2 < b->numAnt;
 }
 
+/* Coefficients of the four model correlations (XX, XY, YX, YY) for one
+ * component from P(i, j) = J1[i] conj(J2[j]), as cudaJonesCor1_Lin_{I,Q,U,V}
+ * (ObitSystem/Obit/include/CUDALinCorSum.h:104-455) and the CPU
+ * ObitSkyModelVMBeamJonesCorSum (ObitSystem/Obit/src/ObitSkyModelVMBeam.c:1117-1240)
+ * form them. */
+static void beam_coeffs(const OracleBeam *b, const float *J1, const float *J2, double cr[4],
+                        double ci[4]) {
+  double pr[4][4], pi[4][4];
+  for (int x = 0; x < 4; x++)
+    for (int y = 0; y < 4; y++) {
+      pr[x][y] = (double)J1[2 * x] * J2[2 * y] + (double)J1[2 * x + 1] * J2[2 * y + 1];
+      pi[x][y] = (double)J1[2 * x + 1] * J2[2 * y] - (double)J1[2 * x] * J2[2 * y + 1];
+    }
+  /* the (a, b) terms of each correlation: XX (0,0)(1,1) ...; see the table below */
+  static const int A[4][4] = {{0, 1, 1, 0}, {0, 1, 1, 0}, {2, 3, 3, 2}, {2, 3, 3, 2}};
+  static const int B[4][4] = {{0, 1, 0, 1}, {2, 3, 2, 3}, {0, 1, 0, 1}, {2, 3, 2, 3}};
+  /* per correlation q: D = P(A0,B0) - P(A1,B1) ("difference"), S = P(A2,B2) + P(A3,B3) ("sum") */
+  for (int q = 0; q < 4; q++) {
+    const double Dr = pr[A[q][0]][B[q][0]] - pr[A[q][1]][B[q][1]];
+    const double Di = pi[A[q][0]][B[q][0]] - pi[A[q][1]][B[q][1]];
+    const double Sr = pr[A[q][2]][B[q][2]] + pr[A[q][3]][B[q][3]];
+    const double Si = pi[A[q][2]][B[q][2]] + pi[A[q][3]][B[q][3]];
+    switch (b->stokType) {
+      case 2: /* Q: c2p D - s2p S */
+        cr[q] = b->c2p * Dr - b->s2p * Sr;
+        ci[q] = b->c2p * Di - b->s2p * Si;
+        break;
+      case 3: /* U: c2p S + s2p D */
+        cr[q] = b->c2p * Sr + b->s2p * Dr;
+        ci[q] = b->c2p * Si + b->s2p * Di;
+        break;
+      default: break;
+    }
+  }
+  if (b->stokType == 1) { /* I: XX P00+P11, XY P13+P02, YX P20+P31, YY P22+P33 */
+    cr[0] = pr[0][0] + pr[1][1]; ci[0] = pi[0][0] + pi[1][1];
+    cr[1] = pr[1][3] + pr[0][2]; ci[1] = pi[1][3] + pi[0][2];
+    cr[2] = pr[2][0] + pr[3][1]; ci[2] = pi[2][0] + pi[3][1];
+    cr[3] = pr[2][2] + pr[3][3]; ci[3] = pi[2][2] + pi[3][3];
+  } else if (b->stokType == 4) { /* V: i (P01-P13), i (P03-P12), i (P21-P30), i (P23-P32) */
+    const int a0[4] = {0, 0, 2, 2}, b0[4] = {1, 3, 1, 3}, a1[4] = {1, 1, 3, 3}, b1[4] = {3, 2, 0, 2};
+    for (int q = 0; q < 4; q++) {
+      const double dr = pr[a0[q]][b0[q]] - pr[a1[q]][b1[q]];
+      const double di = pi[a0[q]][b0[q]] - pi[a1[q]][b1[q]];
+      cr[q] = -di;
+      ci[q] = dr;
+    }
+  }
+}
+
 /* model correlation (0 XX, 1 XY, 2 YX, 3 YY) of record polarization p (XX, YY, XY, YX) */
 static const int kModelOf[4] = {0, 3, 1, 2};
 
@@ -78,15 +128,8 @@ static void *beam_slice(void *arg) {
           const double vr = amp * cos(ph), vi = amp * sin(ph);
           const float *J1 = b->jones + (((size_t)t1 * j->ncomp + ic) * b->numJChan + jc) * 8;
           const float *J2 = b->jones + (((size_t)t2 * j->ncomp + ic) * b->numJChan + jc) * 8;
-          /* P(x, y) = J1[x] conj(J2[y]) */
-#define PR(x, y) ((double)J1[2 * (x)] * J2[2 * (y)] + (double)J1[2 * (x) + 1] * J2[2 * (y) + 1])
-#define PI(x, y) ((double)J1[2 * (x) + 1] * J2[2 * (y)] - (double)J1[2 * (x)] * J2[2 * (y) + 1])
-          const double cr[4] = {PR(0, 0) + PR(1, 1), PR(1, 3) + PR(0, 2), PR(2, 0) + PR(3, 1),
-                                PR(2, 2) + PR(3, 3)};
-          const double ci[4] = {PI(0, 0) + PI(1, 1), PI(1, 3) + PI(0, 2), PI(2, 0) + PI(3, 1),
-                                PI(2, 2) + PI(3, 3)};
-#undef PR
-#undef PI
+          double cr[4], ci[4];
+          beam_coeffs(b, J1, J2, cr, ci);
           for (int q = 0; q < 4; q++) {
             mr[q] += cr[q] * vr - ci[q] * vi;
             mi[q] += cr[q] * vi + ci[q] * vr;
@@ -122,6 +165,7 @@ static void *beam_slice(void *arg) {
 int oracle_beam_apply(const OracleJob *j, const OracleBeam *b, float *vis, double *l1, int nthreads) {
   if (j->modType < ORACLE_POINT || j->modType > ORACLE_GAUSS_TSPEC) return -1;
   if (j->numberPoln < 1 || j->numberPoln > 4) return -2;
+  if (b->stokType < 1 || b->stokType > 4) return -3;
   if (j->nvis <= 0 || j->ncomp <= 0) return 0;
   if (nthreads < 1) nthreads = 1;
   if (nthreads > j->nvis) nthreads = j->nvis;

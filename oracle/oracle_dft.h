@@ -98,6 +98,8 @@ typedef struct OracleBeam {
   int ilocb;            /* BASELINE offset in the record, or -1 */
   int iloca1, iloca2;   /* ANTENNA1 / ANTENNA2 offsets when ilocb < 0 */
   const float *jones;   /* [numAntType][ncomp][numJChan][8]: XX, XY, YX, YY complex */
+  int stokType;         /* 1..4 = I, Q, U, V sky */
+  double c2p, s2p;      /* cos, sin of twice the parallactic angle (Q, U) */
 } OracleBeam;
 
 /* Applies the beam-corrected FP64 model (Stokes I, linear feeds) to the

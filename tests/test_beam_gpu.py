@@ -1,8 +1,9 @@
 """Beam-corrected DFT (obit_dft_set_beam) on a B200 against the FP64 beam
 oracle: random Jones matrices per antenna type, component and Jones plane,
 2 or 4 correlations, subtract / replace / divide with flags, every model
-family; unit Jones matrices reproduce the plain sky model; a record whose
-antennas fall outside the table is reported and left untouched."""
+family, Stokes I, Q, U and V skies; unit Jones matrices reproduce the plain
+sky model; a record whose antennas fall outside the table is reported and
+left untouched."""
 import numpy as np
 import pytest
 
@@ -115,7 +116,7 @@ def test_beam_description_is_validated():
         from obit_b200.beam import Beam
         for b, msg in ((Beam(bad_type, beam.jchan, beam.jones), "antenna type"),
                        (Beam(beam.antType, beam.jchan + 5, beam.jones), "Jones plane"),
-                       (Beam(beam.antType, beam.jchan, beam.jones, stokType=2), "Stokes I")):
+                       (Beam(beam.antType, beam.jchan, beam.jones, stokType=5), "Stokes type")):
             with pytest.raises(_lib.DFTError) as e:
                 gm.set_beam(b, d_jones.data_ptr())
             assert msg in str(e.value)
@@ -131,6 +132,18 @@ def test_beam_nonuniform_channels_take_the_direct_form():
     uv, sky, beam = beam_case(nstok=4, nrow=40, nchan=24, nif=2, ncomp=100, seed=19, flag_frac=0.1)
     rng = np.random.default_rng(3)
     uv.freqArr = np.sort(uv.freqArr + rng.uniform(-3e5, 3e5, uv.freqArr.shape))
+    p = SkyModelParams(op=OP_SUB)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
+
+
+@pytest.mark.parametrize("stok", [2, 3, 4])
+def test_beam_polarized_skies(stok):
+    """Stokes Q, U (with a parallactic angle) and V skies."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=4, nrow=50, nchan=20, nif=2, ncomp=110, seed=23 + stok, flag_frac=0.1,
+                              stok=stok, par_ang=0.61)
     p = SkyModelParams(op=OP_SUB)
     got = _run_beam(uv, sky, p, beam, torch)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
