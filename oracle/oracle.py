@@ -20,6 +20,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_A = HERE / "liboracle_dft.so"
 LIB_B = HERE / "_ref" / "libobit_refcpu.so"
+LIB_J = HERE / "_ref" / "libobit_refjones.so"
 
 
 class OracleJob(C.Structure):
@@ -216,6 +217,43 @@ def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None):
     if rc:
         raise ValueError(f"oracle_beam_apply returned {rc}")
     return out, l1.reshape(uv.nvis, uv.nif, uv.nchan, 4)
+
+
+def beam_coeffs(stok: int, c2p: float, s2p: float, J1, J2):
+    """The beam oracle's four model coefficients (XX, XY, YX, YY) of one Jones
+    pair (8 floats each): complex128 (4,)."""
+    lib = lib_a()
+    lib.oracle_beam_coeffs.restype = None
+    lib.oracle_beam_coeffs.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_float),
+                                       C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    a = np.ascontiguousarray(J1, dtype=np.float32)
+    b = np.ascontiguousarray(J2, dtype=np.float32)
+    cr, ci = np.zeros(4), np.zeros(4)
+    lib.oracle_beam_coeffs(stok, c2p, s2p, _p(a, C.c_float), _p(b, C.c_float), _p(cr, C.c_double),
+                           _p(ci, C.c_double))
+    return cr + 1j * ci
+
+
+def have_refjones() -> bool:
+    return LIB_J.exists()
+
+
+def ref_jones_cor1(stok: int, flux: float, sin_ph: float, cos_ph: float, J1, J2, c2p: float, s2p: float):
+    """The reference's own cudaJonesCor1_Lin_{I,Q,U,V} for one component (compiled
+    for the host): the XX, XY, YX, YY sums as complex128 (4,)."""
+    lib = C.CDLL(str(LIB_J))
+    lib.ref_jones_cor1.restype = C.c_int
+    lib.ref_jones_cor1.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), C.c_float, C.c_float, C.POINTER(C.c_float)]
+    a = np.ascontiguousarray(J1, dtype=np.float32)
+    b = np.ascontiguousarray(J2, dtype=np.float32)
+    out = np.zeros(8, np.float32)
+    rc = lib.ref_jones_cor1(stok, flux, sin_ph, cos_ph, _p(a, C.c_float), _p(b, C.c_float), c2p, s2p,
+                            _p(out, C.c_float))
+    if rc:
+        raise ValueError(f"ref_jones_cor1 returned {rc}")
+    o = out.astype(np.float64)
+    return o[0::2] + 1j * o[1::2]
 
 
 def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):

@@ -20,6 +20,7 @@
 #include <math.h>
 #include <pthread.h>
 #include <stdlib.h>
+#include <string.h>
 
 #include "oracle_dft.h"
 
@@ -93,6 +94,18 @@ static void beam_coeffs(const OracleBeam *b, const float *J1, const float *J2, d
       ci[q] = dr;
     }
   }
+}
+
+/* The coefficients for one Jones pair, exported for the check against the
+ * reference's own cudaJonesCor1_Lin_* (oracle/refjones.cpp). */
+void oracle_beam_coeffs(int stokType, double c2p, double s2p, const float *J1, const float *J2,
+                        double *cr, double *ci) {
+  OracleBeam b;
+  memset(&b, 0, sizeof(b));
+  b.stokType = stokType;
+  b.c2p = c2p;
+  b.s2p = s2p;
+  beam_coeffs(&b, J1, J2, cr, ci);
 }
 
 /* model correlation (0 XX, 1 XY, 2 YX, 3 YY) of record polarization p (XX, YY, XY, YX) */

@@ -110,6 +110,11 @@ typedef struct OracleBeam {
 int oracle_beam_apply(const OracleJob *job, const OracleBeam *beam, float *vis, double *l1,
                       int nthreads);
 
+/* The four model coefficients (XX, XY, YX, YY) of one Jones pair for Stokes
+ * 1..4 (the step oracle_beam_apply takes per component). */
+void oracle_beam_coeffs(int stokType, double c2p, double s2p, const float *J1, const float *J2,
+                        double *cr, double *ci);
+
 #ifdef __cplusplus
 }
 #endif

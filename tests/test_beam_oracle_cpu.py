@@ -108,3 +108,22 @@ def test_subtract_leaves_flagged_correlations():
     flagged = src[..., 2] <= 0
     assert flagged.any() and np.array_equal(v[flagged], src[flagged])
     assert not np.array_equal(v[~flagged], src[~flagged])
+
+
+@pytest.mark.skipif(not oracle.have_refjones(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("stok", [1, 2, 3, 4])
+def test_coefficients_match_the_reference_code(stok):
+    """The oracle's coefficients times the component term equal the sums of the
+    reference's own cudaJonesCor1_Lin_{I,Q,U,V}, compiled for the host from its
+    header (oracle/refjones.cpp), for random Jones pairs and parallactic angles."""
+    r = np.random.default_rng(40 + stok)
+    for _ in range(50):
+        J1 = r.standard_normal(8).astype(np.float32)
+        J2 = r.standard_normal(8).astype(np.float32)
+        flux, ph, pa = float(r.uniform(0.1, 2.0)), float(r.uniform(-np.pi, np.pi)), float(r.uniform(0, np.pi))
+        c2p, s2p = float(np.float32(np.cos(2 * pa))), float(np.float32(np.sin(2 * pa)))
+        s, c = float(np.float32(np.sin(ph))), float(np.float32(np.cos(ph)))
+        want = oracle.ref_jones_cor1(stok, flux, s, c, J1, J2, c2p, s2p)
+        got = oracle.beam_coeffs(stok, c2p, s2p, J1, J2) * (flux * (c + 1j * s))
+        scale = flux * np.abs(J1).sum() * np.abs(J2).sum()
+        assert np.max(np.abs(got - want)) < 1e-6 * scale
