@@ -157,3 +157,27 @@ def test_log_frequency_quadratic_fits(harness, nterm):
 def test_rejects_bad_selection(harness):
     assert plan(harness, nchan=16, chanb=4, chane=20)["rc"] == 3
     assert plan(harness, nchan=16, K=3)["rc"] == 3
+
+
+def test_default_cta_size_for_short_rows(harness):
+    """Left to the planner (threads 0), recurrence plans take 128-thread CTAs
+    when the rows have at most two channel blocks (a 256-thread tile would
+    span 128 rows), 256 otherwise; the plain comparator keeps 256."""
+    p = plan(harness, nchan=64, nif=1, threads=0)  # 2 blocks of 32
+    assert p["rc"] == 0 and p["threads"] == 128 and p["Bt"] == 2 and p["R"] == 64
+    p = plan(harness, nchan=256, nif=4, threads=0)
+    assert p["rc"] == 0 and p["threads"] == 256
+    p = plan(harness, nchan=64, nif=1, threads=0, flavor=1)
+    assert p["rc"] == 0 and p["threads"] == 256
+
+
+def test_factored_point_tiles_keep_128_components(harness):
+    """The factored point kernels (compensation terms and s^8 in shared memory,
+    plus the low-part region) still take 128-component tiles at the tile
+    shapes the autotuner and planner use: two 128-thread CTAs per SM (110 KB
+    each) and one 256-thread CTA (200 KB)."""
+    p = plan(harness, kind=0, lcomp=4, nchan=256, nif=1, threads=128, Bt=8, ct=128)
+    assert p["rc"] == 0 and p["K"] == 32 and p["R"] == 16 and p["ct"] == 128
+    assert p["smem"] <= 110 * 1024
+    p = plan(harness, kind=0, lcomp=4, nchan=512, nif=8, threads=256, Bt=16, ct=128)
+    assert p["rc"] == 0 and p["ct"] == 128 and p["smem"] <= 200 * 1024
