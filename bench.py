@@ -36,6 +36,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 FLOPS_PER_EVAL = 10.0  # complex rotate (6) + accumulate (4), algorithmic
+# one metric string for every arm and workload, so that lines can be compared
+METRIC = "component-visibility evals/s (DFT subtract)"
+# parity bound of every GPU line, checked against the FP64 oracle by the -m gpu tests
+ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per visibility",
+            "checked_by": "tests/test_configs_gpu.py, tests/test_dft_gpu.py (-m gpu)"}
 # DRAM bytes (read + write) per record of a workload's records, each from one ncu
 # capture of the recurrence kernel on a smaller case of the same layout; traffic
 # grows in proportion to records, so a launch's traffic is the figure times its
@@ -68,7 +73,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-peak", action="store_true", help="skip the SGEMM FP32 peak measurement")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="CPU work of the cpu_baseline leg's sample")
+    ap.add_argument("--cpu-step-seconds", type=float, default=2.0,
+                    help="reference arm: CPU work per step (the row sample is sized to it)")
     ap.add_argument("--workload", default="config2",
                     choices=["config1", "config2", "config3", "config4", "config5"],
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
@@ -77,7 +85,10 @@ def parse():
                     help="config5: fraction of each facet's drawn rows held in HBM")
     ap.add_argument("--no-autotune", action="store_true", help="config5: keep the planner's tile")
     ap.add_argument("--no-compare", action="store_true",
-                    help="config5: skip the per-facet comparator launches")
+                    help="skip the comparators (config2-4: the FP64-phase plain kernel on the same "
+                         "records and a short config-5 batch pass; config5: the per-facet launches)")
+    ap.add_argument("--compare-row-scale", type=float, default=0.01,
+                    help="row scale of the config-5 batch pass among the comparators")
     return ap.parse_args()
 
 
@@ -260,85 +271,102 @@ def fp32_peak_tflops(torch, device) -> float:
 # ---- CPU baseline ------------------------------------------------------------------
 
 
-def cpu_baseline(g: Geometry, seconds: float):
+def host_info() -> dict:
+    """Host cores usable by this process and the CPU model."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": len(os.sched_getaffinity(0)), "cpu_model": model}
+
+
+class CpuDFT:
     """Reference CPU DFT restatement (oracle/_ref: the reference's ObitSinCosVec /
     ObitExpVec, FP32 phase, rows split over pthreads as ObitSkyModelFTDFT) on a
-    bounded sample of the same workload; returns (evals/s, cores, sample text, kind)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle
-    from obit_b200 import uvdata as U
-    from obit_b200.skymodel import SkyModelParams
+    row sample of the workload, on every host core.  Used by the cpu_baseline leg
+    and by the reference arm, with the same sizing rule: the sample is grown from
+    one row per core until one pass takes about `seconds`."""
 
-    cores = oracle.nthreads_default()
-    have_ref = oracle.have_refcpu()
-    kind = "port"
+    def __init__(self, g: Geometry, seconds: float):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        from obit_b200 import uvdata as U
+        from obit_b200.skymodel import SkyModelParams
 
-    sky = g.sky
+        self.g = g
+        self.cores = oracle.nthreads_default()
+        self.have_ref = oracle.have_refcpu()
+        self._fn = oracle.apply_refcpu if self.have_ref else oracle.apply_fp64
+        self._params = SkyModelParams()
+        self._U = U
+        nrow = self.cores
+        self._set_rows(nrow)
+        dt = self.run()
+        if dt < seconds / 2:
+            nrow = max(self.cores, int(nrow * seconds / max(dt, 1e-3)))
+            nrow = min(self.cores * ((nrow + self.cores - 1) // self.cores), g.rows)
+            self._set_rows(nrow)
 
-    def run(nrow):
-        uv = U.make_uvdata(g.uvw[:nrow], g.nstok, g.nchan, g.nif, g.freq, g.fa,
-                           np.random.default_rng(9))
+    def _set_rows(self, nrow: int):
+        g = self.g
+        self.nrow = nrow
+        self.uv = self._U.make_uvdata(g.uvw[:nrow], g.nstok, g.nchan, g.nif, g.freq, g.fa,
+                                      np.random.default_rng(9))
+        self.evals = nrow * g.channels * g.sky.ncomp
+
+    def run(self) -> float:
+        """One pass over the sample; wall seconds."""
         t0 = time.perf_counter()
-        if have_ref:
-            oracle.apply_refcpu(uv, sky, SkyModelParams(), nthreads=cores)
-        else:
-            oracle.apply_fp64(uv, sky, SkyModelParams(), nthreads=cores)
+        self._fn(self.uv, self.g.sky, self._params, nthreads=self.cores)
         return time.perf_counter() - t0
 
-    nrow = cores
-    dt = run(nrow)
-    if dt < seconds / 3:
-        nrow = max(cores, int(nrow * (seconds / max(dt, 1e-3))))
-        nrow = min(nrow, g.rows)
-        dt = run(nrow)
-    evals = nrow * g.channels * sky.ncomp
-    name = ("restatement of the reference CPU DFT loop (FP32 phase) linked with the reference's own "
-            "ObitSinCosVec/ObitExpVec compiled from its sources") if have_ref \
-        else "FP64 oracle (reference vector math not built)"
-    return (evals / dt, cores,
-            f"{nrow} rows x {g.channels} channels x {sky.ncomp} components ({name}), {dt:.1f} s", kind)
+    def sample(self) -> str:
+        g = self.g
+        what = ("restatement of the reference CPU DFT loop (FP32 phase) linked with the reference's own "
+                "ObitSinCosVec/ObitExpVec compiled from its sources") if self.have_ref \
+            else "FP64 oracle (reference vector math not built)"
+        return (f"{self.nrow} rows x {g.channels} channels x {g.sky.ncomp} components per pass ({what}), "
+                f"{self.cores} threads")
+
+
+def cpu_baseline(g: Geometry, seconds: float):
+    """The cpu_baseline leg: one sized pass of CpuDFT; returns (evals/s, cores,
+    sample text, kind)."""
+    c = CpuDFT(g, seconds)
+    dt = c.run()
+    return c.evals / dt, c.cores, f"{c.sample()}, {dt:.1f} s", "port"
 
 
 # ---- arms ------------------------------------------------------------------------
 
 
 def run_reference(args):
+    """Reference arm: the reference CPU DFT restatement on every host core, each
+    step one pass over a row sample of the same workload (about
+    --cpu-step-seconds of CPU work)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     g = workload_geometry(args.workload, 0, args.rows, args.ncomp)
-    sky = g.sky
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle
-    from obit_b200 import uvdata as U
-    from obit_b200.skymodel import SkyModelParams
-
-    cores = oracle.nthreads_default()
-    have_ref = oracle.have_refcpu()
-    nrow = max(cores, 8)
-    uv = U.make_uvdata(g.uvw[:nrow], g.nstok, g.nchan, g.nif, g.freq, g.fa, np.random.default_rng(9))
-    fn = oracle.apply_refcpu if have_ref else oracle.apply_fp64
+    c = CpuDFT(g, args.cpu_step_seconds)
     for _ in range(args.warmup):
-        fn(uv, sky, SkyModelParams(), nthreads=cores)
-    ts = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        fn(uv, sky, SkyModelParams(), nthreads=cores)
-        ts.append(time.perf_counter() - t0)
-    evals = nrow * g.channels * sky.ncomp
-    v = evals * len(ts) / sum(ts) / 1e9
+        c.run()
+    ts = [c.run() for _ in range(args.steps)]
+    v = c.evals * len(ts) / sum(ts) / 1e9
     line = {
-        "impl": "reference", "metric": "component-visibility evals/s (DFT subtract)",
+        "impl": "reference", "metric": METRIC,
         "value": v, "unit": "Gevals/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(ts) / len(ts), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (FP32 phase, FP64 component sum)", "data": "synthetic",
-        "config": config_block(g, nrow_override=nrow),
-        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": cores,
-                         "kind": "port",
-                         "sample": f"{nrow} rows x {g.channels} channels x {sky.ncomp} components per step "
-                                   "(restatement of the reference CPU DFT loop linked with the reference's "
-                                   "own ObitSinCosVec/ObitExpVec)" if have_ref else
-                                   f"{nrow} rows x {g.channels} channels x {sky.ncomp} components per step (FP64 oracle)"},
+        "config": {**config_block(g, nrow_override=c.nrow), "l2": "not applicable (host cores)"},
+        "host": host_info(),
+        "cpu_baseline": {"value": v, "unit": "Gevals/s", "cores": c.cores, "kind": "port",
+                         "sample": c.sample()},
         "e2e": {"value": v, "unit": "Gevals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -397,91 +425,125 @@ def config5_data(torch, device, row_scale: float, seed: int = 5):
     return facets, keep, full_evals
 
 
+def _timed_on(torch, stream, fn, steps, warmup, after=None):
+    """Total and per-step CUDA-event milliseconds of `steps` calls of fn on stream."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per = []
+    e0.record(stream)
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        per.append((a, b))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if after:
+        after()
+    return e0.elapsed_time(e1), [a.elapsed_time(b) for a, b in per]
+
+
+def config5_measure(torch, device, row_scale, steps, warmup, autotune=True, tile=None,
+                    compare=True, sampler=None):
+    """The 96-facet batch: one graph launch of the persistent batched kernel per
+    step (autotuned tile unless `tile` fixes it), and, with `compare`, one launch
+    per facet of the recurrence and of the FP64-phase plain kernel.  Returns a
+    dict of the measurements."""
+    from obit_b200 import _lib
+    from obit_b200.batch import DFTBatch
+
+    facets, keep, full_evals = config5_data(torch, device, row_scale)
+    batch = DFTBatch(facets)
+    try:
+        info0 = batch.info()
+        stream = torch.cuda.Stream(device=device)
+        sp = stream.cuda_stream
+        t0 = time.perf_counter()
+        if tile:
+            batch.set_tile(*tile)
+        tuned = batch.autotune(sp) if (autotune and not tile) else None
+        torch.cuda.synchronize()
+        tune_s = time.perf_counter() - t0
+        info = batch.info()
+        evals = info["evals"]
+        if sampler is not None:
+            with sampler:
+                t_ms, per = _timed_on(torch, stream, lambda: batch.run(sp), steps, warmup, batch.check)
+        else:
+            t_ms, per = _timed_on(torch, stream, lambda: batch.run(sp), steps, warmup, batch.check)
+        out = {"evals": evals, "full_evals": full_evals, "t_ms": t_ms, "per_ms": per,
+               "rows": sum(f.nvis for f in facets), "info": info, "info0": info0, "tuned": tuned,
+               "tune_s": tune_s, "batch_gevals_s": evals * steps / (t_ms * 1e-3) / 1e9}
+        if compare:
+            r_ms, _ = _timed_on(torch, stream, lambda: batch.run_per_facet(_lib.OBIT_DFT_RECUR, sp), 1, 1,
+                                batch.check)
+            p_ms, _ = _timed_on(torch, stream, lambda: batch.run_per_facet(_lib.OBIT_DFT_PLAIN, sp), 1, 0,
+                                batch.check)
+            out["per_facet_recur_gevals_s"] = evals / (r_ms * 1e-3) / 1e9
+            out["per_facet_plain_gevals_s"] = evals / (p_ms * 1e-3) / 1e9
+            out["batch_vs_per_facet_plain"] = out["batch_gevals_s"] / out["per_facet_plain_gevals_s"]
+            out["batch_vs_per_facet_recur"] = out["batch_gevals_s"] / out["per_facet_recur_gevals_s"]
+        return out
+    finally:
+        batch.close()
+        del keep
+        torch.cuda.empty_cache()
+
+
 def run_config5(args):
     """One step = one pass of the DFT subtract over all 96 facets: one graph
     launch of the persistent batched kernel (autotuned tile), against one
     launch per facet of the recurrence and of the FP64-phase plain kernel."""
     import torch
 
-    from obit_b200 import _lib
-    from obit_b200.batch import DFTBatch
-
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
-    facets, keep, full_evals = config5_data(torch, device, args.row_scale)
-    batch = DFTBatch(facets)
-    info0 = batch.info()
-    stream = torch.cuda.Stream(device=device)
-    sp = stream.cuda_stream
-    t0 = time.perf_counter()
     fixed = any((args.K, args.ct, args.Bt, args.threads))
-    if fixed:  # an explicit tile shape replaces the autotuner
-        batch.set_tile(args.K, args.ct, args.Bt, args.threads)
-    tuned = None if (args.no_autotune or fixed) else batch.autotune(sp)
-    torch.cuda.synchronize()
-    tune_s = time.perf_counter() - t0
-    info = batch.info()
-    evals = info["evals"]
-
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        per = []
-        e0.record(stream)
-        for _ in range(steps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fn()
-            b.record(stream)
-            per.append((a, b))
-        e1.record(stream)
-        torch.cuda.synchronize()
-        batch.check()
-        return e0.elapsed_time(e1), [a.elapsed_time(b) for a, b in per]
-
     sampler = ClockSampler(0)
-    with sampler:
-        t_ms, per = timed(lambda: batch.run(sp), args.steps, args.warmup)
+    m = config5_measure(torch, device, args.row_scale, args.steps, args.warmup,
+                        autotune=not args.no_autotune,
+                        tile=(args.K, args.ct, args.Bt, args.threads) if fixed else None,
+                        compare=not args.no_compare, sampler=sampler)
+    info, evals = m["info"], m["evals"]
+    t_ms, per = m["t_ms"], m["per_ms"]
     value = evals * args.steps / (t_ms * 1e-3)
-    comp = {}
-    if not args.no_compare:
-        r_ms, _ = timed(lambda: batch.run_per_facet(_lib.OBIT_DFT_RECUR, sp), 1, 1)
-        p_ms, _ = timed(lambda: batch.run_per_facet(_lib.OBIT_DFT_PLAIN, sp), 1, 0)
-        comp = {"per_facet_recur_gevals_s": evals / (r_ms * 1e-3) / 1e9,
-                "per_facet_plain_gevals_s": evals / (p_ms * 1e-3) / 1e9,
-                "batch_vs_per_facet_plain": (evals / (t_ms / args.steps * 1e-3)) / (evals / (p_ms * 1e-3))}
+    comp = {k: m[k] for k in ("per_facet_recur_gevals_s", "per_facet_plain_gevals_s",
+                              "batch_vs_per_facet_plain", "batch_vs_per_facet_recur") if k in m}
     peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
     achieved = evals * FLOPS_PER_EVAL / (statistics.mean(per) * 1e-3) / 1e12
     line = {
-        "metric": "component-visibility evals/s (batched DFT subtract, 96 uneven facets)",
+        "metric": METRIC,
         "value": value / 1e9, "unit": "Gevals/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (split-FP32 phase)",
         "data": "synthetic (seeded facet draw, noise visibilities, random point components)",
+        "accuracy": ACCURACY,
         "config": {"workload": f"config5: 96 facets, rows x {args.row_scale} of the drawn 1e5-1e7 "
                                "per facet held in HBM, 1-8 IF x 32-512 ch, 2 pol, 500-60000 point "
                                "components per facet",
-                   "evals_per_step": evals, "full_draw_evals": full_evals,
-                   "rows": sum(f.nvis for f in facets), "facets": info["facets"],
-                   "l2": "inputs larger than L2", "tile_planner": {k: info0[k] for k in ("K", "ct", "Bt", "R", "threads")},
-                   "tile_autotuned": tuned, "autotune_s": tune_s,
+                   "evals_per_step": evals, "full_draw_evals": m["full_evals"],
+                   "rows": m["rows"], "facets": info["facets"],
+                   "l2": "inputs larger than L2",
+                   "tile_planner": {k: m["info0"][k] for k in ("K", "ct", "Bt", "R", "threads")},
+                   "tile_autotuned": m["tuned"], "autotune_s": m["tune_s"],
                    "launch": f"1 CUDA graph launch per step ({info['launches']} persistent kernel(s), "
                              f"grid {info['grid']})"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak,
-                     "traffic": NCU_DRAM_BYTES_PER_RECORD["config5"][0] * sum(f.nvis for f in facets),
+                     "traffic": NCU_DRAM_BYTES_PER_RECORD["config5"][0] * m["rows"],
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per record ("
                                        + NCU_DRAM_BYTES_PER_RECORD["config5"][1] + ") x records per launch",
                      "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)"},
         "comparators": comp,
+        "host": host_info(),
         "cpu_baseline": None, "e2e": None,
         "gpu_launches": info["launches"] * args.steps,
         "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)
-    batch.close()
 
 
 def main():
@@ -603,6 +665,35 @@ def main():
                "h2d_bytes_per_step": rows * lrec * 4, "d2h_bytes_per_step": rows * lrec * 4,
                "timing": "wall clock around the synchronous C-ABI call, max over ranks"}
 
+    # comparators on one GPU, measured in the same run: the FP64-phase plain
+    # kernel on the same device-resident records, and a short pass of the
+    # multi-facet batch against one plain launch per facet
+    comp = None
+    if world == 1 and not args.no_compare:
+        comp = {}
+        if args.flavor == "recur":
+            gm.set_kernel(_lib.OBIT_DFT_PLAIN, 0, 0, 0, 0)
+            pt_ms, _ = _timed_on(torch, stream, lambda: gm.calc_device(d_vis.data_ptr(), rows, sp), 2, 1,
+                                 gm.check)
+            pl = evals * 2 / (pt_ms * 1e-3) / 1e9
+            gm.set_kernel(flavor, args.K, args.ct, args.Bt, args.threads)
+            comp["same_records"] = {
+                "plain_fp64_phase_gevals_s": pl, "recur_vs_plain": (value / 1e9) / pl,
+                "what": "FP64-phase plain kernel (one sin/cos per component-visibility) on the same "
+                        "records and model, 2 launches"}
+    if world == 1 and not args.no_compare and args.workload == "config2":
+        m = config5_measure(torch, device, args.compare_row_scale, 2, 1, autotune=True, compare=True)
+        comp["config5_batch"] = {
+            "what": f"config 5: 96 uneven facets, rows x {args.compare_row_scale} of the draw resident; "
+                    "one CUDA-graph launch of the persistent batch (autotuned tile) vs one launch "
+                    "per facet",
+            "evals_per_pass": m["evals"], "batch_gevals_s": m["batch_gevals_s"],
+            "per_facet_recur_gevals_s": m["per_facet_recur_gevals_s"],
+            "per_facet_plain_gevals_s": m["per_facet_plain_gevals_s"],
+            "batch_vs_per_facet_plain": m["batch_vs_per_facet_plain"],
+            "batch_vs_per_facet_recur": m["batch_vs_per_facet_recur"],
+            "tile_autotuned": m["tuned"]}
+
     line = None
     if rank == 0:
         peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
@@ -616,12 +707,13 @@ def main():
         kern = (f"{args.flavor} K={pi['K']} ct={pi['ct']} Bt={pi['Bt']} R={pi['R']} "
                 f"threads={pi['threads']}")
         line = {
-            "metric": "component-visibility evals/s (DFT subtract, max rel err <= 1e-5 vs FP64)",
+            "metric": METRIC,
             "value": value / 1e9, "unit": "Gevals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (split-FP32 phase)" if args.flavor == "recur" else "f32 (FP64 phase)",
             "data": "synthetic (seeded uvw, noise visibilities, random components)",
+            "accuracy": ACCURACY,
             "config": {**config_block(g, kernel=kern),
                        "timing": "sum of per-launch CUDA-event times, L2 flushed before each"
                        if flush is not None else "CUDA events around all steps"},
@@ -634,6 +726,8 @@ def main():
                                            + ") x records per launch",
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
                          "flops_per_eval": FLOPS_PER_EVAL},
+            "comparators": comp,
+            "host": host_info(),
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,

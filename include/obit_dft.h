@@ -268,10 +268,11 @@ int obit_dft_plan_info(GPUInfo *gpuInfo, int *info, int n);
  * place on `stream`.  Polarizations follow GPUModelInfo (stokFact, doSwap).
  * Scratch lives in a fixed 8 MiB device array inside the library (error flag,
  * channel blocks, padded component table): larger models are rejected with
- * OBIT_DFT_EUNSUPPORTED.  No cudaMalloc/cudaFree is called.  The first call on
- * a device resolves the array's address and should precede any stream capture.
- * All calls share the array: calls that overlap on the GPU race and must be
- * serialized.  Returns after the stream has completed the update. */
+ * OBIT_DFT_EUNSUPPORTED.  No cudaMalloc/cudaFree is called.  Device
+ * descriptors (freqScale, a device specIndex) are read in order on `stream`.
+ * The call is synchronous -- it waits for `stream` and returns after the update
+ * is complete -- and must never be made while a stream is capturing.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialized. */
 int obit_dft_calc_noalloc(const GPUVisInfo *visInfo, const GPUModelInfo *modelInfo,
                           const double *freqArr, double uvRefFreq, double modelRefFreq,
                           const double *specFreq, int nSpec, float *d_vis, int nvis,

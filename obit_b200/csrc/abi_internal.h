@@ -39,14 +39,17 @@ struct ModelCfg {
 // GPUModelInfo -> ModelCfg.  ncomp/lcomp give the component count and record
 // length (the caller resolves GPUInfo.nmodel / modelSize); validates the
 // record length for the type; copies specIndex (host pointer, else device).
+// A device specIndex is read with a blocking copy on the legacy default stream,
+// or, when `order` is given, on that stream (then synchronized), so that the
+// read follows work the caller queued there.
 int model_from_info(const GPUModelInfo* m, int ncomp, int lcomp, const GPUVisInfo* v, ModelCfg* mc,
-                    std::string* err);
+                    std::string* err, const cudaStream_t* order = nullptr);
 
 // GPUVisInfo (+ FP64 side table) -> LayoutDesc, including the frequency ratio
 // and log-frequency tables; reads the FP32 freqScale from the device when no
-// FP64 table is set.
+// FP64 table is set (on the legacy default stream, or on *order as above).
 int layout_from_info(const GPUVisInfo* v, const ModelCfg& mc, const FreqSide& fs, LayoutDesc* L,
-                     std::string* err);
+                     std::string* err, const cudaStream_t* order = nullptr);
 
 // Operation and polarization handling.
 int apply_from_info(const ModelCfg& mc, const PolnRules& pr, const LayoutDesc& L, ApplyDesc* A,
@@ -56,6 +59,14 @@ int apply_from_info(const ModelCfg& mc, const PolnRules& pr, const LayoutDesc& L
 // table of md.ncomp rows of md.lcomp floats, ordered on `stream`.
 int copy_comps(float* dst, const float* src, const ModelDesc& md, cudaStream_t stream,
                std::string* err);
+
+// Status of a kernel error flag read back by the host (0: none).  Codes:
+// 2 a component-tile copy did not land within the wait limit (the CTA left
+// after its copy landed: the context stays usable, OBIT_DFT_EKERNEL);
+// 3 a record's antenna number outside the beam's antenna table (EKERNEL);
+// 5 a copy was still in flight after the second wait window when the CTA left:
+// the CUDA context must be treated as unusable (OBIT_DFT_ECUDA).
+int kernel_flag_status(int flag, std::string* msg);
 
 // Thread-local last-error message of the C ABI.
 void set_last_error(const std::string& msg);

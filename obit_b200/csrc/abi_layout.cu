@@ -14,13 +14,32 @@ int bad(std::string* err, int code, const std::string& msg) {
   *err = msg;
   return code;
 }
+
+// Device -> host copy, blocking on the legacy default stream, or ordered on
+// *order and then synchronized with it.
+cudaError_t read_device(void* dst, const void* src, size_t bytes, const cudaStream_t* order) {
+  if (!order) return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+  cudaError_t ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, *order);
+  return ce == cudaSuccess ? cudaStreamSynchronize(*order) : ce;
+}
 }  // namespace
+
+int kernel_flag_status(int flag, std::string* msg) {
+  if (!flag) return OBIT_DFT_OK;
+  const char* what = flag == 2   ? ": a component-tile copy did not complete within the wait limit"
+                     : flag == 3 ? ": a record's antenna number is outside the beam's antenna table"
+                     : flag == 5 ? ": a component-tile copy was still in flight when a CTA gave up; "
+                                   "the CUDA context must be treated as unusable"
+                                 : "";
+  *msg = "kernel reported internal error code " + std::to_string(flag) + what;
+  return flag == 5 ? OBIT_DFT_ECUDA : OBIT_DFT_EKERNEL;
+}
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 
 int model_from_info(const GPUModelInfo* m, int ncomp, int lcomp, const GPUVisInfo* v, ModelCfg* mc,
-                    std::string* err) {
+                    std::string* err, const cudaStream_t* order) {
   if (!m) return bad(err, OBIT_DFT_EBADARG, "GPUModelInfo is NULL");
   ModelDesc md;
   md.kind = (int)m->type;
@@ -54,8 +73,7 @@ int model_from_info(const GPUModelInfo* m, int ncomp, int lcomp, const GPUVisInf
       mc->specIndex.assign(m->specIndex, m->specIndex + nfreq);
     } else if (m->d_specIndex) {
       mc->specIndex.resize(nfreq);
-      cudaError_t ce = cudaMemcpy(mc->specIndex.data(), m->d_specIndex, sizeof(int) * nfreq,
-                                  cudaMemcpyDeviceToHost);
+      cudaError_t ce = read_device(mc->specIndex.data(), m->d_specIndex, sizeof(int) * nfreq, order);
       if (ce != cudaSuccess)
         return bad(err, OBIT_DFT_ECUDA, std::string("specIndex copy: ") + cudaGetErrorString(ce));
     } else {
@@ -66,7 +84,7 @@ int model_from_info(const GPUModelInfo* m, int ncomp, int lcomp, const GPUVisInf
 }
 
 int layout_from_info(const GPUVisInfo* v, const ModelCfg& mc, const FreqSide& fs, LayoutDesc* L,
-                     std::string* err) {
+                     std::string* err, const cudaStream_t* order) {
   if (!v) return bad(err, OBIT_DFT_EBADARG, "GPUVisInfo is NULL");
   L->lrec = v->lenvis;
   L->nrparm = v->nrparm;
@@ -108,7 +126,7 @@ int layout_from_info(const GPUVisInfo* v, const ModelCfg& mc, const FreqSide& fs
   } else {
     if (!v->freqScale) return bad(err, OBIT_DFT_EBADARG, "GPUVisInfo.freqScale is NULL");
     std::vector<float> f32(nfreq);
-    cudaError_t ce = cudaMemcpy(f32.data(), v->freqScale, sizeof(float) * nfreq, cudaMemcpyDeviceToHost);
+    cudaError_t ce = read_device(f32.data(), v->freqScale, sizeof(float) * nfreq, order);
     if (ce != cudaSuccess)
       return bad(err, OBIT_DFT_ECUDA, std::string("freqScale copy: ") + cudaGetErrorString(ce));
     for (int i = 0; i < nfreq; i++) L->fscale[i] = (double)f32[i];

@@ -552,7 +552,9 @@ extern "C" int obit_dft_batch_check(ObitDFTBatch* b) {
   CUDA_TRY(cudaMemcpy(&h, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
     CUDA_TRY(cudaMemset(b->d_err, 0, sizeof(int)));
-    return fail(OBIT_DFT_EKERNEL, "kernel reported internal error code " + std::to_string(h));
+    std::string msg;
+    const int rc = kernel_flag_status(h, &msg);
+    return fail(rc, msg);
   }
   return OBIT_DFT_OK;
 }

@@ -195,7 +195,7 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
   phase ^= 1u;
   const bool failed = __syncthreads_or(done == 0) != 0;
   if (failed) {
-    if (threadIdx.x == 0 && p.errFlag) atomicExch(p.errFlag, 2);
+    if (threadIdx.x == 0 && p.errFlag) atomicMax(p.errFlag, 2);
     // give an in-flight copy a second bounded window to land before exiting
     for (int it = 0; it < (1 << 22) && !done; it++) {
       asm volatile(
@@ -204,6 +204,10 @@ __device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int 
           : "r"(bar_s), "r"(phase ^ 1u)
           : "memory");
     }
+    // still in flight after both windows: the CTA leaves with the copy
+    // writing its shared memory, which the host must treat as fatal for the
+    // context (code 5 outranks code 2)
+    if (__syncthreads_or(done == 0) && threadIdx.x == 0 && p.errFlag) atomicMax(p.errFlag, 5);
   }
   return !failed;
 }

@@ -220,10 +220,9 @@ int read_err_flag(State* s) {
   CUDA_TRY(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
     CUDA_TRY(cudaMemset(s->d_err, 0, sizeof(int)));
-    const char* what = h == 2   ? ": a component-tile copy did not complete within the wait limit"
-                       : h == 3 ? ": a record's antenna number is outside the beam's antenna table"
-                                : "";
-    return fail(OBIT_DFT_EKERNEL, "kernel reported internal error code " + std::to_string(h) + what);
+    std::string msg;
+    const int rc = kernel_flag_status(h, &msg);
+    return fail(rc, msg);
   }
   return OBIT_DFT_OK;
 }

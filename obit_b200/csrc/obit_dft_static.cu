@@ -12,14 +12,16 @@
 // only for its inputs and outputs.
 //
 // The array exists once per GPU that loads the library and lives until the
-// process exits.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress) with that device current; make that first call
-// before any stream capture.  Every call reuses the array and leaves the last
+// process exits.  Every call looks up the array's device address
+// (cudaGetSymbolAddress) with the caller's device current -- cheap next to the
+// copies and the synchronization, and never stale after a context is re-created.
+// The call is synchronous: it reads device descriptors on the caller's stream,
+// waits for the stream and copies the error flag back, so it must not be made
+// while a stream is capturing.  Every call reuses the array and leaves the last
 // call's contents behind, so calls that overlap on the GPU (other streams, other
 // host threads) race: serialize them.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "abi_internal.h"
@@ -32,38 +34,21 @@ using namespace obit;
 // Scratch limit: error flag, channel-block table and the padded component table.
 constexpr size_t kScratchBytes = 8u << 20;  // 8 MiB
 constexpr size_t kFlagBytes = 256;
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) unsigned char g_dft_scratch[kScratchBytes];
 
-std::mutex g_addr_mu;
-unsigned char* g_addr[kMaxDevices] = {};
-
 size_t round256(size_t n) { return (n + 255) & ~(size_t)255; }
 
-// Device address of the scratch array on the current device (looked up once).
+// Device address of the scratch array in the current device's context.  Host
+// code must not use g_dft_scratch itself: there it names a host-side stand-in.
 int scratch_address(unsigned char** out, std::string* err) {
-  int dev = 0;
-  cudaError_t ce = cudaGetDevice(&dev);
-  if (ce != cudaSuccess) {
-    *err = std::string("cudaGetDevice: ") + cudaGetErrorString(ce);
+  void* p = nullptr;
+  cudaError_t ce = cudaGetSymbolAddress(&p, g_dft_scratch);
+  if (ce != cudaSuccess || !p) {
+    *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce);
     return OBIT_DFT_ECUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    *err = "device index beyond the supported range";
-    return OBIT_DFT_EUNSUPPORTED;
-  }
-  std::lock_guard<std::mutex> lk(g_addr_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    ce = cudaGetSymbolAddress(&p, g_dft_scratch);
-    if (ce != cudaSuccess || !p) {
-      *err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(ce);
-      return OBIT_DFT_ECUDA;
-    }
-    g_addr[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = g_addr[dev];
+  *out = static_cast<unsigned char*>(p);
   return OBIT_DFT_OK;
 }
 
@@ -83,8 +68,10 @@ extern "C" int obit_dft_calc_noalloc(const GPUVisInfo* visInfo, const GPUModelIn
   if (nvis < 0) return failed(OBIT_DFT_EBADARG, "negative record count");
   if (nvis > 0 && !d_vis) return failed(OBIT_DFT_EBADARG, "NULL visibility buffer");
   std::string err;
+  cudaStream_t st = (cudaStream_t)stream;
   ModelCfg mc;
-  int rc = model_from_info(modelInfo, modelInfo->nmodel[0], modelInfo->size, visInfo, &mc, &err);
+  // device descriptors (specIndex, freqScale) are read in order on the caller's stream
+  int rc = model_from_info(modelInfo, modelInfo->nmodel[0], modelInfo->size, visInfo, &mc, &err, &st);
   if (rc) return failed(rc, err);
   FreqSide fs;
   if (freqArr) {
@@ -98,7 +85,7 @@ extern "C" int obit_dft_calc_noalloc(const GPUVisInfo* visInfo, const GPUModelIn
   }
   LayoutDesc L;
   ApplyDesc A;
-  rc = layout_from_info(visInfo, mc, fs, &L, &err);
+  rc = layout_from_info(visInfo, mc, fs, &L, &err, &st);
   if (!rc) rc = apply_from_info(mc, PolnRules(), L, &A, &err);
   if (rc) return failed(rc, err);
   if (nvis == 0 || mc.model.ncomp == 0) return OBIT_DFT_OK;
@@ -120,7 +107,6 @@ extern "C" int obit_dft_calc_noalloc(const GPUVisInfo* visInfo, const GPUModelIn
   int* d_flag = reinterpret_cast<int*>(base);
   BlockDesc* d_blocks = reinterpret_cast<BlockDesc*>(base + kFlagBytes);
   float* d_comps = reinterpret_cast<float*>(base + kFlagBytes + blkBytes);
-  cudaStream_t st = (cudaStream_t)stream;
 
   // the previous call's flag and tables are still in the array: clear the flag
   cudaError_t ce = cudaMemsetAsync(d_flag, 0, sizeof(int), st);
@@ -134,6 +120,10 @@ extern "C" int obit_dft_calc_noalloc(const GPUVisInfo* visInfo, const GPUModelIn
   ce = cudaMemcpyAsync(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
   if (ce != cudaSuccess) return failed(OBIT_DFT_ECUDA, std::string("completion: ") + cudaGetErrorString(ce));
-  if (flag) return failed(OBIT_DFT_EKERNEL, "kernel reported internal error code " + std::to_string(flag));
+  if (flag) {
+    std::string msg;
+    const int frc = kernel_flag_status(flag, &msg);
+    return failed(frc, msg);
+  }
   return OBIT_DFT_OK;
 }

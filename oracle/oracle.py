@@ -82,7 +82,7 @@ def _p(a, t):
 class Job:
     """An OracleJob plus the arrays it points into."""
 
-    def __init__(self, uv, sky, params=None, exact: bool = True, xyz=None):
+    def __init__(self, uv, sky, params=None, exact: bool = True, xyz=None, gpu_rules=None):
         from obit_b200.skymodel import OP_DIV, OP_REPL, SkyModelParams
         p = params or SkyModelParams()
         j = OracleJob()
@@ -111,6 +111,18 @@ class Job:
         j.stokFactor = p.stokFactor
         for i in range(4):
             j.polFact[i] = 1.0
+        if gpu_rules is not None:
+            # the reference GPU plug-in's rules (ObitCUDASkyModel.cu:134-160): the
+            # model times stokFact of each polarization, i on polarization 3 when
+            # doSwap, no running stokFactor product
+            stok_fact, do_swap = gpu_rules
+            j.stokFactor = 1.0
+            j.flipMask = 0
+            for i in range(j.numberPoln):
+                ist = j.startPoln + i
+                j.polFact[i] = float(stok_fact[ist]) if ist < 4 else 1.0
+                if do_swap and ist == 3:
+                    j.flipMask |= 1 << i
         fa = np.asarray(uv.freqArr, dtype=np.float64)
         self.fscale32 = np.ascontiguousarray(uv.fscale, dtype=np.float32)
         if exact:
@@ -145,12 +157,13 @@ def nthreads_default() -> int:
     return max(1, len(os.sched_getaffinity(0)))
 
 
-def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None):
+def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None,
+               gpu_rules=None):
     """FP64 component sum and L1 norm per (row, IF, channel):
     returns (model complex128 (nvis, nif, nchan), l1 float64 (nvis, nif, nchan));
     unselected entries are NaN.  xyz: optional (ncomp, 3) FP64 positions used
     for the phase instead of the table's FP32 fields 1-3."""
-    jb = Job(uv, sky, params, exact, xyz)
+    jb = Job(uv, sky, params, exact, xyz, gpu_rules)
     nfreq = uv.nchan * uv.nif
     model = np.full((uv.nvis, nfreq, 2), np.nan)
     l1 = np.full((uv.nvis, nfreq), np.nan)
@@ -164,9 +177,12 @@ def model_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = 
     return m, l1.reshape(uv.nvis, uv.nif, uv.nchan)
 
 
-def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None):
-    """FP64 oracle applied to a copy of uv.vis; returns the new float32 records."""
-    jb = Job(uv, sky, params, exact, xyz)
+def apply_fp64(uv, sky, params=None, exact: bool = True, nthreads: int | None = None, xyz=None,
+               gpu_rules=None):
+    """FP64 oracle applied to a copy of uv.vis; returns the new float32 records.
+    gpu_rules: None for the CPU DFT's polarization rules, or (stokFact[4],
+    doSwap) for those of the reference GPU plug-in."""
+    jb = Job(uv, sky, params, exact, xyz, gpu_rules)
     out = np.ascontiguousarray(uv.vis, dtype=np.float32).copy()
     rc = lib_a().oracle_apply_fp64(C.byref(jb.job), _p(out, C.c_float), nthreads or nthreads_default())
     if rc:

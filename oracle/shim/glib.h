@@ -1,8 +1,9 @@
 /* Minimal stand-in for the few GLib declarations that Obit's vector-math
- * sources (ObitSinCos.c, ObitExp.c, ObitVecFunc.c) and the headers they pull
- * in (Obit.h, ObitTypes.h, ObitErr.h, ObitInfoList.h) need at compile time.
- * Only used to build the reference-derived CPU baseline library; nothing in
- * the product includes it. */
+ * sources (ObitSinCos.c, ObitExp.c, ObitVecFunc.c), its GPU sky-model host glue
+ * (ObitGPUSkyModel.c) and the headers they pull in (Obit.h, ObitTypes.h,
+ * ObitErr.h, ObitInfoList.h, ObitThread.h, ObitUV.h, ObitSkyModel.h ...) need
+ * at compile time.  Only used to build the reference-derived test libraries
+ * under _ref/; nothing in the product includes it. */
 #ifndef OBIT_ORACLE_GLIB_SHIM_H
 #define OBIT_ORACLE_GLIB_SHIM_H
 #include <stddef.h>
@@ -58,4 +59,8 @@ void g_error(const gchar *fmt, ...);
 gpointer g_malloc0(gsize n);
 void g_free(gpointer p);
 gchar *g_strdup(const gchar *s);
+typedef gpointer (*GThreadFunc)(gpointer data);
+#define g_assert(e) ((void)0)
+gchar *g_strconcat(const gchar *s, ...);
+gint g_snprintf(gchar *s, gulong n, const gchar *fmt, ...);
 #endif

@@ -1,15 +1,26 @@
 """Regenerate struct_offsets.json: byte offsets of GPUVisInfo, GPUModelInfo and
 GPUInfo as the reference header declares them
 (ObitSystem/Obit/include/ObitCUDASkyModelInfoDef.h:66-195), compiled with gcc
-on this LP64 host.  Needs the reference tree; the JSON is committed."""
+on this LP64 host.  Needs the reference tree: its Obit include directory as the
+first argument, else $OBIT_REFERENCE/ObitSystem/Obit/include, else the
+reference checked out beside this repository (../reference).  The JSON is
+committed."""
 import json
+import os
 import subprocess
 import sys
 import tempfile
 from pathlib import Path
 
-REF_INC = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/ObitSystem/Obit/include")
-OUT = Path(__file__).resolve().parent / "struct_offsets.json"
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "struct_offsets.json"
+
+
+def ref_include() -> Path:
+    if len(sys.argv) > 1:
+        return Path(sys.argv[1])
+    root = os.environ.get("OBIT_REFERENCE") or str(HERE.parent.parent.parent / "reference")
+    return Path(root) / "ObitSystem" / "Obit" / "include"
 
 FIELDS = {
     "GPUVisInfo": ["nvis", "nprod", "nrparm", "lenvis", "nchan", "ilocu", "ilocv", "ilocw", "iloct",
@@ -36,7 +47,7 @@ def main():
     with tempfile.TemporaryDirectory() as d:
         src = Path(d) / "p.c"
         src.write_text("\n".join(lines))
-        subprocess.run(["gcc", "-I", str(REF_INC), str(src), "-o", str(Path(d) / "p")], check=True)
+        subprocess.run(["gcc", "-I", str(ref_include()), str(src), "-o", str(Path(d) / "p")], check=True)
         out = subprocess.run([str(Path(d) / "p")], capture_output=True, text=True, check=True).stdout
     res = {s: {"sizeof": 0, "offsets": {}} for s in FIELDS}
     for ln in out.splitlines():

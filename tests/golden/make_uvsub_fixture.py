@@ -38,6 +38,7 @@ from __future__ import annotations
 import gzip
 import json
 import math
+import os
 import sys
 from pathlib import Path
 
@@ -238,7 +239,14 @@ def vis_compare(a, b, nrparm):
 
 
 def main():
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference/ObitSystem/Obit")
+    # the reference's ObitSystem/Obit directory: the first argument, else
+    # $OBIT_REFERENCE/ObitSystem/Obit, else the reference checked out beside
+    # this repository (../reference)
+    if len(sys.argv) > 1:
+        ref = Path(sys.argv[1])
+    else:
+        root = os.environ.get("OBIT_REFERENCE") or str(Path(__file__).resolve().parents[3] / "reference")
+        ref = Path(root) / "ObitSystem" / "Obit"
     td = ref / "testData"
     rec, freq_arr, axes = read_uvtab(td / "UVSubTestIn.uvtab")
     master, _, _ = read_uvtab(td / "UVSubTestMaster.uvtab")

@@ -37,9 +37,12 @@ def _regular(uv, sky, params, torch):
     return d_vis.cpu().numpy()
 
 
-def _noalloc(uv, sky, params, torch):
+def _noalloc(uv, sky, params, torch, check_mem=False):
     """Records after obit_dft_calc_noalloc; inputs and outputs in device memory
-    the test owns, descriptors filled as ObitGPUSkyModelDFTInit/SetMod would."""
+    the test owns, descriptors filled as ObitGPUSkyModelDFTInit/SetMod would.
+    check_mem: the device's free memory must be the same before and after the
+    call (use it on a repeated call: the first launch of a kernel may load its
+    code, which takes device memory)."""
     lib = _lib.load()
     keep = []
     fscale = torch.from_numpy(uv.fscale).cuda()
@@ -71,12 +74,16 @@ def _noalloc(uv, sky, params, torch):
         spec = np.ascontiguousarray(sky.specFreq, dtype=np.float64)
         keep.append(spec)
     fa = np.ascontiguousarray(uv.freqArr, dtype=np.float64)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0] if check_mem else None
     rc = lib.obit_dft_calc_noalloc(
         C.byref(vi), C.byref(mi), fa.ctypes.data_as(C.POINTER(C.c_double)), uv.freq,
         sky.refFreq if sky.refFreq > 0 else uv.freq,
         spec.ctypes.data_as(C.POINTER(C.c_double)) if spec is not None else None,
         0 if spec is None else len(spec), C.c_void_p(d_vis.data_ptr()), uv.nvis, None)
     _lib.check(rc)
+    if check_mem:
+        assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
     return d_vis.cpu().numpy()
 
 
@@ -102,6 +109,9 @@ def test_noalloc_matches_regular_entry_point_twice():
         got = _noalloc(uv, sky, params, torch)
         assert not np.array_equal(got, uv.vis)
         assert _max_rel(got, want, uv, sky, params) < TOL_REL
+        # the same call again, its kernel now loaded: no device memory is taken
+        again = _noalloc(uv, sky, params, torch, check_mem=True)
+        assert np.array_equal(again, got)
 
 
 def test_noalloc_rejects_models_beyond_the_static_limit():
