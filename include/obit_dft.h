@@ -150,7 +150,10 @@ enum {
 /* Kernel flavors for obit_dft_set_kernel. */
 enum {
   OBIT_DFT_RECUR = 0, /* split-FP32 phase + complex channel recurrence (default) */
-  OBIT_DFT_PLAIN = 1  /* FP64 phase, one sin/cos per component-visibility */
+  OBIT_DFT_PLAIN = 1, /* FP64 phase, one sin/cos per component-visibility */
+  OBIT_DFT_RECUR_CHAIN = 2 /* the recurrence, with point components that carry a
+                              spectral index kept on the chain form (no
+                              spectral-factored form); a comparator */
 };
 
 /* Status forms of the four calls above. */
@@ -250,10 +253,12 @@ int obit_dft_set_tile(GPUInfo *gpuInfo, int blocksPerTile, int threadsPerCTA);
  * (a cudaStream_t; NULL = default stream).  No host copies. */
 int obit_dft_calc_device(GPUInfo *gpuInfo, float *d_vis, int nvis, void *stream);
 
-/* The plan the next call will use (building it if needed): info[0..7] =
+/* The plan the next call will use (building it if needed): info[0..8] =
  * flavor, channels per thread, components per tile, blocks per tile, rows per
- * tile, threads per CTA, channel blocks per row, channel-increment classes.
- * Writes min(n, 8) entries. */
+ * tile, threads per CTA, channel blocks per row, channel-increment classes,
+ * and 1 when point components with one spectral index take the
+ * spectral-factored recurrence (0: the chain form).  Writes min(n, 9)
+ * entries. */
 int obit_dft_plan_info(GPUInfo *gpuInfo, int *info, int n);
 
 /* No counterpart in the reference.  The same model application as

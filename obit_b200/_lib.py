@@ -178,6 +178,7 @@ SIGNATURES = {
 
 OBIT_DFT_RECUR = 0
 OBIT_DFT_PLAIN = 1
+OBIT_DFT_RECUR_CHAIN = 2  # recurrence without the spectral-factored form (comparator)
 
 _lib = None
 

@@ -370,14 +370,19 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // item = rt * nBlockTiles + bt.  smem is the CTA's dynamic shared memory, bar
 // its bulk-copy mbarrier with the running parity in phase.  Returns false (the
 // error flag set, uniformly across the CTA) when a component copy did not land;
-// the caller must then leave the kernel.
-template <int K, int MODE, bool kProbe = false, bool kLo = false>
+// the caller must then leave the kernel.  kFS (point families with one spectral
+// index, K a multiple of 8) selects the spectral-factored form; its component
+// table must be ordered by spectral index for the planner to have chosen it.
+template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false>
 __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* smem, uint64_t* bar,
                                            uint32_t& phase) {
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
   constexpr int H = K / 2;
   using F = Fields<MODE>;
-  constexpr bool kFact = point_factored(MODE, K);
+  constexpr bool kSF = kFS && spec_factorable(MODE, K);
+  constexpr bool kFact = point_factored(MODE, K) || kSF;
+  // spectral amplitude table of the chain form (point families with a spectrum)
+  constexpr bool kChainTable = F::kTable && !kSF;
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
@@ -388,7 +393,12 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   float2* sT = reinterpret_cast<float2*>(sS + p.ndf * ct * R);
   float* sQ = reinterpret_cast<float*>(sT + (kFact ? p.ndf * ct * R : 0));
   float* sG = sQ + (F::kGaussian ? ct * R : 0);
-  f2x* sCmp = reinterpret_cast<f2x*>(sG + (F::kTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
+  // spectral-factored instances: per (component, block) {A exp(e0), exp(e1),
+  // exp(4 e1), exp(8 e1)}, then per (block, pair) the tile's quadratic factor
+  float4* sF = reinterpret_cast<float4*>(sG);
+  f2x* sPhi = reinterpret_cast<f2x*>(sG + ct * Bt * 4);
+  f2x* sCmp = reinterpret_cast<f2x*>(
+      sG + (kSF ? ct * Bt * 4 + Bt * K : kChainTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
   // low parts of X, Y, Z (kLo instances), after everything else
   float* sLo = reinterpret_cast<float*>(sCmp) + (kFact ? 2 * K * R * Bt : 0);
   float2* stage = reinterpret_cast<float2*>(smem);
@@ -485,12 +495,45 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           for (int d = 0; d < p.ndf; d++) step_of(idx, P0, d);
         }
       }
+      // (component, block), spectral-factored form: the block's amplitude
+      // A exp(e0 + e1 k + e2 k^2), e_i = alpha l_i, is written as
+      // A exp(e0') exp(e1' k) exp(alpha_t l2 k^2) with the tile's reference
+      // index alpha_t and the residual (alpha - alpha_t) l2 k^2 replaced by its
+      // minimax line over k in [0, n], n = len - 1: k^2 ~ n k - n^2 / 8 (error
+      // at most (alpha - alpha_t) l2 n^2 / 8, which the planner bounds).  The
+      // first two factors ride on the anchor and the step; the last is the
+      // same for every component of the tile and multiplies the tile's sums.
+      if constexpr (kSF) {
+        const int nc = min(ct, p.ncomp - c0);
+        const float at =
+            0.5f * (sComp[kSpecIndexField] + sComp[(nc - 1) * p.cstride + kSpecIndexField]);
+        for (int idx = threadIdx.x; idx < ct * Bt; idx += blockDim.x) {
+          const int c = idx >> lgBt;
+          const int b = idx & (Bt - 1);
+          const float* cp = sComp + c * p.cstride;
+          const BlockDesc& bb = sBlk[b];
+          const float A = F::kTSpec ? cp[F::kTabOff + bb.plane] : cp[0];
+          const float al = cp[kSpecIndexField];
+          const float n = (float)(bb.len - 1);
+          const float r = (al - at) * bb.l[0][2];
+          const float e1 = __fmaf_rn(al, bb.l[0][1], r * n);
+          const float e0 = __fmaf_rn(al, bb.l[0][0], -0.125f * r * n * n);
+          sF[idx] = make_float4(A * expf(e0), expf(e1), expf(4.0f * e1), expf(8.0f * e1));
+        }
+        for (int idx = threadIdx.x; idx < Bt * H; idx += blockDim.x) {
+          const int b = idx >> lgH;
+          const int j = idx & (H - 1);
+          const float q = at * sBlk[b].l[0][2];
+          const float k1 = (float)(8 * (j >> 2) + (j & 3)), k2 = k1 + 4.0f;
+          sPhi[idx] = pk2(expf(q * k1 * k1), expf(q * k2 * k2));
+        }
+      }
       // (component, block): spectral amplitudes A exp(e0 + e1 k + e2 k^2) for the
       // block's K channels (point families with a spectrum), by packed
       // amplitude recurrences g <- g r, r <- r q started from exact
       // exponentials; items are taken two at a time so their recurrences
       // interleave.
-      if constexpr (F::kTable) {
+      if constexpr (kChainTable) {
         auto table_row = [&](int idx) {
           const int c = idx >> lgBt;
           const int b = idx & (Bt - 1);
@@ -564,16 +607,30 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         // anchor A exp(2 pi i P f0) of component c, one component ahead of
         // the multiply-accumulates so that its latency (shared loads,
         // split-FP32 product, MUFU) overlaps them; the tile is zero-filled to
-        // ct components, so the look-ahead index is clamped to the tile
+        // ct components, so the look-ahead index is clamped to the tile.
+        // Spectral-factored: amplitude A exp(e0') and steps w = s exp(e1'),
+        // w^4 = s^4 exp(4 e1'), w^8 = s^8 exp(8 e1').
         auto anchor = [&](int c, float2& g, float4& st, float2& s8) {
           const int i = c * R + tr;
           const float2 Pp = sP[i];
           st = sSd[i];
           s8 = sTd[i];
           g = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
-          const float A = sComp[c * p.cstride];
-          g.x *= A;
-          g.y *= A;
+          if constexpr (kSF) {
+            const float4 fa = sF[c * Bt + tb];
+            g.x *= fa.x;
+            g.y *= fa.x;
+            st.x *= fa.y;
+            st.y *= fa.y;
+            st.z *= fa.z;
+            st.w *= fa.z;
+            s8.x *= fa.w;
+            s8.y *= fa.w;
+          } else {
+            const float A = sComp[c * p.cstride];
+            g.x *= A;
+            g.y *= A;
+          }
         };
         float2 gn, s8n;
         float4 stn;
@@ -685,6 +742,11 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         const int nt = blockDim.x;
 #pragma unroll
         for (int j = 0; j < H; j++) {
+          if constexpr (kSF) {  // the tile's quadratic spectral factor
+            const f2x ph = sPhi[tb * H + j];
+            AR[j] = mul2(AR[j], ph);
+            AI[j] = mul2(AI[j], ph);
+          }
           f2x c = cmp[(2 * j) * nt];
           f2x y = sub2(AR[j], c);
           f2x s = add2(TR[j], y);
@@ -733,7 +795,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   return true;
 }
 
-template <int K, int MODE, bool kProbe = false, bool kLo = false>
+template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false>
 __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
     dft_recur_kernel(const __grid_constant__ KParams p) {
   extern __shared__ __align__(16) float smem[];
@@ -742,7 +804,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
   uint32_t phase = 0;
   const int nItems = ((p.nvis + p.R - 1) / p.R) * p.nBlockTiles;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x)
-    if (!recur_item<K, MODE, kProbe, kLo>(p, item, smem, &bar, phase)) return;
+    if (!recur_item<K, MODE, kProbe, kLo, kFS>(p, item, smem, &bar, phase)) return;
   inval_bar(&bar);
 }
 

@@ -40,8 +40,28 @@ KernelFn pick_plain(int mode) {
   return nullptr;
 }
 
+// Spectral-factored instances: point families with one spectral index, K a
+// multiple of 8.
+template <int K, bool kLo>
+KernelFn pick_spec_factored(int mode) {
+  if constexpr (K >= 8 && K % 8 == 0) {
+    if (mode == kPointSpec) return dft_recur_kernel<K, kPointSpec, false, kLo, true>;
+    if (mode == kPointTSpec) return dft_recur_kernel<K, kPointTSpec, false, kLo, true>;
+  }
+  return nullptr;
+}
+
 template <bool kLo>
-KernelFn pick_flavor(int flavor, int K, int mode) {
+KernelFn pick_flavor(int flavor, int K, int mode, bool fs) {
+  if (fs) {
+    if (flavor != kFlavorRecur) return nullptr;
+    switch (K) {
+      case 8: return pick_spec_factored<8, kLo>(mode);
+      case 16: return pick_spec_factored<16, kLo>(mode);
+      case 32: return pick_spec_factored<32, kLo>(mode);
+    }
+    return nullptr;
+  }
   if (flavor == kFlavorRecur) {
     switch (K) {
       case 2: return pick_recur<2, kLo>(mode);
@@ -64,13 +84,20 @@ KernelFn pick_flavor(int flavor, int K, int mode) {
 
 // The wait-limit diagnostic runs its own instance (32 channels, point +
 // spectrum) so that no production instance reads the limit at run time; FP64
-// positions (lo) select the instances that stage and add the low parts.
-KernelFn pick_kernel(int flavor, int K, int mode, bool probe, bool lo) {
+// positions (lo) select the instances that stage and add the low parts; fs the
+// spectral-factored instances.
+KernelFn pick_kernel(int flavor, int K, int mode, bool probe, bool lo, bool fs) {
   if (probe)
-    return (flavor == kFlavorRecur && K == 32 && mode == kPointSpec && !lo)
+    return (flavor == kFlavorRecur && K == 32 && mode == kPointSpec && !lo && !fs)
                ? dft_recur_kernel<32, kPointSpec, true>
                : nullptr;
-  return lo ? pick_flavor<true>(flavor, K, mode) : pick_flavor<false>(flavor, K, mode);
+  return lo ? pick_flavor<true>(flavor, K, mode, fs) : pick_flavor<false>(flavor, K, mode, fs);
+}
+
+KernelFn plan_kernel(const Plan& plan) {
+  return pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind,
+                     plan.kp.waitPolls != kDefaultWaitPolls, plan.kp.compsLo != nullptr,
+                     plan.specFactored);
 }
 
 }  // namespace
@@ -105,11 +132,10 @@ int build_plan(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, cons
 
 int finalize_plan(Plan* plan, BlockDesc* dst, cudaStream_t stream, std::string* err) {
   KParams& kp = plan->kp;
-  const int K = plan->tune.K;
   const int threads = plan->threads;
   const int nblocks = kp.nblocks;
   const bool probe = kp.waitPolls != kDefaultWaitPolls;
-  KernelFn fn = pick_kernel(plan->tune.flavor, K, plan->model.kind, probe, kp.compsLo != nullptr);
+  KernelFn fn = plan_kernel(*plan);
   if (!fn) {
     *err = probe ? "the wait-limit diagnostic runs 32-channel point+spectrum plans without FP64 positions only"
                  : "no kernel for this flavor and channel count";
@@ -171,8 +197,7 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   kp.errFlag = d_err;
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);
-  KernelFn fn = pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind,
-                            plan.kp.waitPolls != kDefaultWaitPolls, plan.kp.compsLo != nullptr);
+  KernelFn fn = plan_kernel(plan);
   if (!fn) {
     *err = "no kernel for this plan";
     return 3;

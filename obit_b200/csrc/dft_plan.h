@@ -31,7 +31,19 @@ struct ModelDesc {
   int lcomp = 4;      // floats per component in the source table
   int ncomp = 0;
   int nspec = 0;      // planes for tabulated spectra
+  // Planning only (not kept by the plan): the spectral index of each component
+  // in the order of the device table the kernel will read, or NULL.  Point
+  // families with one spectral index may take the spectral-factored kernel only
+  // when it is given (the table must be ordered by it; see spec_factorable).
+  const float* specIndex = nullptr;
 };
+
+// Bound on the per-term relative amplitude error of the spectral-factored form
+// (|alpha - alpha_tile| |l2| n^2 / 8 over every tile and block); plans above it
+// keep the chain form.  A tenth of the 1e-5 parity bound (relative to the sum
+// of |A|); 20,000 indices over [-1.5, 0.5] in 128-component tiles with 1 MHz
+// channels at 1.4 GHz give 2e-7.
+constexpr double kSpecResidualTol = 1e-6;
 
 struct ApplyDesc {
   int op = kOpSub;
@@ -47,6 +59,7 @@ struct TuneDesc {
   int ct = 128;  // components per shared-memory tile (shrunk to fit shared memory)
   int Bt = 0;   // blocks per tile (power of two); 0 = chosen by the planner
   int threads = 0;  // CTA size, 128 or 256; 0 = chosen by the planner
+  int specFactor = 1;  // 0: point families with a spectrum keep the chain form
 };
 
 // A compiled plan: block table on the device plus the fixed kernel fields.
@@ -59,6 +72,7 @@ struct Plan {
   int gridCap = 0;                 // CTAs resident across the device
   TuneDesc tune;
   ModelDesc model;
+  bool specFactored = false;       // spectral-factored instance (spec_factorable)
   bool linear = true;              // every block has a uniform channel increment
   double maxNonLin = 0.0;          // largest deviation from a linear frequency run
 };

@@ -251,23 +251,54 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   // spectral amplitude table: point families with a spectrum (Gaussian
   // families fold the spectrum into their per-row amplitude recurrence)
   const bool table = (M.kind == kPointSpec || M.kind == kPointTSpec);
-  const bool factored = (T.flavor == kFlavorRecur) && point_factored(M.kind, K);
+  // spectral-factored form: point families with one spectral index whose
+  // component order (M.specIndex) is known
+  bool fspec = (T.flavor == kFlavorRecur) && T.specFactor && spec_factorable(M.kind, K) &&
+               (M.kind == kPointTSpec || M.nterm == 1) && M.specIndex != nullptr && M.ncomp > 0;
   // shrink the component tile until the CTAs that the register budget lets
   // share an SM also fit its shared memory (32-channel recurrences run one
   // 256-thread CTA per SM)
-  int ct = (T.ct + 1) & ~1;  // even: the recurrence kernel takes components in pairs
   const bool oneCta = (T.flavor == kFlavorRecur && K >= 32);
   // (one 256-thread or two 128-thread CTAs per SM: 228 KB of shared memory,
   // less 1 KB reserved per CTA)
   const size_t budget = oneCta ? (threads == 128 ? 110 * 1024 : 200 * 1024)
                                : (threads == 128 ? 52 * 1024 : 110 * 1024);
   auto need = [&](int c) {
+    const bool factored = (T.flavor == kFlavorRecur) && (point_factored(M.kind, K) || fspec);
     size_t mainf = (T.flavor == kFlavorRecur)
-                       ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored)
+                       ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored,
+                                          fspec)
                        : (size_t)c * kp.cstride + (size_t)((kp.R * 3 + 3) & ~3) + 4 * (size_t)c;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
-  while (ct > 8 && need(ct) > budget) ct /= 2;
+  auto fit_tile = [&]() {
+    int c = (T.ct + 1) & ~1;  // even: the recurrence kernel takes components in pairs
+    while (c > 8 && need(c) > budget) c /= 2;
+    return c;
+  };
+  int ct = fit_tile();
+  if (fspec) {
+    // residual bound: the kernel's tile reference index is the midpoint of the
+    // tile's first and last index (as floats, as the kernel forms it)
+    double quad = 0.0;  // max over blocks of |l2| n^2 / 8
+    for (const BlockDesc& b : plan->blocks) {
+      const double n = (double)(b.len - 1);
+      quad = std::max(quad, std::fabs((double)b.l[0][2]) * n * n / 8.0);
+    }
+    double spread = 0.0;
+    for (int c0 = 0; c0 < M.ncomp; c0 += ct) {
+      const int nc = std::min(ct, M.ncomp - c0);
+      const float at = 0.5f * (M.specIndex[c0] + M.specIndex[c0 + nc - 1]);
+      for (int c = c0; c < c0 + nc; c++)
+        spread = std::max(spread, std::fabs((double)M.specIndex[c] - (double)at));
+    }
+    if (!(spread * quad <= kSpecResidualTol)) {
+      fspec = false;
+      ct = fit_tile();
+    }
+  }
+  plan->specFactored = fspec;
+  plan->model.specIndex = nullptr;  // valid during planning only
   kp.ct = ct;
   plan->smemBytes = need(ct);
   if (plan->smemBytes > 220 * 1024) {

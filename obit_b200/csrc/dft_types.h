@@ -86,6 +86,22 @@ struct BatchParams {
 // packed complex multiply-accumulate.
 OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == kPoint && K >= 8 && K % 8 == 0; }
 
+// Point models with one spectral index (PointSpec with one term, PointTSpec)
+// take the same factored form when the planner allows it (spectral-factored
+// instances): amplitude A exp(e0 + e1 k + e2 k^2) over a block; the linear part
+// rides on a non-unit step w = s exp(e1), the quadratic part is split into the
+// tile's common exp(alpha_t l2 k^2), applied per channel when the tile's sums
+// are folded, and a residual (alpha - alpha_t) l2 k^2 replaced by its minimax
+// line over the block.  alpha_t is the midpoint of the tile's first and last
+// spectral index: the component table is ordered by spectral index, so the
+// components of a tile have nearly equal indices and the residual is tiny.
+OBIT_HD constexpr inline bool spec_factorable(int mode, int K) {
+  return (mode == kPointSpec || mode == kPointTSpec) && K >= 8 && K % 8 == 0;
+}
+// Field of the spectral index: PointSpec's first term, PointTSpec's alpha
+// (ObitSkyModel.c:2044-2063, ObitSkyModelMF.c:1497-1514).
+constexpr int kSpecIndexField = 4;
+
 //--------------------------------------------------------------------------
 // Shared memory per CTA of the recurrence kernel (dynamic):
 //   comps  : ct * cstride floats (component tile, zero-filled past ncomp)
@@ -97,6 +113,9 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 //   Q      : ct * R floats            (Gaussian form, Gaussian models)
 //   G      : ct * Bt * 4 * (max(K/4, 1) + 1) floats (spectral amplitudes, point
 //            families with a spectrum: 16-byte entries, one padding entry per row)
+//            Spectral-factored instances instead: F, ct * Bt float4 (amplitude
+//            at the block's first channel, exp(e1), exp(4 e1), exp(8 e1)), and
+//            Phi, Bt * K floats (the tile's per-channel exp(alpha_t l2 k^2))
 //   Cmp    : 2 * K * R * Bt floats    (Kahan compensation of the totals, factored
 //            point models: K/2 re and K/2 im pairs per thread, thread-minor)
 //   lo     : ct * 4 floats            (low parts of X, Y, Z: instances for FP64
@@ -104,11 +123,12 @@ OBIT_HD constexpr inline bool point_factored(int mode, int K) { return mode == k
 // The model stage of the epilogue (R * Bt * K float2) reuses the same space.
 //--------------------------------------------------------------------------
 OBIT_HD inline size_t smem_floats_main(int R, int Bt, int K, int ct, int cstride, int ndf, bool gauss,
-                                       bool table, bool factored = false) {
+                                       bool table, bool factored = false, bool fspec = false) {
   size_t n = (size_t)ct * cstride + 4 * (size_t)ct + (size_t)((R * 3 + 3) & ~3) +
              (size_t)Bt * (sizeof(BlockDesc) / 4) + 2 * (size_t)ct * R + 4 * (size_t)ndf * ct * R;
   if (gauss) n += (size_t)ct * R;
-  if (table) n += (size_t)ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1);
+  if (fspec) n += (size_t)ct * Bt * 4 + (size_t)Bt * K;
+  else if (table) n += (size_t)ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1);
   if (factored) n += 2 * (size_t)ndf * ct * R + 2 * (size_t)K * R * Bt;
   return n;
 }

@@ -6,6 +6,7 @@
 // exactly as in the reference, and is only read here.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -72,6 +73,13 @@ struct State {
   float* d_lo = nullptr;  // low parts of FP64 positions (obit_dft_set_mod_d)
   size_t loBytes = 0;
   bool haveLo = false;
+  // The recurrence kernels' copy of the table (and of the low parts) ordered by
+  // spectral index, for point families with one index (spectral-factored
+  // form); the beam kernel and the FP64 side table keep the caller's order.
+  float* d_sorted = nullptr;
+  float* d_sortedLo = nullptr;
+  size_t sortedBytes = 0, sortedLoBytes = 0;
+  const float* runComps = nullptr;  // table the plan's launches read
   // plan
   Plan plan;
   bool planValid = false;
@@ -120,12 +128,67 @@ void release_state(State* s) {
   free_plan(&s->plan);
   if (s->d_comps) cudaFree(s->d_comps);
   if (s->d_lo) cudaFree(s->d_lo);
+  if (s->d_sorted) cudaFree(s->d_sorted);
+  if (s->d_sortedLo) cudaFree(s->d_sortedLo);
   if (s->d_err) cudaFree(s->d_err);
   free_beam_tables(s->beam);
   if (s->beam.d_antType) cudaFree(s->beam.d_antType);
   if (s->beam.d_jchan) cudaFree(s->beam.d_jchan);
   for (float* b : s->ownBufs) cudaFree(b);
   for (cudaStream_t st : s->ownStreams) cudaStreamDestroy(st);
+}
+
+// Fill s->d_sorted (and s->d_sortedLo with FP64 positions) with the model's
+// padded table stably ordered by spectral index; *index receives the ordered
+// indices.  Leaves *index empty (no ordering) when an index is not finite.
+int sort_by_spec_index(State* s, std::vector<float>* index) {
+  index->clear();
+  const ModelDesc& md = s->mc.model;
+  const size_t stride = (size_t)comp_stride(md), n = (size_t)md.ncomp;
+  std::vector<float> tab(n * stride), lo;
+  CUDA_TRY(cudaMemcpy(tab.data(), s->d_comps, sizeof(float) * tab.size(), cudaMemcpyDeviceToHost));
+  if (s->haveLo) {
+    lo.resize(n * 4);
+    CUDA_TRY(cudaMemcpy(lo.data(), s->d_lo, sizeof(float) * lo.size(), cudaMemcpyDeviceToHost));
+  }
+  for (size_t i = 0; i < n; i++)
+    if (!std::isfinite(tab[i * stride + kSpecIndexField])) return OBIT_DFT_OK;
+  std::vector<int> perm(n);
+  for (size_t i = 0; i < n; i++) perm[i] = (int)i;
+  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
+    return tab[(size_t)a * stride + kSpecIndexField] < tab[(size_t)b * stride + kSpecIndexField];
+  });
+  std::vector<float> out(tab.size()), outLo(lo.size());
+  index->resize(n);
+  for (size_t i = 0; i < n; i++) {
+    const size_t j = (size_t)perm[i];
+    std::copy(tab.begin() + j * stride, tab.begin() + (j + 1) * stride, out.begin() + i * stride);
+    if (s->haveLo) std::copy(lo.begin() + j * 4, lo.begin() + (j + 1) * 4, outLo.begin() + i * 4);
+    (*index)[i] = tab[j * stride + kSpecIndexField];
+  }
+  auto upload = [&](const std::vector<float>& h, float** d, size_t* cap) -> int {
+    const size_t bytes = std::max<size_t>(16, sizeof(float) * h.size());
+    if (bytes > *cap) {
+      if (*d) cudaFree(*d);
+      *d = nullptr;
+      *cap = 0;
+      CUDA_TRY(cudaMalloc(d, bytes));
+      *cap = bytes;
+    }
+    CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+    return OBIT_DFT_OK;
+  };
+  if (int rc = upload(out, &s->d_sorted, &s->sortedBytes)) {
+    index->clear();
+    return rc;
+  }
+  if (s->haveLo) {
+    if (int rc = upload(outLo, &s->d_sortedLo, &s->sortedLoBytes)) {
+      index->clear();
+      return rc;
+    }
+  }
+  return OBIT_DFT_OK;
 }
 
 int ensure_plan(GPUInfo* g, State* s) {
@@ -138,9 +201,27 @@ int ensure_plan(GPUInfo* g, State* s) {
   if (!rc) rc = apply_from_info(s->mc, s->pr, L, &A, &err);
   if (rc) return fail(rc, err);
   free_plan(&s->plan);
-  rc = plan_layout(L, s->mc.model, A, s->tune, &s->plan, &err);
+  // Point families with one spectral index: the recurrence kernels read a copy
+  // ordered by the index, which lets the planner choose the spectral-factored
+  // form (the wait-limit diagnostic has a chain-form instance only).
+  TuneDesc T = s->tune;
+  if (s->waitPolls != kDefaultWaitPolls) T.specFactor = 0;
+  ModelDesc md = s->mc.model;
+  std::vector<float> index;
+  s->runComps = s->d_comps;
+  const float* runLo = s->haveLo ? s->d_lo : nullptr;
+  const bool oneIndex = md.kind == kPointTSpec || (md.kind == kPointSpec && md.nterm == 1);
+  if (T.flavor == kFlavorRecur && T.specFactor && oneIndex && md.ncomp > 1) {
+    if ((rc = sort_by_spec_index(s, &index))) return rc;
+    if (!index.empty()) {
+      md.specIndex = index.data();
+      s->runComps = s->d_sorted;
+      if (s->haveLo) runLo = s->d_sortedLo;
+    }
+  }
+  rc = plan_layout(L, md, A, T, &s->plan, &err);
   s->plan.kp.waitPolls = s->waitPolls;  // chooses the diagnostic instance when lowered
-  s->plan.kp.compsLo = s->haveLo ? s->d_lo : nullptr;
+  s->plan.kp.compsLo = runLo;
   if (!rc) rc = finalize_plan(&s->plan, nullptr, 0, &err);
   if (rc) return fail(rc, err);
   if (s->beam.on) {  // launch parameters and per-(channel, IF) tables of the beam kernel
@@ -413,8 +494,10 @@ int obit_dft_set_kernel(GPUInfo* g, int flavor, int chanPerThread, int compsPerT
   State* s;
   int rc = ensure_state(g, &s);
   if (rc) return rc;
-  if (flavor != OBIT_DFT_RECUR && flavor != OBIT_DFT_PLAIN)
+  if (flavor != OBIT_DFT_RECUR && flavor != OBIT_DFT_PLAIN && flavor != OBIT_DFT_RECUR_CHAIN)
     return fail(OBIT_DFT_EBADARG, "unknown kernel flavor");
+  const int specFactor = (flavor == OBIT_DFT_RECUR_CHAIN) ? 0 : 1;
+  if (flavor == OBIT_DFT_RECUR_CHAIN) flavor = OBIT_DFT_RECUR;
   // 0 leaves the choice to the planner (also when switching flavor)
   const int K = chanPerThread ? chanPerThread : (flavor == s->tune.flavor ? s->tune.K : 0);
   if (flavor == OBIT_DFT_RECUR && !(K == 0 || K == 2 || K == 4 || K == 8 || K == 16 || K == 32))
@@ -423,6 +506,7 @@ int obit_dft_set_kernel(GPUInfo* g, int flavor, int chanPerThread, int compsPerT
     return fail(OBIT_DFT_EBADARG, "plain kernel: channels per thread must be 1, 2, 4, 8 or 16");
   if (compsPerTile < 0 || compsPerTile > 1024) return fail(OBIT_DFT_EBADARG, "bad components per tile");
   s->tune.flavor = flavor;
+  s->tune.specFactor = specFactor;
   s->tune.K = K;
   if (compsPerTile) s->tune.ct = compsPerTile;
   s->planValid = false;
@@ -472,7 +556,7 @@ int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
     k.nvis = nvis;
     rc = launch_beam(k, (cudaStream_t)stream, &err);
   } else {
-    rc = launch_plan(s->plan, d_vis, 0, nvis, s->d_comps, s->d_err, (cudaStream_t)stream, &err);
+    rc = launch_plan(s->plan, d_vis, 0, nvis, s->runComps, s->d_err, (cudaStream_t)stream, &err);
   }
   if (rc) return fail(rc, err);
   return OBIT_DFT_OK;
@@ -487,9 +571,9 @@ int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
   rc = ensure_plan(g, s);
   if (rc) return rc;
   const Plan& pl = s->plan;
-  const int v[8] = {pl.tune.flavor, pl.tune.K, pl.kp.ct, pl.kp.Bt, pl.kp.R, pl.threads,
-                    pl.kp.nblocks, pl.kp.ndf};
-  for (int i = 0; i < n && i < 8; i++) info[i] = v[i];
+  const int v[9] = {pl.tune.flavor, pl.tune.K, pl.kp.ct, pl.kp.Bt, pl.kp.R, pl.threads,
+                    pl.kp.nblocks, pl.kp.ndf, pl.specFactored ? 1 : 0};
+  for (int i = 0; i < n && i < 9; i++) info[i] = v[i];
   return OBIT_DFT_OK;
 }
 
@@ -570,7 +654,7 @@ int obit_dft_calc(GPUInfo* g) {
       k.nvis = nr;
       rc = launch_beam(k, streams[b], &err);
     } else {
-      rc = launch_plan(s->plan, bufs[b], 0, nr, s->d_comps, s->d_err, streams[b], &err);
+      rc = launch_plan(s->plan, bufs[b], 0, nr, s->runComps, s->d_err, streams[b], &err);
     }
     if (rc) return fail(rc, err);
     CUDA_TRY(cudaMemcpyAsync(host, bufs[b], bytes, cudaMemcpyDeviceToHost, streams[b]));

@@ -186,9 +186,9 @@ class GPUSkyModel:
 
     def plan_info(self) -> dict:
         """The kernel plan the next call uses (built on demand)."""
-        arr = (C.c_int * 8)()
-        _lib.check(self._lib.obit_dft_plan_info(self.gpuinfo, arr, 8))
-        keys = ("flavor", "K", "ct", "Bt", "R", "threads", "nblocks", "ndf")
+        arr = (C.c_int * 9)()
+        _lib.check(self._lib.obit_dft_plan_info(self.gpuinfo, arr, 9))
+        keys = ("flavor", "K", "ct", "Bt", "R", "threads", "nblocks", "ndf", "specFactored")
         return dict(zip(keys, list(arr)))
 
     def calc_device(self, d_vis_ptr: int, nvis: int, stream_ptr: int = 0) -> None:

@@ -96,6 +96,7 @@ void ObitErrLog(ObitErr *in) { (void)in; }
 /* InfoList: one list per UV object here; the glue reads GPU_no, nVisPIO and
  * doCalSelect and writes nVisPIO. */
 static olong g_nVisPIO = 0, g_gpu_no = 0, g_have_nvispio = 0;
+static int g_buf_records = 0; /* records per DFTCalc buffer of the last run */
 void ObitInfoListAlwaysPut(ObitInfoList *in, gchar *name, ObitInfoType type, gint32 *dim,
                            gconstpointer data) {
   (void)in, (void)type, (void)dim;
@@ -161,6 +162,7 @@ typedef struct {
 
 int refglue_run(const RefGlueJob *j) {
   g_errors = 0;
+  g_buf_records = 0;
   g_gpu_no = j->gpu;
   g_nVisPIO = j->nVisPIO > 0 ? j->nVisPIO : j->nvis;
   g_have_nvispio = 1;
@@ -253,6 +255,7 @@ int refglue_run(const RefGlueJob *j) {
   if (!err.error) ObitGPUSkyModelDFTSetMod(gm, (Obit *)sky, &model, &err);
   /* SubUV: one DFTCalc per I/O buffer of at most nVisPIO records */
   const int per = (int)(uv.bufferSize / j->lrec);
+  g_buf_records = per;
   for (int r0 = 0; !err.error && per > 0 && r0 < j->nvis; r0 += per) {
     const int n = (j->nvis - r0 < per) ? j->nvis - r0 : per;
     desc.numVisBuff = n;
@@ -267,5 +270,6 @@ int refglue_run(const RefGlueJob *j) {
   return (err.error || g_errors) ? 1 : 0;
 }
 
-/* Records per DFTCalc buffer the glue chose at its last DFTInit. */
-int refglue_nvispio(void) { return (int)g_nVisPIO; }
+/* Records per DFTCalc buffer of the last run: the nVisPIO the glue chose at
+ * DFTInit (its DFTShutdown puts the caller's old value back into the list). */
+int refglue_nvispio(void) { return g_buf_records; }

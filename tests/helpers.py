@@ -57,7 +57,7 @@ def model_error(uv, sky, params=None, exact=True, **kw):
 
 def small(modType=U.MOD_POINT, nrow=64, nchan=48, nif=2, nstok=2, ncomp=300, seed=11,
           radius_deg=0.5, max_bl=36e3, freq=1.4e9, dnu=1e6, nterm=1, flag_frac=0.0,
-          nplanes=3, gauss_frac=0.5):
+          nplanes=3, gauss_frac=0.5, alpha=(-1.5, 0.5)):
     """A small seeded workload of any model family."""
     rng = np.random.default_rng(seed)
     pos = U.array_layout(12, max_bl, rng)
@@ -75,7 +75,7 @@ def small(modType=U.MOD_POINT, nrow=64, nchan=48, nif=2, nstok=2, ncomp=300, see
         idx = np.clip(np.searchsorted(edges, fa, side="right") - 1, 0, nplanes - 1)
         kw = dict(spec_freq=spec_freq, spec_index=idx)
     sky = U.make_comps(modType, ncomp, np.random.default_rng(seed + 2), radius_deg=radius_deg,
-                       nterm=nterm, ref_freq=freq, gauss_frac=gauss_frac, **kw)
+                       nterm=nterm, ref_freq=freq, gauss_frac=gauss_frac, alpha=alpha, **kw)
     return uv, sky
 
 

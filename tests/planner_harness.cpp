@@ -6,9 +6,12 @@
 //   kind nterm lcomp ncomp nspec
 //   flavor K ct Bt threads
 //   nfreq, then nfreq fscale values, nfreq lnspec values, nfreq specIndex values
+//   optionally: nidx, then nidx per-component spectral indices in table order
+//   (the component count becomes nidx)
 #include <cstdio>
 #include <iostream>
 #include <string>
+#include <vector>
 
 #include "dft_plan.h"
 
@@ -32,6 +35,14 @@ int main() {
   for (auto& v : L.fscale) std::cin >> v;
   for (auto& v : L.lnspec) std::cin >> v;
   for (auto& v : L.specIndex) std::cin >> v;
+  int nidx = 0;
+  std::vector<float> idx;
+  if (std::cin >> nidx && nidx > 0) {
+    idx.resize(nidx);
+    for (auto& v : idx) std::cin >> v;
+    M.ncomp = nidx;
+    M.specIndex = idx.data();
+  }
   Plan P;
   std::string err;
   const int rc = plan_layout(L, M, A, T, &P, &err);
@@ -39,9 +50,10 @@ int main() {
   if (rc == 0) {
     const KParams& k = P.kp;
     printf(", \"K\": %d, \"Bt\": %d, \"R\": %d, \"ct\": %d, \"threads\": %d, \"nblocks\": %d, "
-           "\"ndf\": %d, \"smem\": %zu, \"linear\": %d, \"nBlockTiles\": %d, \"df\": [",
+           "\"ndf\": %d, \"smem\": %zu, \"linear\": %d, \"nBlockTiles\": %d, \"specFactored\": %d, "
+           "\"df\": [",
            P.tune.K, k.Bt, k.R, k.ct, P.threads, k.nblocks, k.ndf, P.smemBytes, (int)P.linear,
-           k.nBlockTiles);
+           k.nBlockTiles, (int)P.specFactored);
     for (int i = 0; i < k.ndf; i++) printf("%s%.17g", i ? ", " : "", (double)k.df_hi[i] + (double)k.df_lo[i]);
     printf("], \"blocks\": [");
     for (size_t i = 0; i < P.blocks.size(); i++) {

@@ -24,7 +24,7 @@ def harness(tmp_path_factory):
 
 def plan(exe, *, nchan=64, nif=2, nstok=2, chanb=0, chane=None, ifb=0, ife=None, kind=0, nterm=0,
          lcomp=4, nspec=0, flavor=0, K=0, ct=64, Bt=0, threads=256, fscale=None, lnspec=None,
-         specIndex=None):
+         specIndex=None, compIndex=None):
     nrparm = 5
     chane = nchan - 1 if chane is None else chane
     ife = nif - 1 if ife is None else ife
@@ -42,6 +42,8 @@ def plan(exe, *, nchan=64, nif=2, nstok=2, chanb=0, chane=None, ifb=0, ife=None,
              f"{flavor} {K} {ct} {Bt} {threads}",
              str(nfreq), " ".join(repr(float(x)) for x in fscale),
              " ".join(repr(float(x)) for x in lnspec), " ".join(str(int(x)) for x in specIndex)]
+    if compIndex is not None:
+        lines += [str(len(compIndex)), " ".join(repr(float(x)) for x in compIndex)]
     out = subprocess.run([str(exe)], input="\n".join(lines), capture_output=True, text=True,
                          check=True).stdout
     return json.loads(out)
@@ -181,3 +183,31 @@ def test_factored_point_tiles_keep_128_components(harness):
     assert p["smem"] <= 110 * 1024
     p = plan(harness, kind=0, lcomp=4, nchan=512, nif=8, threads=256, Bt=16, ct=128)
     assert p["rc"] == 0 and p["ct"] == 128 and p["smem"] <= 200 * 1024
+
+
+def test_spectral_factored_choice(harness):
+    """Point components with one spectral index take the spectral-factored form
+    only when the table order is known and every tile's spread of indices keeps
+    the residual quadratic below the bound; otherwise the chain form."""
+    nchan, nif = 256, 4
+    f = 1.4e9 + (np.arange(nchan * nif) % nchan) * 1e6 + (np.arange(nchan * nif) // nchan) * 256e6
+    ln = np.log(f / 1.4e9)
+    kw = dict(nchan=nchan, nif=nif, kind=1, nterm=1, lcomp=5, fscale=f / 1.4e9, lnspec=ln, ct=128)
+    rng = np.random.default_rng(5)
+    alpha = rng.uniform(-1.5, 0.5, 20000).astype(np.float32)
+    p = plan(harness, **kw, compIndex=np.sort(alpha))
+    assert p["rc"] == 0 and p["specFactored"] == 1 and p["K"] == 32
+    # the same indices in random order: tiles span the whole range
+    assert plan(harness, **kw, compIndex=alpha)["specFactored"] == 0
+    # order unknown, or turned off, or more than one spectral term
+    assert plan(harness, **kw)["specFactored"] == 0
+    # tabulated spectra take it too
+    p = plan(harness, **{**kw, "kind": 2, "nterm": 0, "lcomp": 9, "nspec": 4,
+                         "specIndex": (np.arange(nchan * nif) // nchan)}, compIndex=np.sort(alpha))
+    assert p["specFactored"] == 1
+    # the layout with the factored table fits the shared-memory budget
+    assert p["smem"] <= 220 * 1024
+    # a handful of components with indices far apart share one tile: chain form
+    assert plan(harness, **kw, compIndex=np.array([-2.0, 0.0, 2.0], np.float32))["specFactored"] == 0
+    # equal indices: any spread is zero
+    assert plan(harness, **kw, compIndex=np.full(300, -0.7, np.float32))["specFactored"] == 1
