@@ -50,7 +50,7 @@ ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per
 #   config5: dft_recur_batch_kernel<32, 0> over the 96-facet draw at 189,029 records
 #            (rows x 0.001; 3,668.0 MB read + 3,567.0 MB written)
 NCU_DRAM_BYTES_PER_RECORD = {
-    "config2": ((500.15e6 + 446.61e6) / 10080, "10,080-record capture"),
+    "config2": ((499.44e6 + 443.81e6) / 10080, "10,080-record capture"),
     "config4": ((296.35e6 + 240.85e6) / 23808, "23,808-record capture"),
     "config5": ((3668.0e6 + 3567.0e6) / 189029, "189,029-record capture of the same facet draw"),
 }
@@ -681,6 +681,17 @@ def main():
                 "plain_fp64_phase_gevals_s": pl, "recur_vs_plain": (value / 1e9) / pl,
                 "what": "FP64-phase plain kernel (one sin/cos per component-visibility) on the same "
                         "records and model, 2 launches"}
+            if gm.plan_info()["specFactored"]:
+                # the chain form of the same recurrence (no spectral factoring)
+                gm.set_kernel(_lib.OBIT_DFT_RECUR_CHAIN, args.K, args.ct, args.Bt, args.threads)
+                ch_ms, _ = _timed_on(torch, stream, lambda: gm.calc_device(d_vis.data_ptr(), rows, sp),
+                                     2, 1, gm.check)
+                ch = evals * 2 / (ch_ms * 1e-3) / 1e9
+                gm.set_kernel(flavor, args.K, args.ct, args.Bt, args.threads)
+                comp["same_records"].update({
+                    "recur_chain_form_gevals_s": ch, "factored_vs_chain": (value / 1e9) / ch,
+                    "chain_what": "the recurrence with the chain form for spectral point models "
+                                  "(OBIT_DFT_RECUR_CHAIN), same records, 2 launches"})
     if world == 1 and not args.no_compare and args.workload == "config2":
         m = config5_measure(torch, device, args.compare_row_scale, 2, 1, autotune=True, compare=True)
         comp["config5_batch"] = {
@@ -705,7 +716,7 @@ def main():
             cpu = {"value": v / 1e9, "unit": "Gevals/s", "cores": cores, "kind": kind, "sample": sample}
         pi = gm.plan_info()
         kern = (f"{args.flavor} K={pi['K']} ct={pi['ct']} Bt={pi['Bt']} R={pi['R']} "
-                f"threads={pi['threads']}")
+                f"threads={pi['threads']}" + (" spectral-factored" if pi["specFactored"] else ""))
         line = {
             "metric": METRIC,
             "value": value / 1e9, "unit": "Gevals/s", "n_gpus": world, "steps": args.steps,
