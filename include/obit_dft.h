@@ -253,11 +253,14 @@ int obit_dft_set_tile(GPUInfo *gpuInfo, int blocksPerTile, int threadsPerCTA);
  * (a cudaStream_t; NULL = default stream).  No host copies. */
 int obit_dft_calc_device(GPUInfo *gpuInfo, float *d_vis, int nvis, void *stream);
 
-/* The plan the next call will use (building it if needed): info[0..8] =
+/* The plan the next call will use (building it if needed): info[0..10] =
  * flavor, channels per thread, components per tile, blocks per tile, rows per
- * tile, threads per CTA, channel blocks per row, channel-increment classes,
- * and 1 when point components with one spectral index take the
- * spectral-factored recurrence (0: the chain form).  Writes min(n, 9)
+ * tile, threads per CTA, channel blocks per row, channel-increment classes;
+ * info[8] = 1 when point components with one spectral index take the
+ * spectral-factored recurrence (0: the chain form); info[9] = 1 when a
+ * Gaussian model with one spectral index runs mixed (its untapered components
+ * as spectral-factored points, the rest in the chain form, one launch), and
+ * info[10] the number of those point components.  Writes min(n, 11)
  * entries. */
 int obit_dft_plan_info(GPUInfo *gpuInfo, int *info, int n);
 

@@ -150,11 +150,12 @@ __device__ __forceinline__ void apply_tile(const KParams& p, const float2* stage
 // (4 floats per component) into sLo on the same mbarrier; the other instances
 // never touch them.
 template <bool kProbe = false, bool kLo = false>
-__device__ __forceinline__ bool stage_comps(const KParams& p, float* sComp, int c0, uint64_t* bar,
-                                            uint32_t& phase, float* sLo = nullptr) {
-  const int nc = min(p.ct, p.ncomp - c0);
+__device__ __forceinline__ bool stage_comps(const KParams& p, const float* tab, int ncomp, float* sComp,
+                                            int c0, uint64_t* bar, uint32_t& phase,
+                                            float* sLo = nullptr) {
+  const int nc = min(p.ct, ncomp - c0);
   const uint32_t bytes = (uint32_t)nc * p.cstride * 4u;
-  const float* src = p.comps + (size_t)c0 * p.cstride;
+  const float* src = tab + (size_t)c0 * p.cstride;
   const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
   const uint32_t bytesLo = kLo ? (uint32_t)nc * 16u : 0u;
   // Bulk copies need 16-byte aligned addresses and sizes; cstride is a multiple
@@ -366,6 +367,16 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // Recurrence kernel.  K channels per thread (even), MODE model family.
 //--------------------------------------------------------------------------
 
+// One pass of a work item over one component table (see recur_item): the
+// table's model family, the spectral-factored form, and whether its partial
+// sums are folded in the chain form's channel pairing (the point pass of a
+// mixed instance, which reads the point sub-table).
+template <int M, bool SF, bool RM>
+struct PassTag {
+  static constexpr int kMode = M;
+  static constexpr bool kSF = SF, kRemap = RM;
+};
+
 // One work item: rows [rt R, rt R + R) x channel-block tile bt of plan p, where
 // item = rt * nBlockTiles + bt.  smem is the CTA's dynamic shared memory, bar
 // its bulk-copy mbarrier with the running parity in phase.  Returns false (the
@@ -373,7 +384,8 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // the caller must then leave the kernel.  kFS (point families with one spectral
 // index, K a multiple of 8) selects the spectral-factored form; its component
 // table must be ordered by spectral index for the planner to have chosen it.
-template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false>
+template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false,
+          bool kMix = false>
 __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* smem, uint64_t* bar,
                                            uint32_t& phase) {
   static_assert(K >= 2 && (K & 1) == 0, "K must be even");
@@ -383,6 +395,17 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   constexpr bool kFact = point_factored(MODE, K) || kSF;
   // spectral amplitude table of the chain form (point families with a spectrum)
   constexpr bool kChainTable = F::kTable && !kSF;
+  // Mixed instances (a Gaussian family with one spectral index): the model's
+  // untapered components, taken out by the host into a point sub-table
+  // (p.compsPt, ordered by spectral index), run first as the matching point
+  // family in the spectral-factored form; the Gaussian components then run the
+  // chain form into the same compensated totals.
+  constexpr int kPtMode = (MODE == kGaussTSpec) ? kPointTSpec : kPointSpec;
+  constexpr bool kMixOn =
+      kMix && (MODE == kGaussSpec || MODE == kGaussTSpec) && spec_factorable(kPtMode, K);
+  // shared-memory regions: the union of both passes' in mixed instances
+  constexpr bool lFact = kFact || kMixOn;
+  constexpr bool lSF = kSF || kMixOn;
 
   const int R = p.R, Bt = p.Bt, ct = p.ct;
   float* sComp = smem;
@@ -391,16 +414,16 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   float2* sP = reinterpret_cast<float2*>(sBlk + Bt);
   float4* sS = reinterpret_cast<float4*>(sP + ct * R);
   float2* sT = reinterpret_cast<float2*>(sS + p.ndf * ct * R);
-  float* sQ = reinterpret_cast<float*>(sT + (kFact ? p.ndf * ct * R : 0));
+  float* sQ = reinterpret_cast<float*>(sT + (lFact ? p.ndf * ct * R : 0));
   float* sG = sQ + (F::kGaussian ? ct * R : 0);
   // spectral-factored instances: per (component, block) {A exp(e0), exp(e1),
   // exp(4 e1), exp(8 e1)}, then per (block, pair) the tile's quadratic factor
   float4* sF = reinterpret_cast<float4*>(sG);
   f2x* sPhi = reinterpret_cast<f2x*>(sG + ct * Bt * 4);
   f2x* sCmp = reinterpret_cast<f2x*>(
-      sG + (kSF ? ct * Bt * 4 + Bt * K : kChainTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
+      sG + (lSF ? ct * Bt * 4 + Bt * K : kChainTable ? ct * Bt * 4 * ((K >= 4 ? K / 4 : 1) + 1) : 0));
   // low parts of X, Y, Z (kLo instances), after everything else
-  float* sLo = reinterpret_cast<float*>(sCmp) + (kFact ? 2 * K * R * Bt : 0);
+  float* sLo = reinterpret_cast<float*>(sCmp) + (lFact ? 2 * K * R * Bt : 0);
   float2* stage = reinterpret_cast<float2*>(smem);
 
   // R and Bt are powers of two (R * Bt == CTA size)
@@ -424,7 +447,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
     const int nblkTile = min(Bt, p.nblocks - blk0);
     __syncthreads();  // the previous item's epilogue is done with the stage
 
-    if constexpr (kFact) {  // this thread's compensation terms start at zero
+    if constexpr (lFact) {  // this thread's compensation terms start at zero
 #pragma unroll
       for (int j = 0; j < 2 * H; j++) sCmp[j * blockDim.x + threadIdx.x] = 0ull;
     }
@@ -439,9 +462,27 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
     for (int j = 0; j < H; j++) TR[j] = TI[j] = CR[j] = CI[j] = 0ull;
 
-    for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
+    // One pass over a component table: the point sub-table (p.compsPt,
+    // p.ncompPt) for a mixed instance's first pass, else the model's table
+    // (p.comps, p.ncomp); records of the pass's family PM (field offsets
+    // Fields<PM>), p.cstride floats each.  pSF: the spectral-factored form;
+    // pRemap: its partial sums are folded in the chain form's pairing (pair j =
+    // channels j, j + H) instead of the factored one.  The table and count
+    // are read from the launch parameters where used (the point-family
+    // kernels run at the register limit).
+    auto pass = [&](auto tag) -> bool {
+      using Tag = decltype(tag);
+      const float* const tab = Tag::kRemap ? p.compsPt : p.comps;
+      const int ncomp = Tag::kRemap ? p.ncompPt : p.ncomp;
+      constexpr int PM = Tag::kMode;
+      using PF = Fields<PM>;
+      constexpr bool pSF = Tag::kSF && spec_factorable(PM, K);
+      constexpr bool pFact = point_factored(PM, K) || pSF;
+      constexpr bool pChainTable = PF::kTable && !pSF;
+      constexpr bool pRemap = Tag::kRemap && pFact;
+    for (int c0 = 0; c0 < ncomp; c0 += ct) {
       __syncthreads();  // previous tile's readers are done with shared memory
-      if (!stage_comps<kProbe, kLo>(p, sComp, c0, bar, phase, sLo)) return false;
+      if (!stage_comps<kProbe, kLo>(p, tab, ncomp, sComp, c0, bar, phase, sLo)) return false;
       __syncthreads();
 
       // (row, component): phase turns, steps, Gaussian form.  Items are taken
@@ -461,7 +502,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
             P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
           }
           sP[idx] = make_float2(P.hi, P.lo);
-          if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
+          if constexpr (PF::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
           return P;
         };
         auto step_of = [&](int idx, ds P, int d) {
@@ -472,18 +513,18 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           // s^Q (Q = K/4), the offset between the two packed chains of a
           // block, or s^H (H = K/2) for one-chain models; factored point
           // models: s^4 and s^8
-          constexpr int SP = kFact ? 4 : (F::kChains == 1 || Q == 0) ? H : Q;
+          constexpr int SP = pFact ? 4 : (PF::kChains == 1 || Q == 0) ? H : Q;
           float2 sq = s;
 #pragma unroll
           for (int m = 1; m < SP; m <<= 1) sq = cmul(sq, sq);
           sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
-          if constexpr (kFact) sT[d * ct * R + idx] = cmul(sq, sq);
+          if constexpr (pFact) sT[d * ct * R + idx] = cmul(sq, sq);
         };
         const int n = ct * R, nt = blockDim.x;
         int idx = threadIdx.x;
         // (Gaussian families: one item at a time -- their main loop is already
         // at the register limit and pairs measured slower there)
-        for (; !F::kGaussian && idx + nt < n; idx += 2 * nt) {
+        for (; !PF::kGaussian && idx + nt < n; idx += 2 * nt) {
           const ds P0 = phase_of(idx), P1 = phase_of(idx + nt);
           for (int d = 0; d < p.ndf; d++) {
             step_of(idx, P0, d);
@@ -503,8 +544,8 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
       // at most (alpha - alpha_t) l2 n^2 / 8, which the planner bounds).  The
       // first two factors ride on the anchor and the step; the last is the
       // same for every component of the tile and multiplies the tile's sums.
-      if constexpr (kSF) {
-        const int nc = min(ct, p.ncomp - c0);
+      if constexpr (pSF) {
+        const int nc = min(ct, ncomp - c0);
         const float at =
             0.5f * (sComp[kSpecIndexField] + sComp[(nc - 1) * p.cstride + kSpecIndexField]);
         for (int idx = threadIdx.x; idx < ct * Bt; idx += blockDim.x) {
@@ -512,7 +553,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           const int b = idx & (Bt - 1);
           const float* cp = sComp + c * p.cstride;
           const BlockDesc& bb = sBlk[b];
-          const float A = F::kTSpec ? cp[F::kTabOff + bb.plane] : cp[0];
+          const float A = PF::kTSpec ? cp[PF::kTabOff + bb.plane] : cp[0];
           const float al = cp[kSpecIndexField];
           const float n = (float)(bb.len - 1);
           const float r = (al - at) * bb.l[0][2];
@@ -533,16 +574,16 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
       // amplitude recurrences g <- g r, r <- r q started from exact
       // exponentials; items are taken two at a time so their recurrences
       // interleave.
-      if constexpr (kChainTable) {
+      if constexpr (pChainTable) {
         auto table_row = [&](int idx) {
           const int c = idx >> lgBt;
           const int b = idx & (Bt - 1);
           const float* cp = sComp + c * p.cstride;
           const BlockDesc& bb = sBlk[b];
           float A, e0, e1, e2;
-          if constexpr (F::kTSpec) {
-            A = cp[F::kTabOff + bb.plane];
-            const float al = cp[F::kAlphaOff];
+          if constexpr (PF::kTSpec) {
+            A = cp[PF::kTabOff + bb.plane];
+            const float al = cp[PF::kAlphaOff];
             e0 = al * bb.l[0][0];
             e1 = al * bb.l[0][1];
             e2 = al * bb.l[0][2];
@@ -552,7 +593,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
             for (int t = 0; t < kMaxNTerm; t++) {
               if (t < p.nterm) {
-                const float a = cp[F::kSpecOff + t];
+                const float a = cp[PF::kSpecOff + t];
                 e0 = __fmaf_rn(a, bb.l[t][0], e0);
                 e1 = __fmaf_rn(a, bb.l[t][1], e1);
                 e2 = __fmaf_rn(a, bb.l[t][2], e2);
@@ -596,12 +637,12 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
       for (int j = 0; j < H; j++) AR[j] = AI[j] = 0ull;
 
-      if (kFact && mine) {
+      if (pFact && mine) {
         // Factored point model: pair m = 4a + b holds channels (8a + b, 8a + b + 4).
         // G pairs (G_b, G_b+4) = A z0 (s^b, s^(b+4)) by a packed chain of three
         // steps; H_a = s^(8a) from the (row, component) prepass; then one packed
         // complex multiply-accumulate per pair of evaluations (a = 0: add).
-        const int nc = min(ct, p.ncomp - c0);
+        const int nc = min(ct, ncomp - c0);
         const float4* sSd = sS + bd.dfc * ct * R;
         const float2* sTd = sT + bd.dfc * ct * R;
         // anchor A exp(2 pi i P f0) of component c, one component ahead of
@@ -616,7 +657,7 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           st = sSd[i];
           s8 = sTd[i];
           g = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
-          if constexpr (kSF) {
+          if constexpr (pSF) {
             const float4 fa = sF[c * Bt + tb];
             g.x *= fa.x;
             g.y *= fa.x;
@@ -672,8 +713,8 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           }
         }
       }
-      if (!kFact && mine) {
-        const int nc = min(ct, p.ncomp - c0);
+      if (!pFact && mine) {
+        const int nc = min(ct, ncomp - c0);
         const float df = bd.df;
         const float4* sSd = sS + bd.dfc * ct * R;
         // Components in pairs: two prologues and four rotation chains in flight
@@ -681,26 +722,26 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         // A Gaussian taper adds five packed registers per chain pair; at 32
         // channels per thread two components' state no longer fits beside the
         // sums, so those take one component at a time.
-        constexpr bool kPairs = !(F::kGaussian && K >= 32);
+        constexpr bool kPairs = !(PF::kGaussian && K >= 32);
         auto table = [&](int c) {
           return reinterpret_cast<const ulonglong2*>(sG) + (c * Bt + tb) * TE;
         };
         auto entry = [&](const ulonglong2* G, int jj) {
-          if constexpr (F::kTable) return G[jj];
+          if constexpr (PF::kTable) return G[jj];
           else return make_ulonglong2(0ull, 0ull);
         };
         if constexpr (!kPairs) {
           for (int c = 0; c < nc; c++) {
             CompChains<H> x;
-            comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
+            comp_setup<PM, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
                                 p.cstride, f0, bd, df, p.nterm);
             const ulonglong2* Gx = table(c);
 #pragma unroll
             for (int jj = 0; jj < Q; jj++) {
               const ulonglong2 gx = entry(Gx, jj);
-              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
+              chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
                                x.NSI);
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
+              chain_step<PM>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
                                x.SR, x.SI, x.NSI);
             }
           }
@@ -708,45 +749,65 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         const int ncp = kPairs ? min(ct, (nc + 1) & ~1) : 0;
         for (int c = 0; c < ncp; c += 2) {
           CompChains<H> x, y;
-          comp_setup<MODE, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
+          comp_setup<PM, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
                               f0, bd, df, p.nterm);
-          comp_setup<MODE, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
+          comp_setup<PM, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
                               (c + 1) * R + tr, sComp, p.cstride, f0, bd, df, p.nterm);
           const ulonglong2* Gx = table(c);
           const ulonglong2* Gy = table(c + 1);
-          if constexpr (F::kChains == 1) {
+          if constexpr (PF::kChains == 1) {
 #pragma unroll
             for (int jj = 0; jj < H; jj++) {
-              chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, 0ull, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
-              chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, 0ull, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
+              chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, 0ull, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
+              chain_step<PM>(AR[jj], AI[jj], y.ZRa, y.ZIa, 0ull, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
             }
             continue;
           }
 #pragma unroll
           for (int jj = 0; jj < QE; jj++) {
             const ulonglong2 gx = entry(Gx, jj), gy = entry(Gy, jj);
-            chain_step<MODE>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
-            chain_step<MODE>(AR[jj], AI[jj], y.ZRa, y.ZIa, gy.x, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
+            chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
+            chain_step<PM>(AR[jj], AI[jj], y.ZRa, y.ZIa, gy.x, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
             if constexpr (Q > 0) {
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
+              chain_step<PM>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
                                x.SR, x.SI, x.NSI);
-              chain_step<MODE>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, gy.y, y.GGb, y.HHb, y.QQ,
+              chain_step<PM>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, gy.y, y.GGb, y.HHb, y.QQ,
                                y.SR, y.SI, y.NSI);
             }
           }
         }
       }
       // compensated fold of this tile's partial sums
-      if constexpr (kFact) {  // compensation terms in shared memory
+      if constexpr (pFact) {  // compensation terms in shared memory
         f2x* cmp = sCmp + threadIdx.x;
         const int nt = blockDim.x;
+        if constexpr (pSF) {  // the tile's quadratic spectral factor
 #pragma unroll
-        for (int j = 0; j < H; j++) {
-          if constexpr (kSF) {  // the tile's quadratic spectral factor
+          for (int j = 0; j < H; j++) {
             const f2x ph = sPhi[tb * H + j];
             AR[j] = mul2(AR[j], ph);
             AI[j] = mul2(AI[j], ph);
           }
+        }
+        if constexpr (pRemap) {
+          // factored pair m = 4a + b holds channels (8a + b, 8a + b + 4); chain
+          // pair j holds (j, j + H): channel c sits in factored pair
+          // 4 (c / 8) + c % 4, lane (c / 4) % 2
+          float xr[K], xi[K];
+#pragma unroll
+          for (int m = 0; m < H; m++) {
+            const int c1 = 8 * (m >> 2) + (m & 3);
+            up2(AR[m], xr[c1], xr[c1 + 4]);
+            up2(AI[m], xi[c1], xi[c1 + 4]);
+          }
+#pragma unroll
+          for (int j = 0; j < H; j++) {
+            AR[j] = pk2(xr[j], xr[j + H]);
+            AI[j] = pk2(xi[j], xi[j + H]);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < H; j++) {
           f2x c = cmp[(2 * j) * nt];
           f2x y = sub2(AR[j], c);
           f2x s = add2(TR[j], y);
@@ -772,6 +833,23 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
         TI[j] = s;
       }
     }
+      return true;
+    };
+    if constexpr (kMixOn) {
+      if (!pass(PassTag<kPtMode, true, true>{})) return false;
+      {  // the Gaussian pass continues the compensated totals in registers
+        const f2x* cmp = sCmp + threadIdx.x;
+        const int nt = blockDim.x;
+#pragma unroll
+        for (int j = 0; j < H; j++) {
+          CR[j] = cmp[(2 * j) * nt];
+          CI[j] = cmp[(2 * j + 1) * nt];
+        }
+      }
+      if (!pass(PassTag<MODE, false, false>{})) return false;
+    } else {
+      if (!pass(PassTag<MODE, kSF, false>{})) return false;
+    }
 
     // stage the tile's model and apply it to the records
     __syncthreads();
@@ -795,7 +873,8 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
   return true;
 }
 
-template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false>
+template <int K, int MODE, bool kProbe = false, bool kLo = false, bool kFS = false,
+          bool kMix = false>
 __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
     dft_recur_kernel(const __grid_constant__ KParams p) {
   extern __shared__ __align__(16) float smem[];
@@ -804,7 +883,7 @@ __global__ void __launch_bounds__(kThreads, (K >= 32 ? 1 : 2))
   uint32_t phase = 0;
   const int nItems = ((p.nvis + p.R - 1) / p.R) * p.nBlockTiles;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x)
-    if (!recur_item<K, MODE, kProbe, kLo, kFS>(p, item, smem, &bar, phase)) return;
+    if (!recur_item<K, MODE, kProbe, kLo, kFS, kMix>(p, item, smem, &bar, phase)) return;
   inval_bar(&bar);
 }
 
@@ -896,7 +975,7 @@ __global__ void __launch_bounds__(kThreads, 2) dft_plain_kernel(const KParams p)
     }
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();
-      if (!stage_comps<false, kLo>(p, sComp, c0, &bar, phase, sLo)) return;
+      if (!stage_comps<false, kLo>(p, p.comps, p.ncomp, sComp, c0, &bar, phase, sLo)) return;
       __syncthreads();
       float2 acc[K];
 #pragma unroll

@@ -51,6 +51,17 @@ KernelFn pick_spec_factored(int mode) {
   return nullptr;
 }
 
+// Mixed instances: a Gaussian family with one spectral index whose untapered
+// components run as the point family in the spectral-factored form.
+template <int K>
+KernelFn pick_mixed(int mode) {
+  if constexpr (K >= 8 && K % 8 == 0) {
+    if (mode == kGaussSpec) return dft_recur_kernel<K, kGaussSpec, false, false, false, true>;
+    if (mode == kGaussTSpec) return dft_recur_kernel<K, kGaussTSpec, false, false, false, true>;
+  }
+  return nullptr;
+}
+
 template <bool kLo>
 KernelFn pick_flavor(int flavor, int K, int mode, bool fs) {
   if (fs) {
@@ -95,6 +106,16 @@ KernelFn pick_kernel(int flavor, int K, int mode, bool probe, bool lo, bool fs) 
 }
 
 KernelFn plan_kernel(const Plan& plan) {
+  if (plan.mixed) {  // no FP64-position or diagnostic instances
+    if (plan.tune.flavor != kFlavorRecur || plan.kp.compsLo || plan.kp.waitPolls != kDefaultWaitPolls)
+      return nullptr;
+    switch (plan.tune.K) {
+      case 8: return pick_mixed<8>(plan.model.kind);
+      case 16: return pick_mixed<16>(plan.model.kind);
+      case 32: return pick_mixed<32>(plan.model.kind);
+    }
+    return nullptr;
+  }
   return pick_kernel(plan.tune.flavor, plan.tune.K, plan.model.kind,
                      plan.kp.waitPolls != kDefaultWaitPolls, plan.kp.compsLo != nullptr,
                      plan.specFactored);
@@ -194,6 +215,13 @@ int launch_plan(const Plan& plan, float* d_vis, int rowBase, int nvis, const flo
   kp.nvis = nvis;
   kp.comps = d_comps;
   kp.ncomp = plan.model.ncomp;
+  kp.compsPt = nullptr;
+  kp.ncompPt = 0;
+  if (plan.mixed) {  // point sub-table first, the Gaussian rows after it
+    kp.compsPt = d_comps;
+    kp.ncompPt = plan.model.ncompPt;
+    kp.comps = d_comps + (size_t)plan.model.ncompPt * kp.cstride;
+  }
   kp.errFlag = d_err;
   const long long nItems = (long long)((nvis + kp.R - 1) / kp.R) * kp.nBlockTiles;
   const int grid = (int)std::min<long long>(nItems, (long long)plan.gridCap);

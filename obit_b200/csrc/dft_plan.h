@@ -36,6 +36,12 @@ struct ModelDesc {
   // families with one spectral index may take the spectral-factored kernel only
   // when it is given (the table must be ordered by it; see spec_factorable).
   const float* specIndex = nullptr;
+  // Mixed Gaussian models (Gaussian family with one spectral index): the
+  // first ncompPt rows of the device table are its untapered components in the
+  // matching point family's field order (same stride, ordered by spectral
+  // index, which specIndex then lists); the ncomp rows after them are the
+  // Gaussian components.  0: an ordinary table.
+  int ncompPt = 0;
 };
 
 // Bound on the per-term relative amplitude error of the spectral-factored form
@@ -73,6 +79,7 @@ struct Plan {
   TuneDesc tune;
   ModelDesc model;
   bool specFactored = false;       // spectral-factored instance (spec_factorable)
+  bool mixed = false;              // mixed instance (ModelDesc.ncompPt > 0)
   bool linear = true;              // every block has a uniform channel increment
   double maxNonLin = 0.0;          // largest deviation from a linear frequency run
 };
@@ -83,7 +90,10 @@ int comp_stride(const ModelDesc& m);
 // Host part of planning: validate, cut the selected channels into blocks,
 // choose channels per thread, tile shape and component tile.  Fills
 // plan->blocks and every KParams field except the pointers and row range.
-// No CUDA calls.  Returns 0 or an error code (3) with a message in err.
+// No CUDA calls.  Returns 0, an error code (3) with a message in err, or 4
+// when a mixed table (ModelDesc.ncompPt > 0) cannot run mixed on this layout
+// (blocks too short for the factored form, or the point rows fail the
+// residual bound): the caller then plans the unsplit table.
 int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, const TuneDesc& T,
                 Plan* plan, std::string* err);
 

@@ -255,6 +255,17 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   // component order (M.specIndex) is known
   bool fspec = (T.flavor == kFlavorRecur) && T.specFactor && spec_factorable(M.kind, K) &&
                (M.kind == kPointTSpec || M.nterm == 1) && M.specIndex != nullptr && M.ncomp > 0;
+  // mixed Gaussian models: the point sub-table in the spectral-factored form,
+  // then the Gaussian components in the chain form (one launch)
+  const int ptKind = (M.kind == kGaussTSpec) ? kPointTSpec : kPointSpec;
+  bool mixed = (T.flavor == kFlavorRecur) && T.specFactor && M.ncompPt > 0 &&
+               M.specIndex != nullptr && (M.kind == kGaussTSpec || (M.kind == kGaussSpec && M.nterm == 1)) &&
+               spec_factorable(ptKind, K);
+  if (M.ncompPt > 0 && !mixed) {  // e.g. short blocks (non-uniform frequencies)
+    *err = "a table split into point and Gaussian parts needs the mixed recurrence";
+    return 4;
+  }
+  const int nIndexed = mixed ? M.ncompPt : M.ncomp;
   // shrink the component tile until the CTAs that the register budget lets
   // share an SM also fit its shared memory (32-channel recurrences run one
   // 256-thread CTA per SM)
@@ -264,10 +275,10 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   const size_t budget = oneCta ? (threads == 128 ? 110 * 1024 : 200 * 1024)
                                : (threads == 128 ? 52 * 1024 : 110 * 1024);
   auto need = [&](int c) {
-    const bool factored = (T.flavor == kFlavorRecur) && (point_factored(M.kind, K) || fspec);
+    const bool factored = (T.flavor == kFlavorRecur) && (point_factored(M.kind, K) || fspec || mixed);
     size_t mainf = (T.flavor == kFlavorRecur)
                        ? smem_floats_main(kp.R, kp.Bt, K, c, kp.cstride, kp.ndf, gauss, table, factored,
-                                          fspec)
+                                          fspec || mixed)
                        : (size_t)c * kp.cstride + (size_t)((kp.R * 3 + 3) & ~3) + 4 * (size_t)c;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
@@ -277,7 +288,7 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
     return c;
   };
   int ct = fit_tile();
-  if (fspec) {
+  if (fspec || mixed) {
     // residual bound: the kernel's tile reference index is the midpoint of the
     // tile's first and last index (as floats, as the kernel forms it)
     double quad = 0.0;  // max over blocks of |l2| n^2 / 8
@@ -286,18 +297,23 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
       quad = std::max(quad, std::fabs((double)b.l[0][2]) * n * n / 8.0);
     }
     double spread = 0.0;
-    for (int c0 = 0; c0 < M.ncomp; c0 += ct) {
-      const int nc = std::min(ct, M.ncomp - c0);
+    for (int c0 = 0; c0 < nIndexed; c0 += ct) {
+      const int nc = std::min(ct, nIndexed - c0);
       const float at = 0.5f * (M.specIndex[c0] + M.specIndex[c0 + nc - 1]);
       for (int c = c0; c < c0 + nc; c++)
         spread = std::max(spread, std::fabs((double)M.specIndex[c] - (double)at));
     }
     if (!(spread * quad <= kSpecResidualTol)) {
+      if (mixed) {  // the caller rebuilds the plan from the unsplit table
+        *err = "point sub-table fails the spectral-factored residual bound";
+        return 4;
+      }
       fspec = false;
       ct = fit_tile();
     }
   }
   plan->specFactored = fspec;
+  plan->mixed = mixed;
   plan->model.specIndex = nullptr;  // valid during planning only
   kp.ct = ct;
   plan->smemBytes = need(ct);

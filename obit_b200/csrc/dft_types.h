@@ -65,6 +65,10 @@ struct KParams {
   const float* compsLo;  // optional ncomp x 4 floats: low parts of X, Y, Z (FP64
                          // positions; fields 1-3 of comps hold the high parts)
   int ncomp, cstride, ct, nterm;
+  // Mixed instances only: the untapered components of a Gaussian-family model
+  // as a point-family sub-table (same stride, ordered by spectral index)
+  const float* compsPt;
+  int ncompPt;
   int nspec;           // planes (tabulated spectra)
   int rowBase;         // first row index of this launch within vis
   int* errFlag;        // set non-zero on an internal error (never traps)

@@ -138,34 +138,63 @@ void release_state(State* s) {
   for (cudaStream_t st : s->ownStreams) cudaStreamDestroy(st);
 }
 
-// Fill s->d_sorted (and s->d_sortedLo with FP64 positions) with the model's
-// padded table stably ordered by spectral index; *index receives the ordered
-// indices.  Leaves *index empty (no ordering) when an index is not finite.
-int sort_by_spec_index(State* s, std::vector<float>* index) {
+// The recurrence kernels' copy of the model table, in s->d_sorted:
+//  - point families with one spectral index: the padded table (and, with FP64
+//    positions, its low parts in s->d_sortedLo) stably ordered by index;
+//  - Gaussian families with one spectral index (no FP64 positions): the
+//    untapered components (g1 = g2 = g3 = 0, the reference's encoding of
+//    points in a Gaussian table, ObitSkyModel.c:2044-2063) re-encoded in the
+//    matching point family's field order and ordered by index, followed by
+//    the Gaussian components.  *md becomes that point family when no Gaussian
+//    is left, else a mixed model (md->ncompPt point rows, md->ncomp Gaussian).
+// *index receives the ordered spectral indices of the point rows; left empty
+// (no copy made, *md unchanged) when an index is not finite or no component
+// qualifies.
+int prepare_run_table(State* s, ModelDesc* md, std::vector<float>* index) {
   index->clear();
-  const ModelDesc& md = s->mc.model;
-  const size_t stride = (size_t)comp_stride(md), n = (size_t)md.ncomp;
+  const bool gauss = md->kind == kGaussSpec || md->kind == kGaussTSpec;
+  const size_t stride = (size_t)comp_stride(*md), n = (size_t)md->ncomp;
+  // spectral index: field 7 of a Gaussian record, 4 of a point record
+  const int aField = gauss ? 7 : kSpecIndexField;
   std::vector<float> tab(n * stride), lo;
   CUDA_TRY(cudaMemcpy(tab.data(), s->d_comps, sizeof(float) * tab.size(), cudaMemcpyDeviceToHost));
-  if (s->haveLo) {
+  const bool withLo = s->haveLo && !gauss;
+  if (withLo) {
     lo.resize(n * 4);
     CUDA_TRY(cudaMemcpy(lo.data(), s->d_lo, sizeof(float) * lo.size(), cudaMemcpyDeviceToHost));
   }
-  for (size_t i = 0; i < n; i++)
-    if (!std::isfinite(tab[i * stride + kSpecIndexField])) return OBIT_DFT_OK;
-  std::vector<int> perm(n);
-  for (size_t i = 0; i < n; i++) perm[i] = (int)i;
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) {
-    return tab[(size_t)a * stride + kSpecIndexField] < tab[(size_t)b * stride + kSpecIndexField];
-  });
-  std::vector<float> out(tab.size()), outLo(lo.size());
-  index->resize(n);
+  std::vector<int> pts, gs;
   for (size_t i = 0; i < n; i++) {
-    const size_t j = (size_t)perm[i];
-    std::copy(tab.begin() + j * stride, tab.begin() + (j + 1) * stride, out.begin() + i * stride);
-    if (s->haveLo) std::copy(lo.begin() + j * 4, lo.begin() + (j + 1) * 4, outLo.begin() + i * 4);
-    (*index)[i] = tab[j * stride + kSpecIndexField];
+    const float* r = tab.data() + i * stride;
+    if (!std::isfinite(r[aField])) return OBIT_DFT_OK;
+    if (!gauss || (r[4] == 0.0f && r[5] == 0.0f && r[6] == 0.0f)) pts.push_back((int)i);
+    else gs.push_back((int)i);
   }
+  if (pts.empty()) return OBIT_DFT_OK;
+  std::stable_sort(pts.begin(), pts.end(), [&](int a, int b) {
+    return tab[(size_t)a * stride + aField] < tab[(size_t)b * stride + aField];
+  });
+  std::vector<float> out(tab.size(), 0.0f), outLo(lo.size());
+  index->resize(pts.size());
+  for (size_t k = 0; k < pts.size(); k++) {
+    const float* src = tab.data() + (size_t)pts[k] * stride;
+    float* dst = out.data() + k * stride;
+    if (!gauss) {
+      std::copy(src, src + stride, dst);
+      if (withLo) std::copy(lo.begin() + (size_t)pts[k] * 4, lo.begin() + (size_t)pts[k] * 4 + 4,
+                            outLo.begin() + k * 4);
+    } else {
+      // [A, X, Y, Z, g1, g2, g3, alpha (, planes)] -> [A, X, Y, Z, alpha (, planes)]
+      std::copy(src, src + 4, dst);
+      dst[4] = src[7];
+      if (md->kind == kGaussTSpec)
+        for (int q = 0; q < md->nspec; q++) dst[5 + q] = src[8 + q];
+    }
+    (*index)[k] = src[aField];
+  }
+  for (size_t k = 0; k < gs.size(); k++)
+    std::copy(tab.begin() + (size_t)gs[k] * stride, tab.begin() + (size_t)(gs[k] + 1) * stride,
+              out.begin() + (pts.size() + k) * stride);
   auto upload = [&](const std::vector<float>& h, float** d, size_t* cap) -> int {
     const size_t bytes = std::max<size_t>(16, sizeof(float) * h.size());
     if (bytes > *cap) {
@@ -178,14 +207,18 @@ int sort_by_spec_index(State* s, std::vector<float>* index) {
     CUDA_TRY(cudaMemcpy(*d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
     return OBIT_DFT_OK;
   };
-  if (int rc = upload(out, &s->d_sorted, &s->sortedBytes)) {
+  int rc = upload(out, &s->d_sorted, &s->sortedBytes);
+  if (!rc && withLo) rc = upload(outLo, &s->d_sortedLo, &s->sortedLoBytes);
+  if (rc) {
     index->clear();
     return rc;
   }
-  if (s->haveLo) {
-    if (int rc = upload(outLo, &s->d_sortedLo, &s->sortedLoBytes)) {
-      index->clear();
-      return rc;
+  if (gauss) {
+    if (gs.empty()) {
+      md->kind = (md->kind == kGaussTSpec) ? kPointTSpec : kPointSpec;
+    } else {
+      md->ncompPt = (int)pts.size();
+      md->ncomp = (int)gs.size();
     }
   }
   return OBIT_DFT_OK;
@@ -210,13 +243,22 @@ int ensure_plan(GPUInfo* g, State* s) {
   std::vector<float> index;
   s->runComps = s->d_comps;
   const float* runLo = s->haveLo ? s->d_lo : nullptr;
-  const bool oneIndex = md.kind == kPointTSpec || (md.kind == kPointSpec && md.nterm == 1);
-  if (T.flavor == kFlavorRecur && T.specFactor && oneIndex && md.ncomp > 1) {
-    if ((rc = sort_by_spec_index(s, &index))) return rc;
+  const bool ptOne = md.kind == kPointTSpec || (md.kind == kPointSpec && md.nterm == 1);
+  const bool gsOne = md.kind == kGaussTSpec || (md.kind == kGaussSpec && md.nterm == 1);
+  if (T.flavor == kFlavorRecur && T.specFactor && md.ncomp > 1 && (ptOne || (gsOne && !s->haveLo))) {
+    ModelDesc m2 = md;
+    if ((rc = prepare_run_table(s, &m2, &index))) return rc;
     if (!index.empty()) {
-      md.specIndex = index.data();
-      s->runComps = s->d_sorted;
-      if (s->haveLo) runLo = s->d_sortedLo;
+      m2.specIndex = index.data();
+      Plan trial;
+      rc = plan_layout(L, m2, A, T, &trial, &err);
+      if (rc == 0) {  // the ordered (and, for Gaussian families, split) copy
+        md = m2;
+        s->runComps = s->d_sorted;
+        if (s->haveLo) runLo = s->d_sortedLo;
+      } else if (rc != 4) {
+        return fail(rc, err);
+      }  // 4: the split table cannot run mixed on this layout; keep the caller's table
     }
   }
   rc = plan_layout(L, md, A, T, &s->plan, &err);
@@ -571,9 +613,10 @@ int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
   rc = ensure_plan(g, s);
   if (rc) return rc;
   const Plan& pl = s->plan;
-  const int v[9] = {pl.tune.flavor, pl.tune.K, pl.kp.ct, pl.kp.Bt, pl.kp.R, pl.threads,
-                    pl.kp.nblocks, pl.kp.ndf, pl.specFactored ? 1 : 0};
-  for (int i = 0; i < n && i < 9; i++) info[i] = v[i];
+  const int v[11] = {pl.tune.flavor, pl.tune.K, pl.kp.ct, pl.kp.Bt, pl.kp.R, pl.threads,
+                     pl.kp.nblocks, pl.kp.ndf, pl.specFactored ? 1 : 0, pl.mixed ? 1 : 0,
+                     pl.mixed ? pl.model.ncompPt : 0};
+  for (int i = 0; i < n && i < 11; i++) info[i] = v[i];
   return OBIT_DFT_OK;
 }
 

@@ -186,9 +186,10 @@ class GPUSkyModel:
 
     def plan_info(self) -> dict:
         """The kernel plan the next call uses (built on demand)."""
-        arr = (C.c_int * 9)()
-        _lib.check(self._lib.obit_dft_plan_info(self.gpuinfo, arr, 9))
-        keys = ("flavor", "K", "ct", "Bt", "R", "threads", "nblocks", "ndf", "specFactored")
+        arr = (C.c_int * 11)()
+        _lib.check(self._lib.obit_dft_plan_info(self.gpuinfo, arr, 11))
+        keys = ("flavor", "K", "ct", "Bt", "R", "threads", "nblocks", "ndf", "specFactored", "mixed",
+                "ncompPoint")
         return dict(zip(keys, list(arr)))
 
     def calc_device(self, d_vis_ptr: int, nvis: int, stream_ptr: int = 0) -> None:

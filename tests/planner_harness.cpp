@@ -7,7 +7,8 @@
 //   flavor K ct Bt threads
 //   nfreq, then nfreq fscale values, nfreq lnspec values, nfreq specIndex values
 //   optionally: nidx, then nidx per-component spectral indices in table order
-//   (the component count becomes nidx)
+//   (the component count becomes nidx), then optionally ngauss: the table is
+//   a mixed one, nidx point rows followed by ngauss Gaussian rows
 #include <cstdio>
 #include <iostream>
 #include <string>
@@ -42,6 +43,11 @@ int main() {
     for (auto& v : idx) std::cin >> v;
     M.ncomp = nidx;
     M.specIndex = idx.data();
+    int ngauss = 0;
+    if (std::cin >> ngauss && ngauss > 0) {
+      M.ncompPt = nidx;
+      M.ncomp = ngauss;
+    }
   }
   Plan P;
   std::string err;
@@ -51,9 +57,9 @@ int main() {
     const KParams& k = P.kp;
     printf(", \"K\": %d, \"Bt\": %d, \"R\": %d, \"ct\": %d, \"threads\": %d, \"nblocks\": %d, "
            "\"ndf\": %d, \"smem\": %zu, \"linear\": %d, \"nBlockTiles\": %d, \"specFactored\": %d, "
-           "\"df\": [",
+           "\"mixed\": %d, \"df\": [",
            P.tune.K, k.Bt, k.R, k.ct, P.threads, k.nblocks, k.ndf, P.smemBytes, (int)P.linear,
-           k.nBlockTiles, (int)P.specFactored);
+           k.nBlockTiles, (int)P.specFactored, (int)P.mixed);
     for (int i = 0; i < k.ndf; i++) printf("%s%.17g", i ? ", " : "", (double)k.df_hi[i] + (double)k.df_lo[i]);
     printf("], \"blocks\": [");
     for (size_t i = 0; i < P.blocks.size(); i++) {

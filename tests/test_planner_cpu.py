@@ -24,7 +24,7 @@ def harness(tmp_path_factory):
 
 def plan(exe, *, nchan=64, nif=2, nstok=2, chanb=0, chane=None, ifb=0, ife=None, kind=0, nterm=0,
          lcomp=4, nspec=0, flavor=0, K=0, ct=64, Bt=0, threads=256, fscale=None, lnspec=None,
-         specIndex=None, compIndex=None):
+         specIndex=None, compIndex=None, ngauss=0):
     nrparm = 5
     chane = nchan - 1 if chane is None else chane
     ife = nif - 1 if ife is None else ife
@@ -43,7 +43,7 @@ def plan(exe, *, nchan=64, nif=2, nstok=2, chanb=0, chane=None, ifb=0, ife=None,
              str(nfreq), " ".join(repr(float(x)) for x in fscale),
              " ".join(repr(float(x)) for x in lnspec), " ".join(str(int(x)) for x in specIndex)]
     if compIndex is not None:
-        lines += [str(len(compIndex)), " ".join(repr(float(x)) for x in compIndex)]
+        lines += [str(len(compIndex)), " ".join(repr(float(x)) for x in compIndex), str(ngauss)]
     out = subprocess.run([str(exe)], input="\n".join(lines), capture_output=True, text=True,
                          check=True).stdout
     return json.loads(out)
@@ -211,3 +211,26 @@ def test_spectral_factored_choice(harness):
     assert plan(harness, **kw, compIndex=np.array([-2.0, 0.0, 2.0], np.float32))["specFactored"] == 0
     # equal indices: any spread is zero
     assert plan(harness, **kw, compIndex=np.full(300, -0.7, np.float32))["specFactored"] == 1
+
+
+def test_mixed_gaussian_plan(harness):
+    """A Gaussian table split into ordered point rows and Gaussian rows plans
+    mixed; layouts that cannot (short blocks from non-uniform frequencies, or
+    point rows failing the residual bound) report 4 so that the caller plans
+    the unsplit table."""
+    nchan, nif = 256, 4
+    f = 1.4e9 + (np.arange(nchan * nif) % nchan) * 1e6 + (np.arange(nchan * nif) // nchan) * 256e6
+    kw = dict(nchan=nchan, nif=nif, kind=4, nterm=1, lcomp=8, fscale=f / 1.4e9, lnspec=np.log(f / 1.4e9),
+              ct=128)
+    alpha = np.sort(np.random.default_rng(6).uniform(-1.5, 0.5, 35000)).astype(np.float32)
+    p = plan(harness, **kw, compIndex=alpha, ngauss=15000)
+    assert p["rc"] == 0 and p["mixed"] == 1 and p["specFactored"] == 0 and p["K"] == 32
+    assert p["smem"] <= 220 * 1024
+    assert plan(harness, **kw, compIndex=alpha[::700], ngauss=15000)["rc"] == 4   # wide tiles
+    g = f.copy()
+    g[3] += 17.0  # one channel off the uniform grid: short blocks
+    assert plan(harness, **{**kw, "fscale": g / 1.4e9}, compIndex=alpha, ngauss=15000)["rc"] == 4
+    # tabulated spectra
+    p = plan(harness, **{**kw, "kind": 5, "nterm": 0, "lcomp": 12, "nspec": 4,
+                         "specIndex": (np.arange(nchan * nif) // nchan)}, compIndex=alpha, ngauss=100)
+    assert p["rc"] == 0 and p["mixed"] == 1
