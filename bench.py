@@ -78,9 +78,10 @@ def parse():
     ap.add_argument("--cpu-step-seconds", type=float, default=2.0,
                     help="reference arm: CPU work per step (the row sample is sized to it)")
     ap.add_argument("--workload", default="config2",
-                    choices=["config1", "config2", "config3", "config4", "config5"],
+                    choices=["config1", "config2", "config3", "config4", "config5", "beam"],
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
-                         "96-facet uneven batch")
+                         "96-facet uneven batch; beam: the beam-corrected DFT on the config-2 "
+                         "layout")
     ap.add_argument("--row-scale", type=float, default=0.01,
                     help="config5: fraction of each facet's drawn rows held in HBM")
     ap.add_argument("--no-autotune", action="store_true", help="config5: keep the planner's tile")
@@ -546,6 +547,96 @@ def run_config5(args):
     print(json.dumps(line), flush=True)
 
 
+def run_beam(args):
+    """The beam-corrected DFT (obit_dft_set_beam) on the config-2 layout: a chunk
+    of `--rows` records (default 20,160 = 10 integrations of 2016 baselines) x 4
+    IF x 256 channels x 4 correlations (XX, YY, XY, YX all modelled), 4,000
+    point components with spectral index, 2 antenna types, 3 Jones planes, a
+    Stokes I sky; seeded Jones matrices near identity.  Device-resident records,
+    CUDA events; the per-channel form (FP64 phase, one sin/cos per evaluation)
+    on the same records as the comparator.  Algorithmic work per evaluation:
+    the phasor (complex rotate, 6 flops) and one complex multiply-accumulate
+    per modelled correlation (8 flops each)."""
+    import torch
+
+    from obit_b200 import _lib
+    from obit_b200 import uvdata as U
+    from obit_b200.beam import Beam, baseline_codes
+    from obit_b200.skymodel import GPUSkyModel, SkyModelParams
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    rows = args.rows or 20160
+    freq = 1.4e9
+    fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
+    uvw = _track(64, 36e3, 2000, freq, 2, rows, 0)
+    sky = U.make_comps(U.MOD_POINT_SPEC, args.ncomp or 4000, np.random.default_rng(4), radius_deg=1.0,
+                       nterm=1, ref_freq=freq)
+    d_vis = build_vis(torch, uvw, 4, 256, 4, device, seed=100)
+    d_vis[:, 3] = torch.from_numpy(baseline_codes(64, rows)).to(device)
+    lrec = d_vis.shape[1]
+    r = np.random.default_rng(7)
+    ntype, njc = 2, 3
+    jones = np.zeros((ntype, sky.ncomp, njc, 8), np.float32)
+    jones[..., 0] = 1.0
+    jones[..., 6] = 1.0
+    jones += (0.1 * r.standard_normal(jones.shape)).astype(np.float32)
+    beam = Beam(np.arange(64) % ntype, (np.arange(1024) * njc // 1024).astype(np.int32), jones)
+    d_jones = torch.from_numpy(jones).to(device)
+    uvh = U.UVData(np.zeros((1, lrec), np.float32), 4, 256, 4, freq, fa)
+    gm = GPUSkyModel("beam-bench")
+    gm.DFTInit(sky, uvh, SkyModelParams(nVisPIO=1, numberPoln=2))
+    gm.set_beam(beam, d_jones.data_ptr())
+    gm.DFTSetMod(sky)
+    stream = torch.cuda.Stream(device=device)
+    sp = stream.cuda_stream
+    evals = rows * 1024 * sky.ncomp
+    ncorr = 4
+    flops = 6.0 + 8.0 * ncorr
+    run = lambda: gm.calc_device(d_vis.data_ptr(), rows, sp)  # noqa: E731
+    with torch.cuda.stream(stream):
+        sampler = ClockSampler(0)
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        gm.check()
+        with sampler:
+            t_ms, launch_ms = _timed_on(torch, stream, run, args.steps, 0, gm.check)
+        comp = None
+        if not args.no_compare:
+            gm.set_kernel(_lib.OBIT_DFT_PLAIN)
+            gm.set_beam(beam, d_jones.data_ptr())
+            pt_ms, _ = _timed_on(torch, stream, run, 1, 1, gm.check)
+            pl = evals / (pt_ms * 1e-3) / 1e9
+            comp = {"per_channel_form_gevals_s": pl, "recur_vs_per_channel": evals * args.steps / (t_ms * 1e-3) / 1e9 / pl,
+                    "what": "the beam kernel's per-channel form (one thread per record and channel, FP64 "
+                            "phase, one sin/cos per component-visibility), same records, 1 launch"}
+    value = evals * args.steps / (t_ms * 1e-3)
+    peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
+    achieved = evals * flops / (statistics.mean(launch_ms) * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value / 1e9, "unit": "Gevals/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (split-FP32 phase)",
+        "data": "synthetic (seeded uvw, noise visibilities, random components and Jones matrices)",
+        "accuracy": {**ACCURACY, "checked_by": "tests/test_beam_gpu.py (-m gpu)"},
+        "config": {"workload": f"beam: {rows} records (64 antennas, 2016 baselines) x 4 IF x 256 ch x 4 "
+                               f"correlations, {sky.ncomp} point components with spectral index, "
+                               f"{ntype} antenna types, {njc} Jones planes, Stokes I sky",
+                   "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024,
+                   "correlations": ncorr, "l2": "inputs larger than L2", "timing": "CUDA events around all steps"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
+                     "flops_per_eval": flops},
+        "comparators": comp, "host": host_info(), "cpu_baseline": None, "e2e": None,
+        "gpu_launches": args.steps, "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    gm.DFTShutdown()
+    gm.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -553,6 +644,9 @@ def main():
         return
     if args.workload == "config5":
         run_config5(args)
+        return
+    if args.workload == "beam":
+        run_beam(args)
         return
 
     import torch

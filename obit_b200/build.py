@@ -43,7 +43,7 @@ def _cuda_include() -> str:
 
 def _inputs() -> list[Path]:
     files = [CSRC / s for s in CU_SOURCES + C_SOURCES + CXX_SOURCES]
-    files += list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
+    files += list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.inc")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
     files.append(Path(__file__))
     return files
 

@@ -1,22 +1,28 @@
-// Beam-corrected DFT (Stokes I, linear feeds): the model of ObitCUDABeamModel's
-// beam*Kernel family (ObitCUDABeamModel.cu:139-1226) with the Jones product of
-// cudaJonesCor1_Lin_I (CUDALinCorSum.h:104-134).
+// Beam-corrected DFT (linear feeds; Stokes I, Q, U or V sky): the model of
+// ObitCUDABeamModel's beam*Kernel family (ObitCUDABeamModel.cu:139-1226) with
+// the Jones products of cudaJonesCor1_Lin_{I,Q,U,V} (CUDALinCorSum.h:104-455).
 #pragma once
 #include <cuda_runtime.h>
 
 #include <string>
 
+#include "dft_types.h"
+
 namespace obit {
 
+// Channels per block of the beam recurrence kernel.
+constexpr int kBeamK = 8;
+
 struct BeamKParams {
-  float* vis;                    // device records, nvis x lrec floats
-  int nvis, lrec, nrparm, ilocu, ilocv, ilocw;
+  // Records, layout, channel blocks (at most kBeamK channels, never spanning a
+  // change of Jones plane), tile shape R x Bt, component table and tile ct,
+  // error flag: the fields the DFT kernels use, same meaning.
+  KParams k;
   int ilocb, iloca1, iloca2;     // BASELINE offset, or ANTENNA1 / ANTENNA2 (ilocb < 0)
-  int incs, incf, incif;         // float increments between correlations, channels, IFs
   int ncorr;                     // modelled correlations of XX, YY, XY, YX (1, 2 or 4)
-  int op;                        // OpKind
   float polFact[4];              // per record correlation
-  int chanb, nchanSel, ifb, nifSel, kincf, kincif;  // selection and table increments
+  // per-channel form (the plain comparator): selection and tables
+  int nrparm, chanb, nchanSel, ifb, nifSel, kincf, kincif, incif;
   const double* fscale;          // device, per (channel, IF) table index: nu / nu_uvref
   const double* lnspec;          // device or null: log-frequency term per table index
   const int* plane;              // device or null: tabulated-spectrum plane per table index
@@ -25,18 +31,21 @@ struct BeamKParams {
   int numAnt, numAntType, numJChan;
   const float* jones;            // device: [type][component][plane] x 8 floats (XX, XY, YX, YY)
   int jonesComps;                // components per type in the Jones table (>= ncomp)
-  const float* comps;            // device: ncomp records of cstride floats
-  int ncomp, cstride, ct, nterm, mode;
-  int* errFlag;                  // set to 3 for a record whose antennas are outside the table
+  int mode;                      // ModelKind
   int stokType;                  // sky Stokes: 1 I, 2 Q, 3 U, 4 V
   float c2p, s2p;                // cos, sin of twice the parallactic angle (Q, U)
+  int flavor;                    // kFlavorRecur (blocks) or kFlavorPlain (one thread per channel)
 };
 
-// Shared memory of one launch: the component tile and its Jones coefficients
-// for every (type, type) pair and plane, 8 floats each.
-inline size_t beam_smem_bytes(const BeamKParams& p) {
-  return sizeof(float) * ((size_t)p.ct * p.cstride + (size_t)p.numAntType * p.numAntType * p.ct * p.numJChan * 8);
-}
+// Correlation slots the recurrence kernel accumulates: XX and YY, or all four.
+inline int beam_nq(const BeamKParams& p) { return p.ncorr > 2 ? 4 : 2; }
+
+// Dynamic shared memory of a launch with component tile p.k.ct.
+size_t beam_smem_bytes(const BeamKParams& p);
+
+// Largest component tile (<= 128, a multiple of 8) whose shared memory fits
+// one CTA per SM; sets p->k.ct.  Returns 0 or an error code with err.
+int beam_fit_tile(BeamKParams* p, std::string* err);
 
 // One launch over all records of kp (stream-ordered, asynchronous).
 int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);

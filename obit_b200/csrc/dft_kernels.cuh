@@ -367,16 +367,6 @@ __device__ __forceinline__ void comp_setup(CompChains<H>& x, int c, float2 Pp, f
 // Recurrence kernel.  K channels per thread (even), MODE model family.
 //--------------------------------------------------------------------------
 
-// One pass of a work item over one component table (see recur_item): the
-// table's model family, the spectral-factored form, and whether its partial
-// sums are folded in the chain form's channel pairing (the point pass of a
-// mixed instance, which reads the point sub-table).
-template <int M, bool SF, bool RM>
-struct PassTag {
-  static constexpr int kMode = M;
-  static constexpr bool kSF = SF, kRemap = RM;
-};
-
 // One work item: rows [rt R, rt R + R) x channel-block tile bt of plan p, where
 // item = rt * nBlockTiles + bt.  smem is the CTA's dynamic shared memory, bar
 // its bulk-copy mbarrier with the running parity in phase.  Returns false (the
@@ -462,381 +452,22 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
 #pragma unroll
     for (int j = 0; j < H; j++) TR[j] = TI[j] = CR[j] = CI[j] = 0ull;
 
-    // One pass over a component table: the point sub-table (p.compsPt,
-    // p.ncompPt) for a mixed instance's first pass, else the model's table
-    // (p.comps, p.ncomp); records of the pass's family PM (field offsets
-    // Fields<PM>), p.cstride floats each.  pSF: the spectral-factored form;
-    // pRemap: its partial sums are folded in the chain form's pairing (pair j =
-    // channels j, j + H) instead of the factored one.  The table and count
-    // are read from the launch parameters where used (the point-family
-    // kernels run at the register limit).
-    auto pass = [&](auto tag) -> bool {
-      using Tag = decltype(tag);
-      const float* const tab = Tag::kRemap ? p.compsPt : p.comps;
-      const int ncomp = Tag::kRemap ? p.ncompPt : p.ncomp;
-      constexpr int PM = Tag::kMode;
-      using PF = Fields<PM>;
-      constexpr bool pSF = Tag::kSF && spec_factorable(PM, K);
-      constexpr bool pFact = point_factored(PM, K) || pSF;
-      constexpr bool pChainTable = PF::kTable && !pSF;
-      constexpr bool pRemap = Tag::kRemap && pFact;
-    for (int c0 = 0; c0 < ncomp; c0 += ct) {
-      __syncthreads();  // previous tile's readers are done with shared memory
-      if (!stage_comps<kProbe, kLo>(p, tab, ncomp, sComp, c0, bar, phase, sLo)) return false;
-      __syncthreads();
-
-      // (row, component): phase turns, steps, Gaussian form.  Items are taken
-      // two at a time so their long dependent chains (split-FP32 products,
-      // accurate sin/cos) interleave.
-      {
-        auto phase_of = [&](int idx) {
-          const int c = idx >> lgR;
-          const int r = idx & (R - 1);
-          const float* cp = sComp + c * p.cstride;
-          const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-          ds P;
-          if constexpr (kLo) {  // FP64 positions
-            const float* lo = sLo + 4 * c;
-            P = ds_mul(ds_dot3_lo(cp[1], lo[0], u, cp[2], lo[1], v, cp[3], lo[2], w), ds{kInv2PiHi, kInv2PiLo});
-          } else {
-            P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
-          }
-          sP[idx] = make_float2(P.hi, P.lo);
-          if constexpr (PF::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
-          return P;
-        };
-        auto step_of = [&](int idx, ds P, int d) {
-          // reduced step angle: exact integer removal from the high part, the
-          // low part kept for the first-order correction
-          const ds t = ds_mul(P, ds{p.df_hi[d], p.df_lo[d]});
-          const float2 s = phasor_accurate(ds{__fsub_rn(t.hi, rintf(t.hi)), t.lo});
-          // s^Q (Q = K/4), the offset between the two packed chains of a
-          // block, or s^H (H = K/2) for one-chain models; factored point
-          // models: s^4 and s^8
-          constexpr int SP = pFact ? 4 : (PF::kChains == 1 || Q == 0) ? H : Q;
-          float2 sq = s;
-#pragma unroll
-          for (int m = 1; m < SP; m <<= 1) sq = cmul(sq, sq);
-          sS[d * ct * R + idx] = make_float4(s.x, s.y, sq.x, sq.y);
-          if constexpr (pFact) sT[d * ct * R + idx] = cmul(sq, sq);
-        };
-        const int n = ct * R, nt = blockDim.x;
-        int idx = threadIdx.x;
-        // (Gaussian families: one item at a time -- their main loop is already
-        // at the register limit and pairs measured slower there)
-        for (; !PF::kGaussian && idx + nt < n; idx += 2 * nt) {
-          const ds P0 = phase_of(idx), P1 = phase_of(idx + nt);
-          for (int d = 0; d < p.ndf; d++) {
-            step_of(idx, P0, d);
-            step_of(idx + nt, P1, d);
-          }
-        }
-        for (; idx < n; idx += nt) {
-          const ds P0 = phase_of(idx);
-          for (int d = 0; d < p.ndf; d++) step_of(idx, P0, d);
-        }
-      }
-      // (component, block), spectral-factored form: the block's amplitude
-      // A exp(e0 + e1 k + e2 k^2), e_i = alpha l_i, is written as
-      // A exp(e0') exp(e1' k) exp(alpha_t l2 k^2) with the tile's reference
-      // index alpha_t and the residual (alpha - alpha_t) l2 k^2 replaced by its
-      // minimax line over k in [0, n], n = len - 1: k^2 ~ n k - n^2 / 8 (error
-      // at most (alpha - alpha_t) l2 n^2 / 8, which the planner bounds).  The
-      // first two factors ride on the anchor and the step; the last is the
-      // same for every component of the tile and multiplies the tile's sums.
-      if constexpr (pSF) {
-        const int nc = min(ct, ncomp - c0);
-        const float at =
-            0.5f * (sComp[kSpecIndexField] + sComp[(nc - 1) * p.cstride + kSpecIndexField]);
-        for (int idx = threadIdx.x; idx < ct * Bt; idx += blockDim.x) {
-          const int c = idx >> lgBt;
-          const int b = idx & (Bt - 1);
-          const float* cp = sComp + c * p.cstride;
-          const BlockDesc& bb = sBlk[b];
-          const float A = PF::kTSpec ? cp[PF::kTabOff + bb.plane] : cp[0];
-          const float al = cp[kSpecIndexField];
-          const float n = (float)(bb.len - 1);
-          const float r = (al - at) * bb.l[0][2];
-          const float e1 = __fmaf_rn(al, bb.l[0][1], r * n);
-          const float e0 = __fmaf_rn(al, bb.l[0][0], -0.125f * r * n * n);
-          sF[idx] = make_float4(A * expf(e0), expf(e1), expf(4.0f * e1), expf(8.0f * e1));
-        }
-        for (int idx = threadIdx.x; idx < Bt * H; idx += blockDim.x) {
-          const int b = idx >> lgH;
-          const int j = idx & (H - 1);
-          const float q = at * sBlk[b].l[0][2];
-          const float k1 = (float)(8 * (j >> 2) + (j & 3)), k2 = k1 + 4.0f;
-          sPhi[idx] = pk2(expf(q * k1 * k1), expf(q * k2 * k2));
-        }
-      }
-      // (component, block): spectral amplitudes A exp(e0 + e1 k + e2 k^2) for the
-      // block's K channels (point families with a spectrum), by packed
-      // amplitude recurrences g <- g r, r <- r q started from exact
-      // exponentials; items are taken two at a time so their recurrences
-      // interleave.
-      if constexpr (pChainTable) {
-        auto table_row = [&](int idx) {
-          const int c = idx >> lgBt;
-          const int b = idx & (Bt - 1);
-          const float* cp = sComp + c * p.cstride;
-          const BlockDesc& bb = sBlk[b];
-          float A, e0, e1, e2;
-          if constexpr (PF::kTSpec) {
-            A = cp[PF::kTabOff + bb.plane];
-            const float al = cp[PF::kAlphaOff];
-            e0 = al * bb.l[0][0];
-            e1 = al * bb.l[0][1];
-            e2 = al * bb.l[0][2];
-          } else {
-            A = cp[0];
-            e0 = e1 = e2 = 0.f;
-#pragma unroll
-            for (int t = 0; t < kMaxNTerm; t++) {
-              if (t < p.nterm) {
-                const float a = cp[PF::kSpecOff + t];
-                e0 = __fmaf_rn(a, bb.l[t][0], e0);
-                e1 = __fmaf_rn(a, bb.l[t][1], e1);
-                e2 = __fmaf_rn(a, bb.l[t][2], e2);
-              }
-            }
-          }
-          // amplitude exp(E(k)) and ratio exp(D(k)) = A(k+1) / A(k) at channel k
-          auto E = [&](float k) { return A * exp_fast(__fmaf_rn(k, __fmaf_rn(k, e2, e1), e0)); };
-          auto D = [&](float k) { return exp_fast(__fmaf_rn(e2, 2.0f * k + 1.0f, e1)); };
-          const float fh = (float)H, fe = (float)QE;
-          // layout [component][block][entry e], entry e = {pair e, pair e + QE}
-          // with pair j = channels (j, j + H): one 128-bit load feeds a step of
-          // both chains.  Two packed recurrences, one per half of the entries,
-          // fill whole entries; the padded row of QE + 1 entries puts the
-          // 128-bit stores of consecutive threads on distinct banks.
-          f2x GA = pk2(E(0.f), E(fh)), RA = pk2(D(0.f), D(fh));
-          f2x GB = pk2(E(fe), E(fe + fh)), RB = pk2(D(fe), D(fe + fh));
-          const float q = exp_fast(2.0f * e2);
-          const f2x QQ = pk2(q, q);
-          ulonglong2* out = reinterpret_cast<ulonglong2*>(sG) + (c * Bt + b) * TE;
-#pragma unroll
-          for (int e = 0; e < QE; e++) {
-            out[e] = make_ulonglong2(GA, GB);
-            GA = mul2(GA, RA);
-            RA = mul2(RA, QQ);
-            GB = mul2(GB, RB);
-            RB = mul2(RB, QQ);
-          }
-        };
-        const int n = ct * Bt, nt = blockDim.x;
-        int idx = threadIdx.x;
-        for (; idx + nt < n; idx += 2 * nt) {
-          table_row(idx);
-          table_row(idx + nt);
-        }
-        if (idx < n) table_row(idx);
-      }
-      __syncthreads();
-
-      f2x AR[H], AI[H];  // this tile's partial sums
-#pragma unroll
-      for (int j = 0; j < H; j++) AR[j] = AI[j] = 0ull;
-
-      if (pFact && mine) {
-        // Factored point model: pair m = 4a + b holds channels (8a + b, 8a + b + 4).
-        // G pairs (G_b, G_b+4) = A z0 (s^b, s^(b+4)) by a packed chain of three
-        // steps; H_a = s^(8a) from the (row, component) prepass; then one packed
-        // complex multiply-accumulate per pair of evaluations (a = 0: add).
-        const int nc = min(ct, ncomp - c0);
-        const float4* sSd = sS + bd.dfc * ct * R;
-        const float2* sTd = sT + bd.dfc * ct * R;
-        // anchor A exp(2 pi i P f0) of component c, one component ahead of
-        // the multiply-accumulates so that its latency (shared loads,
-        // split-FP32 product, MUFU) overlaps them; the tile is zero-filled to
-        // ct components, so the look-ahead index is clamped to the tile.
-        // Spectral-factored: amplitude A exp(e0') and steps w = s exp(e1'),
-        // w^4 = s^4 exp(4 e1'), w^8 = s^8 exp(8 e1').
-        auto anchor = [&](int c, float2& g, float4& st, float2& s8) {
-          const int i = c * R + tr;
-          const float2 Pp = sP[i];
-          st = sSd[i];
-          s8 = sTd[i];
-          g = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, f0));
-          if constexpr (pSF) {
-            const float4 fa = sF[c * Bt + tb];
-            g.x *= fa.x;
-            g.y *= fa.x;
-            st.x *= fa.y;
-            st.y *= fa.y;
-            st.z *= fa.z;
-            st.w *= fa.z;
-            s8.x *= fa.w;
-            s8.y *= fa.w;
-          } else {
-            const float A = sComp[c * p.cstride];
-            g.x *= A;
-            g.y *= A;
-          }
-        };
-        float2 gn, s8n;
-        float4 stn;
-        anchor(0, gn, stn, s8n);
-        for (int c = 0; c < nc; c++) {
-          const float2 g0 = gn, s8 = s8n;
-          const float4 st = stn;
-          anchor(min(c + 1, ct - 1), gn, stn, s8n);
-          const float2 g4 = cmul(g0, make_float2(st.z, st.w));
-          f2x GR[4], GI[4];
-          GR[0] = pk2(g0.x, g4.x);
-          GI[0] = pk2(g0.y, g4.y);
-          const f2x SR = pk2(st.x, st.x), SI = pk2(st.y, st.y), NSI = pk2(-st.y, -st.y);
-#pragma unroll
-          for (int b = 1; b < 4; b++) {
-            const f2x t1 = mul2(GI[b - 1], NSI);
-            const f2x t2 = mul2(GI[b - 1], SR);
-            GR[b] = fma2(GR[b - 1], SR, t1);
-            GI[b] = fma2(GR[b - 1], SI, t2);
-          }
-#pragma unroll
-          for (int b = 0; b < 4; b++) {
-            AR[b] = add2(AR[b], GR[b]);
-            AI[b] = add2(AI[b], GI[b]);
-          }
-          float2 h = s8;
-#pragma unroll
-          for (int a = 1; a < K / 8; a++) {
-            if (a > 1) h = cmul(h, s8);
-            const f2x HR = pk2(h.x, h.x), HI = pk2(h.y, h.y), NHI = pk2(-h.y, -h.y);
-#pragma unroll
-            for (int b = 0; b < 4; b++) {
-              const int m = 4 * a + b;
-              AR[m] = fma2(GR[b], HR, AR[m]);
-              AR[m] = fma2(GI[b], NHI, AR[m]);
-              AI[m] = fma2(GR[b], HI, AI[m]);
-              AI[m] = fma2(GI[b], HR, AI[m]);
-            }
-          }
-        }
-      }
-      if (!pFact && mine) {
-        const int nc = min(ct, ncomp - c0);
-        const float df = bd.df;
-        const float4* sSd = sS + bd.dfc * ct * R;
-        // Components in pairs: two prologues and four rotation chains in flight
-        // (the tile is zero-filled past ncomp, so a padded partner adds zero).
-        // A Gaussian taper adds five packed registers per chain pair; at 32
-        // channels per thread two components' state no longer fits beside the
-        // sums, so those take one component at a time.
-        constexpr bool kPairs = !(PF::kGaussian && K >= 32);
-        auto table = [&](int c) {
-          return reinterpret_cast<const ulonglong2*>(sG) + (c * Bt + tb) * TE;
-        };
-        auto entry = [&](const ulonglong2* G, int jj) {
-          if constexpr (PF::kTable) return G[jj];
-          else return make_ulonglong2(0ull, 0ull);
-        };
-        if constexpr (!kPairs) {
-          for (int c = 0; c < nc; c++) {
-            CompChains<H> x;
-            comp_setup<PM, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp,
-                                p.cstride, f0, bd, df, p.nterm);
-            const ulonglong2* Gx = table(c);
-#pragma unroll
-            for (int jj = 0; jj < Q; jj++) {
-              const ulonglong2 gx = entry(Gx, jj);
-              chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI,
-                               x.NSI);
-              chain_step<PM>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
-                               x.SR, x.SI, x.NSI);
-            }
-          }
-        }
-        const int ncp = kPairs ? min(ct, (nc + 1) & ~1) : 0;
-        for (int c = 0; c < ncp; c += 2) {
-          CompChains<H> x, y;
-          comp_setup<PM, H>(x, c, sP[c * R + tr], sSd[c * R + tr], sQ, c * R + tr, sComp, p.cstride,
-                              f0, bd, df, p.nterm);
-          comp_setup<PM, H>(y, c + 1, sP[(c + 1) * R + tr], sSd[(c + 1) * R + tr], sQ,
-                              (c + 1) * R + tr, sComp, p.cstride, f0, bd, df, p.nterm);
-          const ulonglong2* Gx = table(c);
-          const ulonglong2* Gy = table(c + 1);
-          if constexpr (PF::kChains == 1) {
-#pragma unroll
-            for (int jj = 0; jj < H; jj++) {
-              chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, 0ull, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
-              chain_step<PM>(AR[jj], AI[jj], y.ZRa, y.ZIa, 0ull, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
-            }
-            continue;
-          }
-#pragma unroll
-          for (int jj = 0; jj < QE; jj++) {
-            const ulonglong2 gx = entry(Gx, jj), gy = entry(Gy, jj);
-            chain_step<PM>(AR[jj], AI[jj], x.ZRa, x.ZIa, gx.x, x.GGa, x.HHa, x.QQ, x.SR, x.SI, x.NSI);
-            chain_step<PM>(AR[jj], AI[jj], y.ZRa, y.ZIa, gy.x, y.GGa, y.HHa, y.QQ, y.SR, y.SI, y.NSI);
-            if constexpr (Q > 0) {
-              chain_step<PM>(AR[jj + Q], AI[jj + Q], x.ZRb, x.ZIb, gx.y, x.GGb, x.HHb, x.QQ,
-                               x.SR, x.SI, x.NSI);
-              chain_step<PM>(AR[jj + Q], AI[jj + Q], y.ZRb, y.ZIb, gy.y, y.GGb, y.HHb, y.QQ,
-                               y.SR, y.SI, y.NSI);
-            }
-          }
-        }
-      }
-      // compensated fold of this tile's partial sums
-      if constexpr (pFact) {  // compensation terms in shared memory
-        f2x* cmp = sCmp + threadIdx.x;
-        const int nt = blockDim.x;
-        if constexpr (pSF) {  // the tile's quadratic spectral factor
-#pragma unroll
-          for (int j = 0; j < H; j++) {
-            const f2x ph = sPhi[tb * H + j];
-            AR[j] = mul2(AR[j], ph);
-            AI[j] = mul2(AI[j], ph);
-          }
-        }
-        if constexpr (pRemap) {
-          // factored pair m = 4a + b holds channels (8a + b, 8a + b + 4); chain
-          // pair j holds (j, j + H): channel c sits in factored pair
-          // 4 (c / 8) + c % 4, lane (c / 4) % 2
-          float xr[K], xi[K];
-#pragma unroll
-          for (int m = 0; m < H; m++) {
-            const int c1 = 8 * (m >> 2) + (m & 3);
-            up2(AR[m], xr[c1], xr[c1 + 4]);
-            up2(AI[m], xi[c1], xi[c1 + 4]);
-          }
-#pragma unroll
-          for (int j = 0; j < H; j++) {
-            AR[j] = pk2(xr[j], xr[j + H]);
-            AI[j] = pk2(xi[j], xi[j + H]);
-          }
-        }
-#pragma unroll
-        for (int j = 0; j < H; j++) {
-          f2x c = cmp[(2 * j) * nt];
-          f2x y = sub2(AR[j], c);
-          f2x s = add2(TR[j], y);
-          cmp[(2 * j) * nt] = sub2(sub2(s, TR[j]), y);
-          TR[j] = s;
-          c = cmp[(2 * j + 1) * nt];
-          y = sub2(AI[j], c);
-          s = add2(TI[j], y);
-          cmp[(2 * j + 1) * nt] = sub2(sub2(s, TI[j]), y);
-          TI[j] = s;
-        }
-        continue;
-      }
-#pragma unroll
-      for (int j = 0; j < H; j++) {
-        f2x y = sub2(AR[j], CR[j]);
-        f2x s = add2(TR[j], y);
-        CR[j] = sub2(sub2(s, TR[j]), y);
-        TR[j] = s;
-        y = sub2(AI[j], CI[j]);
-        s = add2(TI[j], y);
-        CI[j] = sub2(sub2(s, TI[j]), y);
-        TI[j] = s;
-      }
-    }
-      return true;
-    };
+    // The component tiles of a work item.  dft_recur_tile.inc is the body of
+    // one tile; it reads the pass's names defined before each loop: PM (the
+    // table's model family), PF = Fields<PM>, pSF (spectral-factored form),
+    // pFact (factored form), pChainTable, pRemap (factored partial sums folded
+    // in the chain form's pairing), tab and ncomp (the table and its size).
     if constexpr (kMixOn) {
-      if (!pass(PassTag<kPtMode, true, true>{})) return false;
+      {  // the untapered components: point sub-table, spectral-factored form
+        constexpr int PM = kPtMode;
+        using PF = Fields<PM>;
+        constexpr bool pSF = true, pFact = true, pChainTable = false, pRemap = true;
+        const float* const tab = p.compsPt;
+        const int ncomp = p.ncompPt;
+        for (int c0 = 0; c0 < ncomp; c0 += ct) {
+#include "dft_recur_tile.inc"
+        }
+      }
       {  // the Gaussian pass continues the compensated totals in registers
         const f2x* cmp = sCmp + threadIdx.x;
         const int nt = blockDim.x;
@@ -846,9 +477,25 @@ __device__ __forceinline__ bool recur_item(const KParams& p, int item, float* sm
           CI[j] = cmp[(2 * j + 1) * nt];
         }
       }
-      if (!pass(PassTag<MODE, false, false>{})) return false;
+      {  // the Gaussian components, chain form
+        constexpr int PM = MODE;
+        using PF = Fields<PM>;
+        constexpr bool pSF = false, pFact = false, pChainTable = false, pRemap = false;
+        const float* const tab = p.comps;
+        const int ncomp = p.ncomp;
+        for (int c0 = 0; c0 < ncomp; c0 += ct) {
+#include "dft_recur_tile.inc"
+        }
+      }
     } else {
-      if (!pass(PassTag<MODE, kSF, false>{})) return false;
+      constexpr int PM = MODE;
+      using PF = Fields<PM>;
+      constexpr bool pSF = kSF, pFact = kFact, pChainTable = kChainTable, pRemap = false;
+      const float* const tab = p.comps;
+      const int ncomp = p.ncomp;
+      for (int c0 = 0; c0 < ncomp; c0 += ct) {
+#include "dft_recur_tile.inc"
+      }
     }
 
     // stage the tile's model and apply it to the records

@@ -23,6 +23,8 @@ struct LayoutDesc {
   std::vector<double> fscale;         // nu/nu_uvref per (chan, IF) table index
   std::vector<double> lnspec;         // Spec: ln(nu/nu_model); TSpec: ln(nu/nu_plane)
   std::vector<int> specIndex;         // TSpec plane per (chan, IF)
+  std::vector<int> blockKey;          // optional, per (chan, IF): blocks never span a change
+                                      // (the beam kernel's Jones plane)
 };
 
 struct ModelDesc {

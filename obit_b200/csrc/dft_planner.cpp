@@ -138,11 +138,14 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
   for (int iIF = L.ifb; iIF <= L.ife; iIF++) {
     int ch = L.chanb;
     while (ch <= L.chane) {
-      // run of channels sharing a plane
+      // run of channels sharing a plane (and a block key)
       int end = ch;
       const int plane = tspec ? L.specIndex[ch * L.kincf + iIF * L.kincif] : 0;
+      const bool keyed = (int)L.blockKey.size() >= nfreq;
+      const int key = keyed ? L.blockKey[ch * L.kincf + iIF * L.kincif] : 0;
       while (end + 1 <= L.chane &&
-             (!tspec || L.specIndex[(end + 1) * L.kincf + iIF * L.kincif] == plane))
+             (!tspec || L.specIndex[(end + 1) * L.kincf + iIF * L.kincif] == plane) &&
+             (!keyed || L.blockKey[(end + 1) * L.kincf + iIF * L.kincif] == key))
         end++;
       for (int c0 = ch; c0 <= end; c0 += K) {
         int len = std::min(K, end - c0 + 1);

@@ -48,17 +48,21 @@ struct BeamState {
   const float* jones = nullptr;
   int* d_antType = nullptr;
   int* d_jchan = nullptr;
+  std::vector<int> jchan;  // host copy: the planner cuts blocks at Jones-plane changes
   double* d_fscale = nullptr;
   double* d_lnspec = nullptr;
   int* d_plane = nullptr;
+  BlockDesc* d_blocks = nullptr;  // channel blocks of the beam plan
   BeamKParams kp{};
 };
 
 void free_beam_tables(BeamState& b) {
-  for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane}) if (q) cudaFree(q);
+  for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane, (void*)b.d_blocks})
+    if (q) cudaFree(q);
   b.d_fscale = nullptr;
   b.d_lnspec = nullptr;
   b.d_plane = nullptr;
+  b.d_blocks = nullptr;
 }
 
 struct State {
@@ -284,24 +288,41 @@ int ensure_plan(GPUInfo* g, State* s) {
     if ((int)L.specIndex.size() >= nfreq &&
         (rc = upload(L.specIndex.data(), sizeof(int) * nfreq, (void**)&b.d_plane)))
       return rc;
+    // channel blocks of at most kBeamK channels that never span a change of
+    // Jones plane (recurrence form), from the same planner
+    LayoutDesc LB = L;
+    LB.blockKey = b.jchan;
+    TuneDesc TB;
+    TB.flavor = kFlavorRecur;
+    TB.K = kBeamK;
+    TB.threads = kThreads;
+    TB.specFactor = 0;
+    Plan bplan;
+    rc = plan_layout(LB, s->mc.model, A, TB, &bplan, &err);
+    if (rc) return fail(rc, err);
+    const int nb = (int)bplan.blocks.size();
+    CUDA_TRY(cudaMalloc(&b.d_blocks, sizeof(BlockDesc) * (size_t)std::max(1, nb)));
+    if (nb)
+      CUDA_TRY(cudaMemcpy(b.d_blocks, bplan.blocks.data(), sizeof(BlockDesc) * (size_t)nb,
+                          cudaMemcpyHostToDevice));
     BeamKParams& k = b.kp;
     k = BeamKParams{};
-    k.lrec = L.lrec;
+    k.k = bplan.kp;
+    k.k.blocks = b.d_blocks;
+    k.k.comps = s->d_comps;
+    k.k.ncomp = s->mc.model.ncomp;
+    k.k.errFlag = s->d_err;
+    k.k.rowBase = 0;
+    k.k.waitPolls = kDefaultWaitPolls;
     k.nrparm = L.nrparm;
-    k.ilocu = L.ilocu;
-    k.ilocv = L.ilocv;
-    k.ilocw = L.ilocw;
     k.ilocb = b.ilocb;
     k.iloca1 = b.iloca1;
     k.iloca2 = b.iloca2;
-    k.incs = L.incs;
-    k.incf = L.incf;
     k.incif = L.incif;
     k.ncorr = L.nstok >= 4 ? 4 : std::min(2, L.nstok);
     if ((long long)L.nrparm + (long long)L.ife * L.incif + (long long)L.chane * L.incf +
             (long long)(k.ncorr - 1) * L.incs + 2 >= L.lrec)
       return fail(OBIT_DFT_EBADARG, "modelled correlations extend past the record");
-    k.op = A.op;
     for (int q = 0; q < 4; q++) k.polFact[q] = s->mc.stokFact[q];
     k.chanb = L.chanb;
     k.nchanSel = L.chane - L.chanb + 1;
@@ -319,20 +340,12 @@ int ensure_plan(GPUInfo* g, State* s) {
     k.numJChan = b.numJChan;
     k.jones = b.jones;
     k.jonesComps = b.jonesComps;
-    k.comps = s->d_comps;
-    k.ncomp = s->mc.model.ncomp;
-    k.cstride = comp_stride(s->mc.model);
-    // component tile: 128, or fewer so that the tile's coefficients (every
-    // type pair and plane) stay within 96 KB of shared memory
-    const size_t perComp =
-        sizeof(float) * ((size_t)k.cstride + (size_t)b.numAntType * b.numAntType * b.numJChan * 8);
-    k.ct = (int)std::max<size_t>(1, std::min<size_t>(128, (96 * 1024) / perComp));
-    k.nterm = s->mc.model.nterm;
     k.mode = s->mc.model.kind;
-    k.errFlag = s->d_err;
     k.stokType = b.stokType;
     k.c2p = b.c2p;
     k.s2p = b.s2p;
+    k.flavor = (s->tune.flavor == kFlavorPlain) ? kFlavorPlain : kFlavorRecur;
+    if ((rc = beam_fit_tile(&k, &err))) return fail(rc, err);
   }
   s->planValid = true;
   return OBIT_DFT_OK;
@@ -481,6 +494,7 @@ int obit_dft_set_beam(GPUInfo* g, const ObitDFTBeam* beam) {
   CUDA_TRY(cudaMemcpy(b.d_antType, beam->antType, sizeof(int) * beam->numAnt, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMalloc(&b.d_jchan, sizeof(int) * nfreq));
   CUDA_TRY(cudaMemcpy(b.d_jchan, beam->jchan, sizeof(int) * nfreq, cudaMemcpyHostToDevice));
+  b.jchan.assign(beam->jchan, beam->jchan + nfreq);
   b.numAnt = beam->numAnt;
   b.numAntType = beam->numAntType;
   b.numJChan = beam->numJChan;
@@ -594,8 +608,8 @@ int obit_dft_calc_device(GPUInfo* g, float* d_vis, int nvis, void* stream) {
   std::string err;
   if (s->beam.on) {
     BeamKParams k = s->beam.kp;
-    k.vis = d_vis;
-    k.nvis = nvis;
+    k.k.vis = d_vis;
+    k.k.nvis = nvis;
     rc = launch_beam(k, (cudaStream_t)stream, &err);
   } else {
     rc = launch_plan(s->plan, d_vis, 0, nvis, s->runComps, s->d_err, (cudaStream_t)stream, &err);
@@ -693,8 +707,8 @@ int obit_dft_calc(GPUInfo* g) {
     CUDA_TRY(cudaMemcpyAsync(bufs[b], host, bytes, cudaMemcpyHostToDevice, streams[b]));
     if (s->beam.on) {
       BeamKParams k = s->beam.kp;
-      k.vis = bufs[b];
-      k.nvis = nr;
+      k.k.vis = bufs[b];
+      k.k.nvis = nr;
       rc = launch_beam(k, streams[b], &err);
     } else {
       rc = launch_plan(s->plan, bufs[b], 0, nr, s->runComps, s->d_err, streams[b], &err);

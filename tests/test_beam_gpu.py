@@ -17,12 +17,14 @@ from test_beam_oracle_cpu import beam_case
 pytestmark = pytest.mark.gpu
 
 
-def _run_beam(uv, sky, p, beam, torch, jones=None):
+def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None):
     out = uv.copy()
     d_jones = torch.from_numpy(np.ascontiguousarray(jones if jones is not None else beam.jones)).cuda()
     gm = GPUSkyModel("beam")
     try:
         gm.DFTInit(sky, out, SkyModelParams(**{**p.__dict__, "nVisPIO": uv.nvis}))
+        if flavor is not None:
+            gm.set_kernel(flavor)
         gm.set_beam(beam, d_jones.data_ptr())
         gm.DFTSetMod(sky)
         gm.DFTCalc(out)
@@ -148,3 +150,35 @@ def test_beam_polarized_skies(stok):
     got = _run_beam(uv, sky, p, beam, torch)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
+
+
+@pytest.mark.parametrize("flavor", [_lib.OBIT_DFT_RECUR, _lib.OBIT_DFT_PLAIN])
+@pytest.mark.parametrize("mt", [U.MOD_POINT_SPEC, U.MOD_GAUSS_TSPEC])
+def test_beam_jones_planes_inside_blocks(flavor, mt):
+    """Seven Jones planes over 2 x 27 channels: plane changes fall inside the
+    recurrence form's 8-channel blocks, which the planner cuts there; the
+    recurrence form and the per-channel comparator both match the oracle."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(mt=mt, nstok=4, nrow=45, nchan=27, nif=2, ncomp=140, seed=41, njc=7,
+                              flag_frac=0.1)
+    p = SkyModelParams(op=OP_SUB)
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
+
+
+def test_beam_selection_and_one_correlation():
+    """A channel and IF selection on single-correlation records."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=1, nrow=40, nchan=30, nif=3, ncomp=100, seed=43, njc=4)
+    p = SkyModelParams(op=OP_SUB, startChannel=4, numberChannel=19, startIF=2, numberIF=2)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    b = want[:, uv.nrparm:].reshape(a.shape)
+    src = uv.vis_view()
+    mask = np.zeros(a.shape[:-1], bool)
+    mask[:, 1:3, 3:22, :] = True
+    assert np.array_equal(a[~mask], src[~mask])
+    d = np.abs((a[..., 0, 0] - b[..., 0, 0]) + 1j * (a[..., 0, 1] - b[..., 0, 1]))[:, 1:3, 3:22]
+    assert np.max(d / np.maximum(l1[:, 1:3, 3:22, 0], 1e-30)) < TOL_REL + 1e-6
