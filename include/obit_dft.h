@@ -216,9 +216,48 @@ typedef struct ObitDFTBeam {
   const float *jones;    /* device, 16-byte aligned: [numAntType][jonesComps][numJChan] 2x2
                             complex matrices of 8 floats (XX, XY, YX, YY as re, im) */
   int jonesComps;        /* components per type in jones, at least the model's */
-  float parAng;          /* parallactic angle, radians (Stokes Q and U) */
+  float parAng;          /* parallactic angle, radians (Stokes Q and U, linear feeds) */
+  int circular;          /* 1: circular feeds, records RR, LL, RL, LR and Jones matrices
+                            in the R, L basis; 0: linear feeds (XX, YY, XY, YX) */
 } ObitDFTBeam;
 int obit_dft_set_beam(GPUInfo *gpuInfo, const ObitDFTBeam *beam);
+
+/* Beam images from which the Jones table is interpolated: for every antenna
+ * type the 8 images of GetJonesKernel's interpolators
+ * (ObitCUDABeamModel.cu:1228-1299): P1 re, P1 im, P2 re, P2 im, X1 re, X1 im,
+ * X2 re, X2 im -- the parallel hands (XX or RR, YY or LL) and the cross terms
+ * (XY or RL, YX or LR) -- each nplane planes (the Jones planes) of ny rows of
+ * nx pixels, on one pixel grid. */
+typedef struct ObitDFTBeamImages {
+  int numAntType;        /* antenna types */
+  int nx, ny, nplane;    /* pixels per row, rows, planes */
+  const float *pixels;   /* device: [numAntType][8][nplane][ny][nx] */
+  float fblank;          /* value of blanked pixels */
+  int hwidth;            /* Lagrange interpolation half-width, 1..4 (2 hwidth + 1 taps per axis) */
+  int projection;        /* 0: linear offsets, 1: -SIN about crval */
+  double crval[2];       /* reference position of the grid (deg) */
+  float crpix[2];        /* reference pixel (1-relative) */
+  float cdelt[2];        /* pixel increments (deg) */
+  const float *planeFreq;/* host [nplane]: frequency (Hz) of each plane */
+  float refSizeFact;     /* primary-beam factor of InvBeam (ObitCUDABeamModel.cu:66-72):
+                            antenna size x 1.052 x DG2RAD / VELIGHT, per Hz per degree */
+} ObitDFTBeamImages;
+
+/* Fill a Jones table in the layout of ObitDFTBeam.jones ([numAntType][ncomp]
+ * [nplane] 2x2 complex matrices of 8 floats, device, 16-byte aligned) by
+ * interpolating the beam images at each component's position, as
+ * GetJonesKernel does: the pixel of the position rotated by the parallactic
+ * angle parAng (radians), a Lagrange interpolation of each image in each
+ * plane (taps on blanked pixels dropped; blank when the remaining weight is
+ * at most 0.9), each value times the inverse primary-beam gain of the
+ * component's offset, and the unit matrix where the position is off the
+ * grid, the gain factor is 10 or more, a parallel hand's real part exceeds
+ * 1.3, or an interpolant is blank (the reference tests P1's real part twice
+ * where P2's is meant, and lets blanks through the cross terms).  pos:
+ * device [ncomp][2], each component's offset from the pointing centre (deg)
+ * in the grid's coordinates.  Asynchronous on `stream`. */
+int obit_dft_beam_jones(const ObitDFTBeamImages *images, const float *pos, int ncomp, float parAng,
+                        float *jones, void *stream);
 
 /* FP64 frequency side table (no reference counterpart; the reference passes
  * only FP32 freqScale).  freqArr: nchan*nIF channel frequencies in Hz indexed

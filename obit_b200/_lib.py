@@ -110,7 +110,16 @@ class ObitDFTBeam(C.Structure):
         ("numAnt", C.c_int), ("numAntType", C.c_int), ("numJChan", C.c_int),
         ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
         ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int), ("stokType", C.c_int),
-        ("jones", C.c_void_p), ("jonesComps", C.c_int), ("parAng", C.c_float),
+        ("jones", C.c_void_p), ("jonesComps", C.c_int), ("parAng", C.c_float), ("circular", C.c_int),
+    ]
+
+
+class ObitDFTBeamImages(C.Structure):
+    _fields_ = [
+        ("numAntType", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nplane", C.c_int),
+        ("pixels", C.c_void_p), ("fblank", C.c_float), ("hwidth", C.c_int), ("projection", C.c_int),
+        ("crval", C.c_double * 2), ("crpix", C.c_float * 2), ("cdelt", C.c_float * 2),
+        ("planeFreq", C.POINTER(C.c_float)), ("refSizeFact", C.c_float),
     ]
 
 
@@ -134,6 +143,8 @@ SIGNATURES = {
     "obit_dft_set_poln": (C.c_int, [_GPUINFO_P, C.c_int, C.c_float, C.c_int]),
     "obit_dft_set_mod_d": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_double), C.c_int]),
     "obit_dft_set_beam": (C.c_int, [_GPUINFO_P, C.POINTER(ObitDFTBeam)]),
+    "obit_dft_beam_jones": (C.c_int, [C.POINTER(ObitDFTBeamImages), C.c_void_p, C.c_int, C.c_float,
+                                      C.c_void_p, C.c_void_p]),
     "obit_dft_set_kernel": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int, C.c_int]),
     "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),

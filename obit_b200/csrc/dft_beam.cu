@@ -77,6 +77,34 @@ __device__ __forceinline__ void beam_coeffs(const BeamKParams& p, const float* J
     pconj(J1r[x], J1i[x], J2r[y], J2i[y], re, im);
   };
   float r0, i0, r1, i1;
+  if (p.circular) {
+    // Circular feeds (ObitSkyModelVMBeamJonesCorSum, ObitSkyModelVMBeam.c:1039-1073
+    // and the product J1 W J2^H of its :1263-1268): correlation (a, b) of RR, RL,
+    // LR, LL is sum_ij M(i, j) P(2a + i, 2b + j) with the sky's matrix M:
+    //   I [[1, 0], [0, 1]]  Q [[0, 1], [1, 0]]  U [[0, i], [-i, 0]]  V [[1, 0], [0, -1]]
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int a = 2 * (q >> 1), b = 2 * (q & 1);
+      if (p.stokType == 1 || p.stokType == 4) {
+        P(a, b, r0, i0);
+        P(a + 1, b + 1, r1, i1);
+        const float sg = (p.stokType == 1) ? 1.0f : -1.0f;
+        cr[q] = r0 + sg * r1;
+        ci[q] = i0 + sg * i1;
+      } else {
+        P(a, b + 1, r0, i0);
+        P(a + 1, b, r1, i1);
+        if (p.stokType == 2) {
+          cr[q] = r0 + r1;
+          ci[q] = i0 + i1;
+        } else {  // U: i (P(a, b+1) - P(a+1, b))
+          cr[q] = -(i0 - i1);
+          ci[q] = r0 - r1;
+        }
+      }
+    }
+    return;
+  }
   if (p.stokType == 1) {
     const int a[4][4] = {{0, 0, 1, 1}, {1, 3, 0, 2}, {2, 0, 3, 1}, {2, 2, 3, 3}};
 #pragma unroll

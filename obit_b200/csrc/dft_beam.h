@@ -33,7 +33,8 @@ struct BeamKParams {
   int jonesComps;                // components per type in the Jones table (>= ncomp)
   int mode;                      // ModelKind
   int stokType;                  // sky Stokes: 1 I, 2 Q, 3 U, 4 V
-  float c2p, s2p;                // cos, sin of twice the parallactic angle (Q, U)
+  int circular;                  // 1: circular feeds (RR, LL, RL, LR), 0: linear
+  float c2p, s2p;                // cos, sin of twice the parallactic angle (linear Q, U)
   int flavor;                    // kFlavorRecur (blocks) or kFlavorPlain (one thread per channel)
 };
 

@@ -43,7 +43,7 @@ int fail(int code, const std::string& msg) {
 struct BeamState {
   bool on = false;
   int numAnt = 0, numAntType = 0, numJChan = 0, ilocb = -1, iloca1 = -1, iloca2 = -1;
-  int jonesComps = 0, stokType = 1;
+  int jonesComps = 0, stokType = 1, circular = 0;
   float c2p = 1.f, s2p = 0.f;
   const float* jones = nullptr;
   int* d_antType = nullptr;
@@ -342,6 +342,7 @@ int ensure_plan(GPUInfo* g, State* s) {
     k.jonesComps = b.jonesComps;
     k.mode = s->mc.model.kind;
     k.stokType = b.stokType;
+    k.circular = b.circular;
     k.c2p = b.c2p;
     k.s2p = b.s2p;
     k.flavor = (s->tune.flavor == kFlavorPlain) ? kFlavorPlain : kFlavorRecur;
@@ -504,6 +505,7 @@ int obit_dft_set_beam(GPUInfo* g, const ObitDFTBeam* beam) {
   b.jones = beam->jones;
   b.jonesComps = beam->jonesComps;
   b.stokType = beam->stokType;
+  b.circular = beam->circular ? 1 : 0;
   b.c2p = (float)std::cos(2.0 * (double)beam->parAng);
   b.s2p = (float)std::sin(2.0 * (double)beam->parAng);
   b.on = true;

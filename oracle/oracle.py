@@ -196,6 +196,7 @@ class OracleBeam(C.Structure):
         ("antType", C.POINTER(C.c_int)), ("jchan", C.POINTER(C.c_int)),
         ("ilocb", C.c_int), ("iloca1", C.c_int), ("iloca2", C.c_int),
         ("jones", C.POINTER(C.c_float)), ("stokType", C.c_int), ("c2p", C.c_double), ("s2p", C.c_double),
+        ("circular", C.c_int),
     ]
 
 
@@ -217,7 +218,8 @@ def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None):
     c2p = float(np.float32(np.cos(2.0 * float(beam.parAng))))
     s2p = float(np.float32(np.sin(2.0 * float(beam.parAng))))
     ob = OracleBeam(len(at), jo.shape[0], jo.shape[2], _p(at, C.c_int), _p(jc, C.c_int), beam.ilocb,
-                    beam.iloca1, beam.iloca2, _p(jo, C.c_float), int(beam.stokType), c2p, s2p)
+                    beam.iloca1, beam.iloca2, _p(jo, C.c_float), int(beam.stokType), c2p, s2p,
+                    int(bool(getattr(beam, "circular", False))))
     # the oracle indexes the table with the model's component count
     if jo.shape[1] != sky.ncomp:
         jo = np.ascontiguousarray(jo[:, :sky.ncomp])
@@ -280,4 +282,23 @@ def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):
     rc = lib_b().refcpu_apply(C.byref(jb.job), _p(out, C.c_float), nthreads or nthreads_default())
     if rc:
         raise ValueError(f"refcpu_apply returned {rc}")
+    return out
+
+
+def beam_jones_fp64(images, pos, par_ang: float):
+    """FP64 Jones table from beam images (oracle_beam.c: oracle_beam_jones).
+    images: obit_b200.beam.BeamImages (host pixels); pos: (ncomp, 2) offsets in
+    degrees.  Returns float32 (ntype, ncomp, nplane, 8)."""
+    px = np.ascontiguousarray(images.pixels, dtype=np.float32)
+    ntype, _, nplane, ny, nx = px.shape
+    pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros((ntype, pos.shape[0], nplane, 8), np.float32)
+    d3 = C.c_double * 2
+    pf = np.ascontiguousarray(images.planeFreq, dtype=np.float64)
+    lib = lib_a()
+    lib.oracle_beam_jones.restype = None
+    lib.oracle_beam_jones(ntype, nx, ny, nplane, _p(px, C.c_float), C.c_float(images.fblank),
+                          int(images.hwidth), int(images.projection), d3(*images.crval), d3(*images.crpix),
+                          d3(*images.cdelt), _p(pf, C.c_double), C.c_double(images.refSizeFact),
+                          C.c_double(par_ang), _p(pos, C.c_float), pos.shape[0], _p(out, C.c_float))
     return out

@@ -1,7 +1,7 @@
 /* Test infrastructure (never linked into the product): FP64 oracle of the
  * beam-corrected DFT, the model of ObitCUDABeamModel's beam*Kernel family
  * (ObitSystem/Obit/src/ObitCUDABeamModel.cu:139-1226) for linear feeds and a
- * Stokes I, Q, U or V sky.
+ * Stokes I, Q, U or V sky, and of the CPU path's circular-feed branch.
  *
  * For a record of baseline (a1, a2) with antenna types t1, t2 and a (channel,
  * IF) whose Jones plane is jc, each component contributes v = amp e^{i phase}
@@ -53,6 +53,37 @@ static int beam_ants(const OracleBeam *b, const float *rec, int *a1, int *a2) {
  * form them. */
 static void beam_coeffs(const OracleBeam *b, const float *J1, const float *J2, double cr[4],
                         double ci[4]) {
+  if (b->circular) {
+    /* Circular feeds: the model matrix is J1 M conj(J2)^T with the sky's
+     * pseudo-visibility matrix M of ObitSkyModelVMBeamJonesCorSum
+     * (ObitSystem/Obit/src/ObitSkyModelVMBeam.c:1039-1073, product at
+     * :1263-1268), per unit visibility:
+     *   I [[1, 0], [0, 1]]  Q [[0, 1], [1, 0]]  U [[0, i], [-i, 0]]  V [[1, 0], [0, -1]]
+     * element (a, b) -> correlation RR, RL, LR, LL = 2a + b. */
+    double mr[2][2] = {{0, 0}, {0, 0}}, mi[2][2] = {{0, 0}, {0, 0}};
+    switch (b->stokType) {
+      case 1: mr[0][0] = mr[1][1] = 1.0; break;
+      case 2: mr[0][1] = mr[1][0] = 1.0; break;
+      case 3: mi[0][1] = 1.0; mi[1][0] = -1.0; break;
+      default: mr[0][0] = 1.0; mr[1][1] = -1.0; break;
+    }
+    for (int a = 0; a < 2; a++)
+      for (int c = 0; c < 2; c++) {
+        double sr = 0.0, si = 0.0;
+        for (int i = 0; i < 2; i++)
+          for (int j = 0; j < 2; j++) {
+            /* J1(a, i) M(i, j) conj(J2(c, j)) */
+            const double ar = J1[2 * (2 * a + i)], ai = J1[2 * (2 * a + i) + 1];
+            const double br = J2[2 * (2 * c + j)], bi = -(double)J2[2 * (2 * c + j) + 1];
+            const double tr = ar * mr[i][j] - ai * mi[i][j], ti = ar * mi[i][j] + ai * mr[i][j];
+            sr += tr * br - ti * bi;
+            si += tr * bi + ti * br;
+          }
+        cr[2 * a + c] = sr;
+        ci[2 * a + c] = si;
+      }
+    return;
+  }
   double pr[4][4], pi[4][4];
   for (int x = 0; x < 4; x++)
     for (int y = 0; y < 4; y++) {
@@ -103,6 +134,7 @@ void oracle_beam_coeffs(int stokType, double c2p, double s2p, const float *J1, c
   OracleBeam b;
   memset(&b, 0, sizeof(b));
   b.stokType = stokType;
+  b.circular = 0;
   b.c2p = c2p;
   b.s2p = s2p;
   beam_coeffs(&b, J1, J2, cr, ci);
@@ -199,4 +231,98 @@ int oracle_beam_apply(const OracleJob *j, const OracleBeam *b, float *vis, doubl
   free(th);
   free(sl);
   return 0;
+}
+
+/* Jones table from beam images, FP64 (test infrastructure): the computation of
+ * GetJonesKernel (ObitSystem/Obit/src/ObitCUDABeamModel.cu:1228-1299) with
+ * CUDAPositionXYpix (ObitSystem/Obit/include/CUDASkyGeom.h:91-286, linear and
+ * -SIN grids), the Lagrange interpolator of CUDABeamInterpPixel /
+ * SetConvKernal (ObitSystem/Obit/include/CUDABeamInterp.h) and InvBeam
+ * (ObitCUDABeamModel.cu:66-72), with the unit matrix where the position is
+ * off the grid, the gain factor is 10 or more, a parallel hand's real part
+ * exceeds 1.3 or an interpolant is blank.  pixels: [ntype][8][nplane][ny][nx]
+ * (P1 re, im, P2 re, im, X1 re, im, X2 re, im); pos: [ncomp][2] (deg);
+ * jones out: [ntype][ncomp][nplane][8] (XX = P1, XY = X1, YX = X2, YY = P2). */
+void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixels, float fblank,
+                       int hwidth, int projection, const double crval[2], const double crpix[2],
+                       const double cdelt[2], const double *planeFreq, double refSizeFact,
+                       double parAng, const float *pos, int ncomp, float *jones) {
+  const double d2r = 1.745329252e-2;
+  const int iwid = 2 * hwidth + 1;
+  const size_t img = (size_t)nplane * ny * nx;
+  for (int t = 0; t < ntype; t++)
+    for (int c = 0; c < ncomp; c++) {
+      float *Jc = jones + ((size_t)t * ncomp + c) * nplane * 8;
+      double x = pos[2 * c], y = pos[2 * c + 1];
+      int ok = 1;
+      const double dx = x - crval[0];
+      if (dx > 180.0) x -= 360.0;
+      if (dx < -180.0) x += 360.0;
+      double l = x - crval[0], m = y - crval[1];
+      if (projection == 1) {
+        const double ra0 = crval[0] * d2r, dec0 = crval[1] * d2r, ra = x * d2r, dec = y * d2r;
+        const double sint = sin(dec) * sin(dec0) + cos(dec) * cos(dec0) * cos(ra - ra0);
+        if (sint < 0.0) ok = 0;
+        l = sin(ra - ra0) * cos(dec) / d2r;
+        m = (sin(dec) * cos(dec0) - cos(dec) * sin(dec0) * cos(ra - ra0)) / d2r;
+      }
+      const double lr = l * cos(parAng) + m * sin(parAng), mr = m * cos(parAng) - l * sin(parAng);
+      const double px = lr / cdelt[0] + crpix[0], py = mr / cdelt[1] + crpix[1];
+      if (!ok || px < 1.0 || px > nx || py < 1.0 || py > ny) {
+        for (int k = 0; k < nplane; k++) {
+          float *J = Jc + 8 * k;
+          for (int e = 0; e < 8; e++) J[e] = (e == 0 || e == 6) ? 1.0f : 0.0f;
+        }
+        continue;
+      }
+      /* Lagrange taps on each axis: nodes 1..iwid counted from the first tap */
+      double w[2][9];
+      int start[2];
+      const double pix[2] = {px, py};
+      const int n[2] = {nx, ny};
+      for (int a = 0; a < 2; a++) {
+        int cen = (int)(pix[a] + 0.5) - hwidth;
+        if (cen > n[a] - iwid + 1) cen = n[a] - iwid + 1;
+        if (cen < 1) cen = 1;
+        start[a] = cen - 1;
+        const double xx = pix[a] - (double)(cen - 1);
+        for (int j = 0; j < iwid; j++) {
+          double prod = 1.0, den = 1.0;
+          for (int i = 0; i < iwid; i++)
+            if (i != j) {
+              prod *= xx - (i + 1);
+              den *= (double)(j - i);
+            }
+          w[a][j] = prod / den;
+        }
+      }
+      const double ang = sqrt(x * x + y * y);
+      for (int k = 0; k < nplane; k++) {
+        double v[8];
+        int blank = 0;
+        for (int q = 0; q < 8; q++) {
+          const float *d = pixels + ((size_t)t * 8 + q) * img + (size_t)k * ny * nx;
+          double sum = 0.0, sumwt = 0.0;
+          for (int j = 0; j < iwid; j++)
+            for (int i = 0; i < iwid; i++) {
+              const float val = d[(size_t)(start[1] + j) * nx + start[0] + i];
+              if (val != fblank) {
+                sumwt += w[0][i] * w[1][j];
+                sum += val * w[0][i] * w[1][j];
+              }
+            }
+          if (sumwt > 0.90) v[q] = sum / sumwt;
+          else blank = 1;
+        }
+        const double arg = refSizeFact * planeFreq[k] * ang;
+        const double g = (arg > 1.02) ? 100.0 : (1.0 - 4.0 * arg * arg) / cos(3.141592653589793 * arg);
+        float *J = Jc + 8 * k;
+        if (blank || !(g < 10.0) || !(fabs(g * v[0]) <= 1.3) || !(fabs(g * v[2]) <= 1.3)) {
+          for (int e = 0; e < 8; e++) J[e] = (e == 0 || e == 6) ? 1.0f : 0.0f;
+          continue;
+        }
+        const int src[8] = {0, 1, 4, 5, 6, 7, 2, 3};
+        for (int e = 0; e < 8; e++) J[e] = (float)(g * v[src[e]]);
+      }
+    }
 }

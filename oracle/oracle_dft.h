@@ -99,7 +99,8 @@ typedef struct OracleBeam {
   int iloca1, iloca2;   /* ANTENNA1 / ANTENNA2 offsets when ilocb < 0 */
   const float *jones;   /* [numAntType][ncomp][numJChan][8]: XX, XY, YX, YY complex */
   int stokType;         /* 1..4 = I, Q, U, V sky */
-  double c2p, s2p;      /* cos, sin of twice the parallactic angle (Q, U) */
+  double c2p, s2p;      /* cos, sin of twice the parallactic angle (linear Q, U) */
+  int circular;         /* 1: circular feeds (RR, LL, RL, LR), 0: linear */
 } OracleBeam;
 
 /* Applies the beam-corrected FP64 model (Stokes I, linear feeds) to the
@@ -107,6 +108,10 @@ typedef struct OracleBeam {
  * YX), the job's channel / IF selection and operation.  l1 (may be NULL)
  * receives per (row, table index, model correlation XX/XY/YX/YY) the sum over
  * components of |amp| |coefficient|.  Returns 0, or < 0 for a bad job. */
+void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixels, float fblank,
+                       int hwidth, int projection, const double crval[2], const double crpix[2],
+                       const double cdelt[2], const double *planeFreq, double refSizeFact,
+                       double parAng, const float *pos, int ncomp, float *jones);
 int oracle_beam_apply(const OracleJob *job, const OracleBeam *beam, float *vis, double *l1,
                       int nthreads);
 

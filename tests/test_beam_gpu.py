@@ -182,3 +182,17 @@ def test_beam_selection_and_one_correlation():
     assert np.array_equal(a[~mask], src[~mask])
     d = np.abs((a[..., 0, 0] - b[..., 0, 0]) + 1j * (a[..., 0, 1] - b[..., 0, 1]))[:, 1:3, 3:22]
     assert np.max(d / np.maximum(l1[:, 1:3, 3:22, 0], 1e-30)) < TOL_REL + 1e-6
+
+
+@pytest.mark.parametrize("stok", [1, 2, 3, 4])
+def test_beam_circular_feeds(stok):
+    """Circular feeds (records RR, LL, RL, LR; Jones matrices in the R, L basis),
+    Stokes I, Q, U and V skies: the model J1 M J2^H of the CPU path's circular
+    branch."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=4, nrow=45, nchan=20, nif=2, ncomp=110, seed=51 + stok, flag_frac=0.1,
+                              stok=stok, circular=True)
+    p = SkyModelParams(op=OP_SUB)
+    got = _run_beam(uv, sky, p, beam, torch)
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)

@@ -14,7 +14,7 @@ from obit_b200.skymodel import OP_REPL, OP_SUB, SkyModelParams
 
 
 def beam_case(mt=U.MOD_POINT_SPEC, nstok=4, nrow=30, nchan=12, nif=2, ncomp=25, seed=5, unit=False,
-              ntype=2, njc=3, flag_frac=0.0, stok=1, par_ang=0.0):
+              ntype=2, njc=3, flag_frac=0.0, stok=1, par_ang=0.0, circular=False):
     uv, sky = small(mt, nrow=nrow, nchan=nchan, nif=nif, nstok=nstok, ncomp=ncomp, seed=seed,
                     flag_frac=flag_frac)
     uv.vis[:, 3] = baseline_codes(12, uv.nvis)
@@ -26,7 +26,7 @@ def beam_case(mt=U.MOD_POINT_SPEC, nstok=4, nrow=30, nchan=12, nif=2, ncomp=25, 
         jones += (0.2 * r.standard_normal(jones.shape)).astype(np.float32)
     ant_type = r.integers(0, ntype, 12)
     jchan = (np.arange(nchan * nif) * njc // (nchan * nif)).astype(np.int32)
-    return uv, sky, Beam(ant_type, jchan, jones, stokType=stok, parAng=par_ang)
+    return uv, sky, Beam(ant_type, jchan, jones, stokType=stok, parAng=par_ang, circular=circular)
 
 
 def np_beam_model(uv, sky, beam):
@@ -57,7 +57,15 @@ def np_beam_model(uv, sky, beam):
                 c2, s2 = (float(np.float32(np.cos(2 * beam.parAng))), float(np.float32(np.sin(2 * beam.parAng))))
                 D = [P(0, 0) - P(1, 1), P(0, 2) - P(1, 3), P(2, 0) - P(3, 1), P(2, 2) - P(3, 3)]
                 S = [P(1, 0) + P(0, 1), P(1, 2) + P(0, 3), P(3, 0) + P(2, 1), P(3, 2) + P(2, 3)]
-                if beam.stokType == 1:
+                if beam.circular:
+                    # J1 M J2^H per component, M the sky's matrix in the R, L basis
+                    M = {1: [[1, 0], [0, 1]], 2: [[0, 1], [1, 0]], 3: [[0, 1j], [-1j, 0]],
+                         4: [[1, 0], [0, -1]]}[beam.stokType]
+                    m1 = j1.reshape(-1, 2, 2)
+                    m2 = j2.reshape(-1, 2, 2)
+                    prod = m1 @ np.asarray(M, np.complex128) @ np.conj(np.transpose(m2, (0, 2, 1)))
+                    C = [prod[:, 0, 0], prod[:, 0, 1], prod[:, 1, 0], prod[:, 1, 1]]
+                elif beam.stokType == 1:
                     C = [P(0, 0) + P(1, 1), P(1, 3) + P(0, 2), P(2, 0) + P(3, 1), P(2, 2) + P(3, 3)]
                 elif beam.stokType == 2:
                     C = [c2 * D[q] - s2 * S[q] for q in range(4)]
@@ -85,9 +93,11 @@ def test_unit_jones_is_the_plain_dft():
     assert np.allclose(l1[..., 0], dl1) and np.allclose(l1[..., 3], dl1) and np.all(l1[..., 1] == 0)
 
 
+@pytest.mark.parametrize("circular", [False, True])
 @pytest.mark.parametrize("nstok,stok", [(2, 1), (4, 1), (4, 2), (4, 3), (4, 4)])
-def test_random_jones_match_numpy(nstok, stok):
-    uv, sky, beam = beam_case(nstok=nstok, nrow=12, nchan=6, ncomp=9, stok=stok, par_ang=0.7)
+def test_random_jones_match_numpy(nstok, stok, circular):
+    uv, sky, beam = beam_case(nstok=nstok, nrow=12, nchan=6, ncomp=9, stok=stok, par_ang=0.7,
+                              circular=circular)
     got, l1 = oracle.apply_beam_fp64(uv, sky, SkyModelParams(op=OP_REPL), beam)
     want = np_beam_model(uv, sky, beam)
     v = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
