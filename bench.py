@@ -82,6 +82,10 @@ def parse():
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
                          "96-facet uneven batch; beam: the beam-corrected DFT on the config-2 "
                          "layout")
+    ap.add_argument("--e2e-row-scale", type=float, default=0.002,
+                    help="config5: row scale of the host-memory (streamed) end-to-end pass")
+    ap.add_argument("--staging-gb", type=float, default=1.0,
+                    help="config5: device staging area of the streamed end-to-end pass (GiB)")
     ap.add_argument("--row-scale", type=float, default=0.01,
                     help="config5: fraction of each facet's drawn rows held in HBM")
     ap.add_argument("--no-autotune", action="store_true", help="config5: keep the planner's tile")
@@ -384,12 +388,22 @@ def config_block(g: Geometry, nrow_override=None, kernel=None):
             "kernel": kernel}
 
 
-def config5_data(torch, device, row_scale: float, seed: int = 5):
+def config5_work(row_scale: float, seed: int = 5) -> list[float]:
+    """Component-visibility evaluations of each facet of the draw at row_scale
+    (the facet sharding's cost)."""
+    from obit_b200 import uvdata as U
+
+    return [float(max(1, int(round(nr * row_scale))) * nc * nif * nch)
+            for nr, nc, nif, nch in U.config5_facets(seed=seed)]
+
+
+def config5_data(torch, device, row_scale: float, seed: int = 5, subset=None):
     """The 96-facet uneven workload (seeded draw: components log-uniform in
     [500, 60000], rows log-uniform in [1e5, 1e7] scaled by row_scale, 1-8 IFs x
     32-512 channels, 2 polarizations), point components within 0.5 deg of each
-    facet centre; records built on the device.  Returns (facets, tensors,
-    full-draw evals)."""
+    facet centre; records built on the device.  subset: the facet indices to
+    build (a rank's share; every facet is drawn the same either way).  Returns
+    (facets, tensors, full-draw evals)."""
     from obit_b200 import uvdata as U
     from obit_b200.batch import Facet
     from obit_b200.skymodel import SkyModelParams
@@ -402,9 +416,13 @@ def config5_data(torch, device, row_scale: float, seed: int = 5):
     freq = 1.4e9
     track = U.make_uvw(pos, 2000, 45.0, 4.0, 34.0, freq).astype(np.float32)  # (2000 * 2016, 3)
     facets, keep = [], []
+    want = set(range(len(draw))) if subset is None else set(subset)
     for k, (nr, nc, nif, nch) in enumerate(draw):
         rows = max(1, int(round(nr * row_scale)))
         r0 = int(rng.integers(0, len(track) - rows + 1)) if rows < len(track) else 0
+        if k not in want:
+            rng.uniform(-1.0, 1.0, 2)  # the facet centre's draw, as when it is built
+            continue
         uvw = track[r0:r0 + rows]
         if len(uvw) < rows:
             uvw = np.resize(track, (rows, 3))
@@ -448,15 +466,15 @@ def _timed_on(torch, stream, fn, steps, warmup, after=None):
 
 
 def config5_measure(torch, device, row_scale, steps, warmup, autotune=True, tile=None,
-                    compare=True, sampler=None):
-    """The 96-facet batch: one graph launch of the persistent batched kernel per
-    step (autotuned tile unless `tile` fixes it), and, with `compare`, one launch
-    per facet of the recurrence and of the FP64-phase plain kernel.  Returns a
-    dict of the measurements."""
+                    compare=True, sampler=None, subset=None):
+    """The 96-facet batch (or a rank's `subset` of it): one graph launch of the
+    persistent batched kernel per step (autotuned tile unless `tile` fixes it),
+    and, with `compare`, one launch per facet of the recurrence and of the
+    FP64-phase plain kernel.  Returns a dict of the measurements."""
     from obit_b200 import _lib
     from obit_b200.batch import DFTBatch
 
-    facets, keep, full_evals = config5_data(torch, device, row_scale)
+    facets, keep, full_evals = config5_data(torch, device, row_scale, subset=subset)
     batch = DFTBatch(facets)
     try:
         info0 = batch.info()
@@ -494,23 +512,88 @@ def config5_measure(torch, device, row_scale, steps, warmup, autotune=True, tile
         torch.cuda.empty_cache()
 
 
+def config5_e2e(torch, device, row_scale, steps, warmup, staging_bytes, tile=None, subset=None):
+    """The batch over HOST records through obit_dft_batch_run_host: every
+    facet's records copied once into pinned host memory, then per step one
+    graph launch that streams them through a device staging area (H2D, batch
+    kernels, D2H) and a synchronize; wall clock per step."""
+    from obit_b200.batch import DFTBatch
+
+    facets, keep, _ = config5_data(torch, device, row_scale, subset=subset)
+    hosts = [keep[2 * i].cpu().pin_memory() for i in range(len(facets))]
+    batch = DFTBatch(facets)
+    try:
+        if tile:
+            batch.set_tile(*tile)
+        stream = torch.cuda.Stream(device=device)
+        ptrs = [h.data_ptr() for h in hosts]
+        for _ in range(warmup):
+            info = batch.run_host(ptrs, staging_bytes, stream.cuda_stream)
+        torch.cuda.synchronize()
+        batch.check()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            info = batch.run_host(ptrs, staging_bytes, stream.cuda_stream)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        batch.check()
+        return {"evals": batch.info()["evals"], "seconds": dt, "waves": info["waves"],
+                "h2d_bytes": info["h2d_bytes"], "rows": sum(f.nvis for f in facets)}
+    finally:
+        batch.close()
+        del keep, hosts
+        torch.cuda.empty_cache()
+
+
 def run_config5(args):
     """One step = one pass of the DFT subtract over all 96 facets: one graph
     launch of the persistent batched kernel (autotuned tile), against one
-    launch per facet of the recurrence and of the FP64-phase plain kernel."""
+    launch per facet of the recurrence and of the FP64-phase plain kernel.
+    Under torchrun every rank takes whole facets (largest first onto the least
+    loaded rank, no data-path collective); the time is the max over ranks."""
     import torch
+    import torch.distributed as dist
 
-    torch.cuda.set_device(0)
-    device = torch.device("cuda", 0)
+    from obit_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    subset = shard.facet_assignment(config5_work(args.row_scale), world)[rank] if world > 1 else None
     fixed = any((args.K, args.ct, args.Bt, args.threads))
-    sampler = ClockSampler(0)
+    tile = (args.K, args.ct, args.Bt, args.threads) if fixed else None
+    sampler = ClockSampler(local)
     m = config5_measure(torch, device, args.row_scale, args.steps, args.warmup,
-                        autotune=not args.no_autotune,
-                        tile=(args.K, args.ct, args.Bt, args.threads) if fixed else None,
-                        compare=not args.no_compare, sampler=sampler)
+                        autotune=not args.no_autotune, tile=tile,
+                        compare=not args.no_compare and world == 1, sampler=sampler, subset=subset)
     info, evals = m["info"], m["evals"]
     t_ms, per = m["t_ms"], m["per_ms"]
+    if world > 1:
+        t_ms = shard.max_over_ranks(t_ms, device)
+        evals = int(sum(config5_work(args.row_scale)))  # every rank's facets
     value = evals * args.steps / (t_ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        # the tuned tile of this rank's batch, on a smaller row sample held in host memory
+        t = tile or ((m["tuned"]["K"], m["tuned"]["ct"], m["tuned"]["Bt"], m["tuned"]["threads"])
+                     if m["tuned"] else None)
+        ee = config5_e2e(torch, device, args.e2e_row_scale, args.steps, 1, args.staging_gb * (1 << 30),
+                         tile=t, subset=subset)
+        sec = shard.max_over_ranks(ee["seconds"], device) if world > 1 else ee["seconds"]
+        tot = int(sum(config5_work(args.e2e_row_scale))) if world > 1 else ee["evals"]
+        e2e = {"value": tot * args.steps / sec / 1e9, "unit": "Gevals/s",
+               "h2d_bytes_per_step": ee["h2d_bytes"], "d2h_bytes_per_step": ee["h2d_bytes"],
+               "timing": "wall clock around obit_dft_batch_run_host + synchronize (graph: waves of "
+                         "H2D -> persistent batch kernels -> D2H), max over ranks",
+               "workload": f"rows x {args.e2e_row_scale} of the draw in pinned host memory, "
+                           f"{ee['waves']} waves through {args.staging_gb} GiB of device staging",
+               "evals_per_step": tot}
     comp = {k: m[k] for k in ("per_facet_recur_gevals_s", "per_facet_plain_gevals_s",
                               "batch_vs_per_facet_plain", "batch_vs_per_facet_recur") if k in m}
     peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
@@ -540,11 +623,17 @@ def run_config5(args):
                      "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)"},
         "comparators": comp,
         "host": host_info(),
-        "cpu_baseline": None, "e2e": None,
+        "cpu_baseline": None, "e2e": e2e,
         "gpu_launches": info["launches"] * args.steps,
         "clocks": sampler.summary(),
     }
-    print(json.dumps(line), flush=True)
+    if world > 1:
+        line["n_gpus"] = world
+        line["config"]["sharding"] = "whole facets per rank (largest first onto the least loaded rank)"
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def run_beam(args):

@@ -381,6 +381,20 @@ int obit_dft_batch_set_tile(ObitDFTBatch *batch, int chanPerThread, int compsPer
  * Asynchronous; obit_dft_batch_check reads the kernels' error flag. */
 int obit_dft_batch_run(ObitDFTBatch *batch, void *stream);
 
+/* Streamed form of obit_dft_batch_run for records in host memory: facet i's
+ * nvis records (the count given at creation) are read from and written back to
+ * h_vis[i] (pinned memory, for the copies to overlap the kernels).  The rows
+ * pass through a device staging area of stagingBytes, in waves that fill one
+ * half of it each: one graph launch on `stream` copies wave w in, applies the
+ * batch kernels to it and copies it out, wave w + 1's upload overlapping wave
+ * w's kernels on a second stream.  The graph is captured at the first call and
+ * again when h_vis, stagingBytes or the tile shape change.  info (may be NULL)
+ * receives {waves, bytes uploaded per run}.  Asynchronous: the host records
+ * are complete once `stream` is; obit_dft_batch_check reads the kernels'
+ * error flag.  The staging area must hold two records of the widest facet. */
+int obit_dft_batch_run_host(ObitDFTBatch *batch, float *const *h_vis, long long stagingBytes, void *stream,
+                            long long *info);
+
 /* Comparator: the same work as one kernel launch per facet on `stream`, with
  * each facet's own planner-default plan of kernel `flavor`
  * (OBIT_DFT_RECUR or OBIT_DFT_PLAIN). */

@@ -158,6 +158,8 @@ SIGNATURES = {
     "obit_dft_batch_set_tile": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "obit_dft_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
     "obit_dft_batch_run_per_facet": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "obit_dft_batch_run_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_longlong, C.c_void_p,
+                                          C.POINTER(C.c_longlong)]),
     "obit_dft_batch_check": (C.c_int, [C.c_void_p]),
     "obit_dft_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
     "obit_dft_batch_destroy": (C.c_int, [C.c_void_p]),

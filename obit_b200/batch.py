@@ -107,6 +107,15 @@ class DFTBatch:
     def run(self, stream: int = 0) -> None:
         _lib.check(self._lib.obit_dft_batch_run(self._h, C.c_void_p(stream)))
 
+    def run_host(self, h_ptrs: list[int], staging_bytes: int, stream: int = 0) -> dict:
+        """Streamed run over host records: h_ptrs[i] is facet i's host buffer
+        (pinned, nvis x lrec floats); staging_bytes of device staging.  Returns
+        {waves, h2d_bytes} of the captured graph."""
+        arr = (C.c_void_p * max(1, len(h_ptrs)))(*h_ptrs)
+        info = (C.c_longlong * 2)()
+        _lib.check(self._lib.obit_dft_batch_run_host(self._h, arr, int(staging_bytes), C.c_void_p(stream), info))
+        return {"waves": int(info[0]), "h2d_bytes": int(info[1])}
+
     def run_per_facet(self, flavor: int = _lib.OBIT_DFT_RECUR, stream: int = 0) -> None:
         _lib.check(self._lib.obit_dft_batch_run_per_facet(self._h, flavor, C.c_void_p(stream)))
 

@@ -60,7 +60,9 @@ struct Group {
   // resolved
   int K = 0, ct = 0, Bt = 0, R = 0, threads = 0, grid = 0;
   size_t smemBytes = 0;
+  int cap = 0;                // CTAs resident across the device
   long long items = 0, evals = 0;
+  std::vector<KParams> hkps;  // host copies of the facets' parameter blocks (group order)
   KParams* d_params = nullptr;
   int* d_itemStart = nullptr;
   int* d_counter = nullptr;
@@ -79,6 +81,33 @@ void free_group(Group& g) {
   g.built = false;
 }
 
+// The streamed form (obit_dft_batch_run_host): waves of rows through a
+// two-half device staging area, captured once as H2D -> batch kernels -> D2H.
+struct HostRun {
+  std::vector<float*> h;       // the facets' host records the graph reads and writes
+  long long stagingBytes = 0;
+  float* d_stage = nullptr;
+  KParams* d_params = nullptr; // per (wave, group): the pieces' parameter blocks
+  int* d_starts = nullptr;
+  int* d_counters = nullptr;
+  cudaStream_t copyStream = nullptr;
+  std::vector<cudaEvent_t> events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int waves = 0;
+  long long h2dBytes = 0;
+};
+
+void free_host_run(HostRun& r) {
+  if (r.exec) cudaGraphExecDestroy(r.exec);
+  if (r.graph) cudaGraphDestroy(r.graph);
+  for (cudaEvent_t e : r.events) cudaEventDestroy(e);
+  for (void* q : {(void*)r.d_stage, (void*)r.d_params, (void*)r.d_starts, (void*)r.d_counters})
+    if (q) cudaFree(q);
+  if (r.copyStream) cudaStreamDestroy(r.copyStream);
+  r = HostRun();
+}
+
 }  // namespace
 
 struct ObitDFTBatch {
@@ -90,6 +119,7 @@ struct ObitDFTBatch {
   cudaStream_t capStream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  HostRun host;
 };
 
 namespace {
@@ -99,6 +129,7 @@ void drop_graph(ObitDFTBatch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->exec = nullptr;
   b->graph = nullptr;
+  free_host_run(b->host);  // its graph holds the groups' parameter blocks too
 }
 
 // Plan every facet of group g with one tile shape and upload its work list.
@@ -192,6 +223,7 @@ int build_group(Group& g, std::vector<Facet>& fs, const float* d_comps, int* d_e
     kps.push_back(kp);
   }
   CUDA_TRY(cudaMemcpy(g.d_params, kps.data(), sizeof(KParams) * kps.size(), cudaMemcpyHostToDevice));
+  g.hkps = kps;
   CUDA_TRY(cudaMemcpy(g.d_itemStart, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemset(g.d_counter, 0, sizeof(int)));
   int cap = 0;
@@ -203,6 +235,7 @@ int build_group(Group& g, std::vector<Facet>& fs, const float* d_comps, int* d_e
   g.threads = T.threads;
   g.R = T.threads / T.Bt;
   g.smemBytes = smem;
+  g.cap = cap;
   g.items = items;
   g.evals = evals;
   g.grid = (int)std::min<long long>(items, cap);
@@ -240,6 +273,171 @@ const Group* main_group(const ObitDFTBatch* b) {
   for (const Group& g : b->groups)
     if (!m || g.evals > m->evals) m = &g;
   return m;
+}
+
+// Streamed run: build the waves, their parameter blocks and the captured graph
+// for host records h (one pointer per facet) and a staging area of
+// stagingBytes, unless the current graph was built for the same.
+int build_host_run(ObitDFTBatch* b, float* const* h, long long stagingBytes) {
+  HostRun& r = b->host;
+  const size_t nf = b->facets.size();
+  if (r.exec && r.stagingBytes == stagingBytes && r.h.size() == nf && std::equal(r.h.begin(), r.h.end(), h))
+    return OBIT_DFT_OK;
+  free_host_run(r);
+  // two halves, each a multiple of 64 floats
+  const size_t half = (size_t)(stagingBytes / (long long)sizeof(float) / 2) / 64 * 64;
+  // facet -> (group, position in the group's work order)
+  std::vector<int> grp(nf, -1), pos(nf, -1);
+  for (size_t gi = 0; gi < b->groups.size(); gi++)
+    for (size_t k = 0; k < b->groups[gi].order.size(); k++) {
+      grp[b->groups[gi].order[k]] = (int)gi;
+      pos[b->groups[gi].order[k]] = (int)k;
+    }
+  // waves: consecutive pieces of rows, facet after facet, each wave within half
+  struct Piece {
+    int f, r0, n;
+    size_t off;  // floats into the wave's half
+  };
+  std::vector<std::vector<Piece>> waves(1);
+  size_t used = 0;
+  for (size_t f = 0; f < nf; f++) {
+    const Facet& fc = b->facets[f];
+    const size_t lrec = (size_t)fc.L.lrec;
+    if (fc.nvis > 0 && lrec > half)
+      return fail(OBIT_DFT_EBADARG, "staging area smaller than two records of facet " + std::to_string(f));
+    int r0 = 0;
+    while (r0 < fc.nvis) {
+      size_t fit = (half - used) / lrec;
+      if (fit == 0) {
+        waves.emplace_back();
+        used = 0;
+        continue;
+      }
+      const int n = (int)std::min<size_t>(fit, (size_t)(fc.nvis - r0));
+      waves.back().push_back({(int)f, r0, n, used});
+      used += (size_t)n * lrec;
+      r0 += n;
+    }
+  }
+  if (waves.back().empty()) waves.pop_back();
+  // per (wave, group): parameter blocks of the pieces in the group's work order
+  const size_t ng = b->groups.size();
+  std::vector<KParams> kps;
+  std::vector<int> starts;
+  struct Launch {
+    size_t wave, group, params, start, pieces;
+    long long items;
+  };
+  std::vector<Launch> launches;
+  CUDA_TRY(cudaMalloc(&r.d_stage, sizeof(float) * std::max<size_t>(64, 2 * half)));
+  for (size_t w = 0; w < waves.size(); w++) {
+    for (size_t gi = 0; gi < ng; gi++) {
+      const Group& g = b->groups[gi];
+      std::vector<Piece> ps;
+      for (const Piece& pc : waves[w])
+        if (grp[pc.f] == (int)gi) ps.push_back(pc);
+      std::stable_sort(ps.begin(), ps.end(), [&](const Piece& a, const Piece& c) { return pos[a.f] < pos[c.f]; });
+      if (ps.empty() || !g.built) continue;
+      Launch L{w, gi, kps.size(), starts.size(), ps.size(), 0};
+      starts.push_back(0);
+      for (const Piece& pc : ps) {
+        KParams kp = g.hkps[pos[pc.f]];
+        kp.vis = r.d_stage + (w % 2) * half + pc.off;
+        kp.nvis = pc.n;
+        kp.rowBase = 0;
+        if (kp.ncomp > 0 && kp.nblocks > 0) L.items += (long long)((pc.n + kp.R - 1) / kp.R) * kp.nBlockTiles;
+        kps.push_back(kp);
+        starts.push_back((int)L.items);
+      }
+      if (L.items > (long long)INT32_MAX - 1) return fail(OBIT_DFT_EUNSUPPORTED, "wave has more than 2^31 work items");
+      launches.push_back(L);
+    }
+  }
+  CUDA_TRY(cudaMalloc(&r.d_params, sizeof(KParams) * std::max<size_t>(1, kps.size())));
+  CUDA_TRY(cudaMalloc(&r.d_starts, sizeof(int) * std::max<size_t>(1, starts.size())));
+  CUDA_TRY(cudaMalloc(&r.d_counters, sizeof(int) * std::max<size_t>(1, launches.size())));
+  if (!kps.empty())
+    CUDA_TRY(cudaMemcpy(r.d_params, kps.data(), sizeof(KParams) * kps.size(), cudaMemcpyHostToDevice));
+  if (!starts.empty())
+    CUDA_TRY(cudaMemcpy(r.d_starts, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaStreamCreateWithFlags(&r.copyStream, cudaStreamNonBlocking));
+  // events: fork, per wave "uploaded" and "applied", join
+  const size_t nw = waves.size();
+  r.events.resize(2 * nw + 2);
+  for (cudaEvent_t& e : r.events) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t fork = r.events[0], join = r.events[1];
+  auto up = [&](size_t w) { return r.events[2 + 2 * w]; };
+  auto done = [&](size_t w) { return r.events[3 + 2 * w]; };
+  // capture: copies in order on the copy stream (H2D of wave w after the D2H
+  // of wave w - 2, which used the same half), kernels on the capture stream
+  std::string err;
+  int rc = 0;
+  CUDA_TRY(cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal));
+  cudaStream_t cs = b->capStream, cp = r.copyStream;
+  auto copy_wave = [&](size_t w, bool toDevice) -> cudaError_t {
+    for (const Piece& pc : waves[w]) {
+      const Facet& fc = b->facets[pc.f];
+      float* dev = r.d_stage + (w % 2) * half + pc.off;
+      float* host = h[pc.f] + (size_t)pc.r0 * fc.L.lrec;
+      const size_t bytes = sizeof(float) * (size_t)pc.n * fc.L.lrec;
+      cudaError_t ce = toDevice ? cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, cp)
+                                : cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, cp);
+      if (ce != cudaSuccess) return ce;
+      if (toDevice) r.h2dBytes += (long long)bytes;
+    }
+    return cudaSuccess;
+  };
+  cudaError_t ce = cudaEventRecord(fork, cs);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cp, fork, 0);
+  size_t li = 0;
+  for (size_t w = 0; w < nw && ce == cudaSuccess && !rc; w++) {
+    if (w >= 2) {  // the half of wave w is free once wave w - 2 is back on the host
+      ce = cudaStreamWaitEvent(cp, done(w - 2), 0);
+      if (ce == cudaSuccess) ce = copy_wave(w - 2, false);
+    }
+    if (ce == cudaSuccess) ce = copy_wave(w, true);
+    if (ce == cudaSuccess) ce = cudaEventRecord(up(w), cp);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs, up(w), 0);
+    for (; li < launches.size() && launches[li].wave == w && ce == cudaSuccess && !rc; li++) {
+      const Launch& L = launches[li];
+      const Group& g = b->groups[L.group];
+      if (L.items <= 0) continue;
+      ce = cudaMemsetAsync(r.d_counters + li, 0, sizeof(int), cs);
+      if (ce != cudaSuccess) break;
+      BatchParams bp{};
+      bp.facets = r.d_params + L.params;
+      bp.itemStart = r.d_starts + L.start;
+      bp.nfacet = (int)L.pieces;
+      bp.counter = r.d_counters + li;
+      rc = launch_batch(g.K, g.kind, bp, (int)std::min<long long>(L.items, g.cap), g.threads, g.smemBytes, cs, &err);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(done(w), cs);
+  }
+  for (size_t w = (nw >= 2 ? nw - 2 : 0); w < nw && ce == cudaSuccess; w++) {
+    ce = cudaStreamWaitEvent(cp, done(w), 0);
+    if (ce == cudaSuccess) ce = copy_wave(w, false);
+  }
+  if (ce == cudaSuccess) ce = cudaEventRecord(join, cp);
+  if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs, join, 0);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce2 = cudaStreamEndCapture(cs, &graph);
+  if (rc || ce != cudaSuccess || ce2 != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    free_host_run(r);
+    if (rc) return fail(rc, err);
+    return fail(OBIT_DFT_ECUDA, std::string("streamed batch capture: ") +
+                                    cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
+  }
+  r.graph = graph;
+  ce = cudaGraphInstantiate(&r.exec, r.graph, 0);
+  if (ce != cudaSuccess) {
+    free_host_run(r);
+    return fail(OBIT_DFT_ECUDA, std::string("streamed batch instantiate: ") + cudaGetErrorString(ce));
+  }
+  r.h.assign(h, h + nf);
+  r.stagingBytes = stagingBytes;
+  r.waves = (int)nw;
+  return OBIT_DFT_OK;
 }
 
 }  // namespace
@@ -361,6 +559,28 @@ extern "C" int obit_dft_batch_run(ObitDFTBatch* b, void* stream) {
     }
   }
   CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_batch_run_host(ObitDFTBatch* b, float* const* h_vis, long long stagingBytes,
+                                       void* stream, long long* info) {
+  set_last_error("");
+  if (!b) return fail(OBIT_DFT_EBADARG, "NULL batch");
+  if (!h_vis && !b->facets.empty()) return fail(OBIT_DFT_EBADARG, "NULL host record pointers");
+  for (size_t f = 0; f < b->facets.size(); f++)
+    if (b->facets[f].nvis > 0 && !h_vis[f])
+      return fail(OBIT_DFT_EBADARG, "facet " + std::to_string(f) + ": NULL host records");
+  if (stagingBytes < 2 * 64 * (long long)sizeof(float)) return fail(OBIT_DFT_EBADARG, "staging area too small");
+  CUDA_TRY(cudaSetDevice(b->device));
+  int rc = ensure_built(b);
+  if (rc) return rc;
+  rc = build_host_run(b, h_vis, stagingBytes);
+  if (rc) return rc;
+  if (info) {
+    info[0] = b->host.waves;
+    info[1] = b->host.h2dBytes;
+  }
+  CUDA_TRY(cudaGraphLaunch(b->host.exec, (cudaStream_t)stream));
   return OBIT_DFT_OK;
 }
 

@@ -86,3 +86,55 @@ def _worker(rank, world, port):
 def test_sharded_subtract_equals_single_process(world):
     mp = pytest.importorskip("torch.multiprocessing")
     mp.spawn(_worker, args=(world, _free_port()), nprocs=world, join=True)
+
+
+def _facet_worker(rank, world, port):
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    for p in (root, root / "oracle", root / "tests"):
+        sys.path.insert(0, str(p))
+    import datetime
+
+    import torch.distributed as dist
+
+    import oracle
+    from helpers import small
+    from obit_b200 import shard as S
+    from obit_b200 import uvdata as U
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        # uneven facets: different rows, channels, IFs and components
+        specs = [(U.MOD_POINT_SPEC, 30 + 17 * i, 8 + 4 * (i % 3), 1 + i % 2, 20 + 13 * i, 70 + i)
+                 for i in range(7)]
+        facets = [small(mt, nrow=nr, nchan=nc, nif=ni, nstok=2, ncomp=ncp, seed=sd)
+                  for mt, nr, nc, ni, ncp, sd in specs]
+        work = [uv.nvis * uv.nchan * uv.nif * sky.ncomp for uv, sky in facets]
+        mine = S.facet_assignment(work, world)[rank]  # no communication
+        done = {i: oracle.apply_fp64(facets[i][0], facets[i][1], nthreads=1) for i in mine}
+        parts = [None] * world
+        dist.all_gather_object(parts, done)
+        got = {}
+        for d in parts:
+            assert not set(d) & set(got)  # each facet on exactly one rank
+            got.update(d)
+        assert sorted(got) == list(range(len(facets)))
+        for i, (uv, sky) in enumerate(facets):
+            assert np.array_equal(got[i], oracle.apply_fp64(uv, sky, nthreads=1))
+        loads = [sum(work[i] for i in S.facet_assignment(work, world)[r]) for r in range(world)]
+        assert max(loads) - min(loads) <= max(work)  # greedy LPT balance
+        assert S.max_over_ranks(float(len(mine))) == max(len(a) for a in S.facet_assignment(work, world))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_facet_sharded_subtract_equals_single_process(world):
+    """Whole facets per rank (bench.py --workload config5 under torchrun): the
+    union of the ranks' facets is every facet once, each applied as a single
+    process applies it."""
+    mp = pytest.importorskip("torch.multiprocessing")
+    mp.spawn(_facet_worker, args=(world, _free_port()), nprocs=world, join=True)
