@@ -21,9 +21,9 @@
  * fields; point fields in a Gaussian model carry zero Gaussian terms.
  * Supported: point, Gaussian, point / Gaussian with polynomial spectrum,
  * -SIN projection, 3-D images, and 2-D images whose centre is the uv phase
- * centre with no rotation or pixel offset.  Tabulated spectra, uniform
- * spheres, exponential disks, -NCP and shifted 2-D images are rejected with
- * OBIT_DFT_EUNSUPPORTED.
+ * centre with no rotation or pixel offset; tabulated spectra through
+ * obit_dft_load_comps_mf below.  Uniform spheres, exponential disks, -NCP
+ * and shifted 2-D images are rejected with OBIT_DFT_EUNSUPPORTED.
  */
 #ifndef OBIT_DFT_COMPS_H
 #define OBIT_DFT_COMPS_H
@@ -85,6 +85,35 @@ int obit_dft_load_comps(const ObitDFTCCField *fields, int nfield, const ObitDFTC
 int obit_dft_load_comps_d(const ObitDFTCCField *fields, int nfield, const ObitDFTCCModel *model,
                           float *table, long long capacity, int *nrowOut, int *ncomp, int *lcomp,
                           int *modType, int *nterm, double *xyz);
+
+/* Settings of a multi-frequency sky model (ObitSkyModelMF members) whose
+ * components carry tabulated spectra: one flux per coarse frequency plane. */
+typedef struct {
+  int nSpec;                /* coarse planes (the model image's NSPEC) */
+  const double *specFreq;   /* [nSpec] plane frequencies, Hz; the fit's reference is specFreq[0] */
+  int noSIfit;              /* 1: no spectral-index fit (polarized data, ObitSkyModelMF.c:1164-1168) */
+  int doAlphaCorr;          /* 1: plane fluxes times (nu / priorAlphaRefF)^priorAlpha */
+  float priorAlpha;
+  double priorAlphaRefF;    /* Hz */
+} ObitDFTCCModelMF;
+
+/* ObitSkyModelMFLoadComps (ObitSkyModelMF.c:1130-1635): the component table
+ * of point or Gaussian components with tabulated spectra (types 20 and 21,
+ * PARMS[4 .. 4 + nSpec - 1] the per-plane fluxes).  Rows at the same position
+ * merge with each plane's flux summed (CCMergeSpec); each output row is
+ * [flux x factor, X, Y, Z, (g1, g2, g3,) alpha, S_0 .. S_nSpec-1] with S_k the
+ * plane flux times factor (and the prior-alpha correction) and alpha the
+ * spectral index fitted to the planes as ObitSpectrumFitSingleArg does for
+ * two terms (weighted least squares of S_0 (nu / nu_0)^alpha, nu_0 =
+ * specFreq[0], every plane's sigma 1e-4 Jy, exactly-zero planes left out;
+ * the fit is kept only if its reduced chi^2 is below 1.5 times the constant
+ * model's, and alpha outside [-2, 2] becomes 0).  Positions and selection as
+ * obit_dft_load_comps.  *modType is 20 or 21; *lcomp = 5 (8 for Gaussians) +
+ * nSpec.  Fields of other types, or of both TSpec types, are rejected with
+ * OBIT_DFT_EUNSUPPORTED. */
+int obit_dft_load_comps_mf(const ObitDFTCCField *fields, int nfield, const ObitDFTCCModel *model,
+                           const ObitDFTCCModelMF *mf, float *table, long long capacity, int *nrowOut,
+                           int *ncomp, int *lcomp, int *modType);
 
 #ifdef __cplusplus
 }

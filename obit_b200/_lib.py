@@ -95,6 +95,13 @@ class ObitDFTCCModel(C.Structure):
     ]
 
 
+class ObitDFTCCModelMF(C.Structure):
+    _fields_ = [
+        ("nSpec", C.c_int), ("specFreq", C.POINTER(C.c_double)), ("noSIfit", C.c_int),
+        ("doAlphaCorr", C.c_int), ("priorAlpha", C.c_float), ("priorAlphaRefF", C.c_double),
+    ]
+
+
 class ObitDFTFacet(C.Structure):
     _fields_ = [
         ("visInfo", C.POINTER(GPUVisInfo)), ("modelInfo", C.POINTER(GPUModelInfo)),
@@ -171,6 +178,10 @@ SIGNATURES = {
                                         C.POINTER(C.c_float), C.c_longlong, C.POINTER(C.c_int),
                                         C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "obit_dft_load_comps_mf": (C.c_int, [C.POINTER(ObitDFTCCField), C.c_int, C.POINTER(ObitDFTCCModel),
+                                         C.POINTER(ObitDFTCCModelMF), C.POINTER(C.c_float), C.c_longlong,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),

@@ -55,10 +55,8 @@ def _f32(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
 
 
-def load_comps(fields: list[CCField], model: CCModel, ref_freq: float = 0.0):
-    """Returns (SkyComps of the components, rows allocated incl. zero rows)."""
-    lib = _lib.load()
-    keep, arr = [], (ObitDFTCCField * max(1, len(fields)))()
+def _field_array(fields: list[CCField], keep: list):
+    arr = (ObitDFTCCField * max(1, len(fields)))()
     for i, f in enumerate(fields):
         cols = [_f32(f.flux), _f32(f.deltaX), _f32(f.deltaY), _f32(f.deltaZ), _f32(f.parms)]
         st = None if f.status is None else np.ascontiguousarray(f.status, dtype=np.int32)
@@ -77,8 +75,20 @@ def load_comps(fields: list[CCField], model: CCModel, ref_freq: float = 0.0):
         d.crvalRA, d.crvalDec, d.rotation, d.do3D = f.crvalRA, f.crvalDec, f.rotation, int(f.do3D)
         d.xPxOff, d.yPxOff, d.cdeltX, d.cdeltY = f.xPxOff, f.yPxOff, f.cdeltX, f.cdeltY
         d.xShift, d.yShift, d.ncpProjection = f.xShift, f.yShift, int(f.ncp)
-    m = ObitDFTCCModel(model.uvRA, model.uvDec, model.uvRotation, model.factor, model.minFlux,
-                       model.minDFT, int(model.noNeg), int(model.do3D))
+    return arr
+
+
+def _model(model: CCModel) -> ObitDFTCCModel:
+    return ObitDFTCCModel(model.uvRA, model.uvDec, model.uvRotation, model.factor, model.minFlux,
+                          model.minDFT, int(model.noNeg), int(model.do3D))
+
+
+def load_comps(fields: list[CCField], model: CCModel, ref_freq: float = 0.0):
+    """Returns (SkyComps of the components, rows allocated incl. zero rows)."""
+    lib = _lib.load()
+    keep: list = []
+    arr = _field_array(fields, keep)
+    m = _model(model)
     nrow, ncomp, lcomp, mtype, nterm = (C.c_int() for _ in range(5))
     _lib.check(lib.obit_dft_load_comps(arr, len(fields), C.byref(m), None, 0, C.byref(nrow),
                                        C.byref(ncomp), C.byref(lcomp), C.byref(mtype), C.byref(nterm)))
@@ -92,3 +102,40 @@ def load_comps(fields: list[CCField], model: CCModel, ref_freq: float = 0.0):
     sky = SkyComps(mtype.value, comps, nterm=nterm.value, refFreq=ref_freq,
                    xyz=np.ascontiguousarray(xyz[:ncomp.value]))
     return sky, nrow.value
+
+
+@dataclass
+class MFModel:
+    """Tabulated-spectrum settings of an MF sky model (ObitSkyModelMF)."""
+
+    specFreq: np.ndarray          # Hz per coarse plane
+    noSIfit: bool = False
+    doAlphaCorr: bool = False
+    priorAlpha: float = 0.0
+    priorAlphaRefF: float = 1.0e9
+
+
+def load_comps_mf(fields: list[CCField], model: CCModel, mf: MFModel, spec_index=None):
+    """obit_dft_load_comps_mf: components with tabulated spectra (CC types 20,
+    21; PARMS[4..] per-plane fluxes) and fitted spectral indices.  Returns
+    (SkyComps of type 20 or 21, rows allocated).  spec_index: the plane of each
+    (channel, IF), kept on the result for the DFT."""
+    from .uvdata import MOD_GAUSS_TSPEC, MOD_POINT_TSPEC
+
+    lib = _lib.load()
+    keep: list = []
+    arr = _field_array(fields, keep)
+    m = _model(model)
+    sf = np.ascontiguousarray(mf.specFreq, dtype=np.float64)
+    mm = _lib.ObitDFTCCModelMF(len(sf), sf.ctypes.data_as(C.POINTER(C.c_double)), int(mf.noSIfit),
+                               int(mf.doAlphaCorr), float(mf.priorAlpha), float(mf.priorAlphaRefF))
+    nrow, ncomp, lcomp, mtype = (C.c_int() for _ in range(4))
+    _lib.check(lib.obit_dft_load_comps_mf(arr, len(fields), C.byref(m), C.byref(mm), None, 0, C.byref(nrow),
+                                          C.byref(ncomp), C.byref(lcomp), C.byref(mtype)))
+    table = np.zeros((max(1, nrow.value), lcomp.value), np.float32)
+    _lib.check(lib.obit_dft_load_comps_mf(arr, len(fields), C.byref(m), C.byref(mm),
+                                          table.ctypes.data_as(C.POINTER(C.c_float)), table.size,
+                                          C.byref(nrow), C.byref(ncomp), C.byref(lcomp), C.byref(mtype)))
+    kind = MOD_POINT_TSPEC if mtype.value == 20 else MOD_GAUSS_TSPEC
+    comps = np.ascontiguousarray(table[:ncomp.value])
+    return SkyComps(kind, comps, specFreq=sf, specIndex=spec_index), nrow.value
