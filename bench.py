@@ -83,10 +83,12 @@ def parse():
     ap.add_argument("--cpu-step-seconds", type=float, default=2.0,
                     help="reference arm: CPU work per step (the row sample is sized to it)")
     ap.add_argument("--workload", default="config2",
-                    choices=["config1", "config2", "config3", "config4", "config5", "beam"],
+                    choices=["config1", "config2", "config3", "config4", "config5", "beam", "grid"],
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
                          "96-facet uneven batch; beam: the beam-corrected DFT on the config-2 "
-                         "layout")
+                         "layout; grid: the gridded model FT on the config-2 layout")
+    ap.add_argument("--grid-kernel", default="reference", choices=["reference", "exact"],
+                    help="grid: interpolation weights (the reference's table or exact Lagrange)")
     ap.add_argument("--e2e-row-scale", type=float, default=0.002,
                     help="config5: row scale of the host-memory (streamed) end-to-end pass")
     ap.add_argument("--staging-gb", type=float, default=1.0,
@@ -731,6 +733,169 @@ def run_beam(args):
     gm.close()
 
 
+def grid_field(N: int, ncomp: int, cell_asec: float, seed: int = 8):
+    """A CLEAN model of `ncomp` components on the cells of the central half of
+    an N x N image of cell_asec pixels (2-D field at the phase centre), fluxes
+    log-uniform over [1 mJy, 1 Jy]."""
+    from obit_b200.comps import CCField, CCModel
+    from obit_b200.grid import GridImage
+
+    r = np.random.default_rng(seed)
+    cell = cell_asec / 3600.0
+    ix = r.integers(-N // 4, N // 4, ncomp)
+    iy = r.integers(-N // 4, N // 4, ncomp)
+    flux = np.exp(r.uniform(math.log(1e-3), 0.0, ncomp)).astype(np.float32)
+    f = CCField(flux=flux, deltaX=(ix * -cell).astype(np.float32), deltaY=(iy * cell).astype(np.float32),
+                crvalRA=0.0, crvalDec=34.0, do3D=False, cdeltX=-cell, cdeltY=cell)
+    return f, GridImage(N, N, N / 2 + 1, N / 2 + 1), CCModel(uvRA=0.0, uvDec=34.0)
+
+
+def run_grid(args):
+    """The gridded model FT (obit_dft_grid_*) on the config-2 layout: a chunk of
+    `--rows` records (default 20,160 = 10 integrations of 2016 baselines) x 4 IF
+    x 256 channels x 4 polarizations (the first two subtracted), against a
+    CLEAN model of `--ncomp` components (default 20,000) on the cells of a
+    4096 x 4096 image of 0.25 arcsec pixels (an 8192 x 8192 grid: the plane
+    reaches 1.8 x the longest baseline).  value: model visibilities (record x
+    channel x IF) per second of the apply kernel on device-resident records,
+    CUDA events; setup: the field's gridding, FFT and plane (wall clock of the
+    blocking create call); e2e: the host-records call (H2D, kernel, D2H per
+    step).  dft_equivalent: components x model visibilities per second, the
+    DFT's metric for the same model and records."""
+    import torch
+
+    from obit_b200 import grid as GR
+    from obit_b200.skymodel import OP_SUB, SkyModelParams
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    rows = args.rows or 20160
+    ncomp = args.ncomp or 20000
+    N = 4096
+    freq = 1.4e9
+    from obit_b200 import uvdata as U
+    fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
+    uvw = _track(64, 36e3, 2000, freq, 2, rows, 0)
+    f, img, m = grid_field(N, ncomp, 0.25)
+    kernel = GR.KERNEL_EXACT if args.grid_kernel == "exact" else GR.KERNEL_REFERENCE
+    d_vis = build_vis(torch, uvw, 4, 256, 4, device, seed=100)
+    lrec = d_vis.shape[1]
+    uvh = U.UVData(np.zeros((1, lrec), np.float32), 4, 256, 4, freq, fa)
+    p = SkyModelParams(op=OP_SUB)
+    d_fs = torch.from_numpy(np.ascontiguousarray(uvh.fscale)).to(device)
+    stream = torch.cuda.Stream(device=device)
+    sp = stream.cuda_stream
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gf = GR.GridField(f, img, m, kernel=kernel, stream=sp)
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    setups = []
+    for _ in range(3):  # repeat the set-up (plans and allocations included)
+        t0 = time.perf_counter()
+        GR.GridField(f, img, m, kernel=kernel, stream=sp).close()
+        setups.append((time.perf_counter() - t0) * 1e3)
+    info = gf.info()
+    nvisch = rows * 1024
+    run = lambda: gf.FTGrid_device(uvh, d_vis.data_ptr(), rows, p, d_fscale=d_fs.data_ptr(), stream=sp)  # noqa: E731
+    with torch.cuda.stream(stream):
+        sampler = ClockSampler(0)
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        with sampler:
+            t_ms, launch_ms = _timed_on(torch, stream, run, args.steps, 0)
+    value = nvisch * args.steps / (t_ms * 1e-3)
+    e2e = None
+    if not args.no_e2e:
+        h = torch.empty((rows, lrec), dtype=torch.float32, pin_memory=True)
+        h.copy_(d_vis.cpu())
+        uvp = U.UVData(h.numpy(), 4, 256, 4, freq, fa)
+        vi, _fs = GR.vis_info(uvp, p)
+        lib = gf._lib
+        call = lambda: lib.obit_dft_grid_apply_host(gf._h, C.byref(vi), p.op, 1.0, 0,  # noqa: E731
+                                                    C.c_void_p(h.data_ptr()), rows, C.c_void_p(sp))
+        call()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            assert call() == 0
+        te = (time.perf_counter() - t0) / args.steps
+        e2e = {"value": nvisch / te / 1e9, "unit": "G model visibilities/s",
+               "h2d_bytes_per_step": rows * lrec * 4, "d2h_bytes_per_step": rows * lrec * 4,
+               "what": "obit_dft_grid_apply_host on pinned host records: H2D, kernel, D2H, synchronized"}
+    # algorithmic DRAM bytes of a launch: the selected correlations of every record
+    # read and written (2 polarizations x 1024 channels x 12 bytes, twice) and u, v, w
+    algo = rows * (3 * 4 + 2 * 2 * 1024 * 12)
+    mean_launch = statistics.mean(launch_ms)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = algo / (mean_launch * 1e-3) / 1e9
+    gather = nvisch * 25 * 13 * 16 / (mean_launch * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu:
+        cpu = grid_cpu_baseline(f, img, m, uvw, fa, freq, args.cpu_seconds)
+    line = {
+        "metric": "model visibilities/s (gridded model FT subtract)", "value": value / 1e9,
+        "unit": "G model visibilities/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded uvw, noise visibilities, components on random cells)",
+        "accuracy": {"bound": "|V - V_oracle| / sum|flux| < 1e-5 (reference kernel, against the oracle's "
+                              "restatement); exact kernel against the DFT oracle < 1e-5",
+                     "checked_by": "tests/test_grid_gpu.py (-m gpu)"},
+        "config": {"workload": f"grid: {rows} records (64 antennas, 2016 baselines) x 4 IF x 256 ch x 4 pol "
+                               f"(2 subtracted), {info['ncomp']} components on the cells of a {N} x {N} "
+                               f"image (0.25 arcsec), {info['nx']} x {info['ny']} grid",
+                   "rows_per_step": rows, "components": info["ncomp"], "kernel": args.grid_kernel,
+                   "l2": "inputs larger than L2 (records); the plane (%.0f MB) is read through L2" %
+                         (info["ny"] * (info["nxp"] + 1) * 8 / 1e6),
+                   "timing": "CUDA events around all steps"},
+        "setup_ms": {"first": setup_ms, "repeat_median": statistics.median(setups),
+                     "what": "obit_dft_grid_create (host gridding, cuFFT plan and R2C, taper and conjugate "
+                             "columns), wall clock, blocking"},
+        "dft_equivalent": {"gevals_s": ncomp * value / 1e9,
+                           "gevals_s_with_setup": ncomp * nvisch * args.steps /
+                           ((t_ms + statistics.median(setups)) * 1e-3) / 1e9,
+                           "what": "components x model visibilities per second: the DFT metric for the same "
+                                   "model and records (one set-up per step counted in the second figure)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                     "note": "algorithmic bytes are the records' selected correlations read and written; the "
+                             "kernel's limit is its window gathers through L1/L2 (25 rows x 13 16-byte pairs "
+                             "per model visibility)",
+                     "gather_tb_s": gather},
+        "host": host_info(), "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    gf.close()
+
+
+def grid_cpu_baseline(f, img, m, uvw, fa, freq, seconds):
+    """The reference's gridded-model loop restated in C (oracle/refcpu_grid.c,
+    single precision, records split over pthreads as ObitSkyModelFTGrid) on a
+    record sample, every host core; the plane from the oracle's FFT (not timed)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    import oracle_grid as OG
+    from obit_b200 import uvdata as U
+    from obit_b200.skymodel import OP_SUB, SkyModelParams
+
+    gm = OG.build(f, OG.GridImage(img.nx, img.ny, img.crpixX, img.crpixY), m)
+    cores = oracle.nthreads_default()
+    p = SkyModelParams(op=OP_SUB)
+    nrow = cores
+    while True:
+        uv = U.make_uvdata(uvw[:nrow], 4, 256, 4, freq, fa, np.random.default_rng(9))
+        t0 = time.perf_counter()
+        OG.apply_c(gm, uv, p, nthreads=cores)
+        dt = time.perf_counter() - t0
+        if dt >= seconds / 2 or nrow >= len(uvw):
+            break
+        nrow = min(len(uvw), max(nrow * 2, int(nrow * seconds / max(dt, 1e-3))))
+    return {"value": nrow * 1024 / dt / 1e9, "unit": "G model visibilities/s", "cores": cores, "kind": "port",
+            "sample": f"{nrow} records x 1024 channels (2 polarizations subtracted), {dt:.1f} s: "
+                      "oracle/refcpu_grid.c, the reference's ThreadSkyModelFTGrid loop in single precision"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -741,6 +906,9 @@ def main():
         return
     if args.workload == "beam":
         run_beam(args)
+        return
+    if args.workload == "grid":
+        run_grid(args)
         return
 
     import torch

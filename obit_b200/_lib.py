@@ -121,6 +121,10 @@ class ObitDFTBeam(C.Structure):
     ]
 
 
+class ObitDFTGridImage(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("crpixX", C.c_float), ("crpixY", C.c_float)]
+
+
 class ObitDFTBeamImages(C.Structure):
     _fields_ = [
         ("numAntType", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nplane", C.c_int),
@@ -182,6 +186,19 @@ SIGNATURES = {
                                          C.POINTER(ObitDFTCCModelMF), C.POINTER(C.c_float), C.c_longlong,
                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]),
+    # gridded model FT (obit_dft_grid.h)
+    "obit_dft_grid_create": (C.c_int, [C.POINTER(ObitDFTCCField), C.POINTER(ObitDFTGridImage),
+                                       C.POINTER(ObitDFTCCModel), C.c_float, C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_void_p)]),
+    "obit_dft_grid_apply": (C.c_int, [C.c_void_p, C.POINTER(GPUVisInfo), C.c_int, C.c_float, C.c_int,
+                                      C.c_void_p, C.c_int, C.c_void_p]),
+    "obit_dft_grid_apply_host": (C.c_int, [C.c_void_p, C.POINTER(GPUVisInfo), C.c_int, C.c_float, C.c_int,
+                                           C.c_void_p, C.c_int, C.c_void_p]),
+    "obit_dft_grid_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]),
+    "obit_dft_grid_plane": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_longlong]),
+    "obit_dft_grid_destroy": (C.c_int, [C.c_void_p]),
+    "obit_dft_choose_mode": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), C.c_int, C.c_longlong, C.c_int]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),
@@ -203,6 +220,8 @@ SIGNATURES = {
 OBIT_DFT_RECUR = 0
 OBIT_DFT_PLAIN = 1
 OBIT_DFT_RECUR_CHAIN = 2  # recurrence without the spectral-factored form (comparator)
+OBIT_DFT_GRID_KERNEL_REFERENCE = 0  # the reference's interpolation-kernel table
+OBIT_DFT_GRID_KERNEL_EXACT = 1      # Lagrange weights at the requested point
 
 _lib = None
 

@@ -23,9 +23,9 @@ LIB = PKG / "libobit_dft.so"
 OBJ = PKG / "_build"
 
 CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "dft_beam.cu", "beam_jones.cu", "abi_layout.cu",
-              "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu"]
+              "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu", "grid_model.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
-CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp"]
+CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp", "grid_host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -92,7 +92,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             print(log, file=sys.stderr)
     objs = [str(OBJ / (s + ".o")) for s in CU_SOURCES + C_SOURCES + CXX_SOURCES]
     tmp = LIB.with_suffix(".so.tmp")
-    _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lpthread"], verbose)
+    # cuFFT (the gridded model's FFT) from the toolkit, found at run time where it lies
+    cuda_lib = str(Path(_cuda_include()).parent / "lib64")
+    _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, f"-L{cuda_lib}", "-lcufft",
+          "-Xlinker", f"-rpath={cuda_lib}", "-lpthread"], verbose)
     os.replace(tmp, LIB)
     return LIB
 

@@ -16,10 +16,14 @@
 #include "abi_internal.h"
 #include "obit_dft.h"
 #include "obit_dft_comps.h"
+#include "sky_geom.h"
 
 namespace {
 
 using obit::set_last_error;
+using obit::geom::shift_sin;
+using obit::geom::shift_sin_d;
+using obit::geom::urot3d;
 
 constexpr double kPi = 3.14159265358979323846;
 // ObitSkyModelCompType numbering (ObitSkyModel.h)
@@ -38,83 +42,6 @@ struct Entry {
   float dx, dy, flux, dz;
   std::vector<float> spec;
 };
-
-// ObitSkyGeomShiftSIN (ObitSkyGeom.c:177-205): FP64 direction cosines of the
-// field centre in the map frame, FP32 phase-shift terms 2 pi (l, m, n - 1).
-void shift_sin(double ra, double dec, float rotate, double xra, double xdec, float dxyzc[3]) {
-  // the reference's DG2RAD macro expands unparenthesized: rotate * pi / 180
-  const float maprr = (float)(rotate * kPi / 180.0);
-  const double d2r = kPi / 180.0;
-  const double xxshft = std::cos(d2r * xdec) * std::sin(d2r * (xra - ra));
-  const double yyshft = std::sin(d2r * xdec) * std::cos(d2r * dec) -
-                        std::cos(d2r * xdec) * std::sin(d2r * dec) * std::cos(d2r * (xra - ra));
-  const float xshift = (float)(std::cos((double)maprr) * xxshft + std::sin((double)maprr) * yyshft);
-  const float yshift = (float)(-std::sin((double)maprr) * xxshft + std::cos((double)maprr) * yyshft);
-  const float x2 = xshift * xshift, y2 = yshift * yshift;  // single-precision squares
-  const double dz = std::sqrt(1.0 - (double)x2 - (double)y2);
-  dxyzc[0] = (float)(2.0 * kPi * (double)xshift);
-  dxyzc[1] = (float)(2.0 * kPi * (double)yshift);
-  dxyzc[2] = (float)(2.0 * kPi * (dz - 1.0));
-}
-
-// The same shift terms with no single-precision rounding (FP64 positions).
-void shift_sin_d(double ra, double dec, float rotate, double xra, double xdec, double dxyzc[3]) {
-  const double maprr = (double)rotate * kPi / 180.0;
-  const double d2r = kPi / 180.0;
-  const double xxshft = std::cos(d2r * xdec) * std::sin(d2r * (xra - ra));
-  const double yyshft = std::sin(d2r * xdec) * std::cos(d2r * dec) -
-                        std::cos(d2r * xdec) * std::sin(d2r * dec) * std::cos(d2r * (xra - ra));
-  const double xshift = std::cos(maprr) * xxshft + std::sin(maprr) * yyshft;
-  const double yshift = -std::sin(maprr) * xxshft + std::cos(maprr) * yyshft;
-  const double dz = std::sqrt(1.0 - xshift * xshift - yshift * yshift);
-  dxyzc[0] = 2.0 * kPi * xshift;
-  dxyzc[1] = 2.0 * kPi * yshift;
-  dxyzc[2] = 2.0 * kPi * (dz - 1.0);
-}
-
-// ObitUVDescShift3DMatrix, 3-D image branch (ObitUVDesc.c:913-978): the uv
-// re-projection matrix R(map +) X R(uv -), FP64 products in the reference's
-// summation order, FP32 result.
-template <typename T>
-void urot3d(double ra, double dec, double xra, double xdec, float mrot, float urot, T U[3][3]) {
-  const double d2r = kPi / 180.0;
-  const double sa = std::sin(d2r * (xra - ra)), ca = std::cos(d2r * (xra - ra));
-  const double sd = std::sin(d2r * xdec), cd = std::cos(d2r * xdec);
-  const double sd0 = std::sin(d2r * dec), cd0 = std::cos(d2r * dec);
-  double rm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 1.0}};
-  double r = d2r * (double)mrot;
-  rm[0][0] = std::cos(r);
-  rm[1][1] = rm[0][0];
-  rm[1][0] = -std::sin(r);
-  rm[0][1] = std::sin(r);
-  double x[3][3];
-  x[0][0] = ca;
-  x[1][0] = -sd * sa;
-  x[2][0] = cd * sa;
-  x[0][1] = sd0 * sa;
-  x[1][1] = cd * cd0 + sd * sd0 * ca;
-  x[2][1] = sd * cd0 - cd * sd0 * ca;
-  x[0][2] = -cd0 * sa;
-  x[1][2] = cd * sd0 - sd * cd0 * ca;
-  x[2][2] = sd * sd0 + cd * cd0 * ca;
-  double t[3][3];
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) {
-      t[j][i] = 0.0;
-      for (int k = 0; k < 3; k++) t[j][i] += x[k][i] * rm[j][k];
-    }
-  r = d2r * (double)urot;
-  rm[0][0] = std::cos(r);
-  rm[1][1] = rm[0][0];
-  rm[1][0] = std::sin(r);
-  rm[0][1] = -std::sin(r);
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++) {
-      double s = 0.0;
-      for (int k = 0; k < 3; k++) s += rm[k][i] * t[j][k];
-      U[j][i] = (T)s;
-    }
-}
 
 // Model type of a field: the first selected row's PARMS[3] (ObitSkyModel.c:1767-1790).
 int field_type(const ObitDFTCCField& f, int start) {

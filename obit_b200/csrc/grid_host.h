@@ -1,0 +1,42 @@
+// Host-side plan of a gridded-model field (grid_host.cpp), consumed by the
+// device half (grid_model.cu).
+#pragma once
+#include <vector>
+
+#include "obit_dft_grid.h"
+
+namespace obit {
+
+constexpr int kGridHalfWidth = 12;                 // HWIDTH, ObitSkyModel.c:75
+constexpr int kGridTaps = 2 * kGridHalfWidth + 1;  // taps per axis
+constexpr int kGridTableRows = 201;                // 1 + 1 / 0.005, ObitCInterpolate.c:760
+
+struct GridHostPlan {
+  int nx = 0, ny = 0;        // grid: OverSample x the image
+  int nxp = 0;               // plane columns: nx / 2 + 1 + HWIDTH conjugate columns
+  int pitch = 0;             // complex values per plane row in device memory (even, > nxp)
+  std::vector<int> cell;     // distinct cells of the quadrant-swapped grid, first-touch order
+  std::vector<float> flux;   // their summed fluxes
+  int ncomp = 0, bad = 0;
+  float gparm[3] = {-1.f, -1.f, -1.f};
+  bool doGaus = false;
+  float b1 = 0.f, b2 = 0.f, b3 = 0.f, dV = 0.f;
+  std::vector<float> UU;     // u of each half-plane column, as the taper loop accumulates it
+  float crpix0 = 0.f, crpix1 = 0.f, cdelt0 = 0.f, cdelt1 = 0.f;
+  std::vector<float> table;  // kGridTableRows x kGridTaps
+  float flip = 1.f;
+  bool do3Dmul = false, doRot = false, doPC = false;
+  float umat[3][3];
+  float ccrot = 1.f, ssrot = 0.f;
+  float dxyzc[3] = {0.f, 0.f, 0.f};
+};
+
+// The reference's Lagrange kernel table (kGridTableRows x kGridTaps).
+void grid_kernel_table(std::vector<float>* tab);
+
+// Everything of a field that is computed on the host.  Returns OBIT_DFT_OK or
+// an error code with the last error set.
+int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+                   float maxGrid, GridHostPlan* g);
+
+}  // namespace obit

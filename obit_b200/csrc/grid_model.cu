@@ -1,0 +1,656 @@
+// Device half of the gridded model FT (include/obit_dft_grid.h).
+//
+// Per field (obit_dft_grid_create): the distinct grid cells from the host plan
+// are stored into a zeroed, quadrant-swapped grid of nx x ny floats; cuFFT
+// transforms it to ny rows of nx/2 + 1 complex values; one kernel then writes
+// the interpolator's plane -- rows swapped (ObitCArray2DCenter), the Gaussian
+// taper applied, HWIDTH conjugate columns in front (ObitCArrayAddConjg) -- in
+// rows of `pitch` complex values, and the FFT buffers are released.
+//
+// Per call (obit_dft_grid_apply), grid_apply_kernel: one warp per 32
+// consecutive (IF, channel) pairs of a record.  Phase A, a lane per pair: u, v,
+// w at the channel, re-projection or rotation, the half-plane conjugation, the
+// plane pixel and the interpolation window with its 25 + 25 weights (the
+// reference's table rows, or exact Lagrange weights) into the warp's
+// shared-memory slots.  Phase B, per pair, the whole warp: 13 lanes read a row
+// of the 25 x 25 window as 16-byte column pairs, the two half-warps take
+// alternate rows, each lane sums its column pair over the rows with the row
+// weights, then weights the two columns and the warp reduces.  Phase C, a lane
+// per pair again: normalization, field-offset phase, conjugation back, doFlip,
+// and subtract / divide / replace over the selected polarizations.  Every
+// single-precision step that decides a window or a table row rounds as the
+// reference's code does (no contraction), so the windows and rows are the
+// reference's.
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "abi_internal.h"
+#include "grid_host.h"
+#include "obit_dft_grid.h"
+
+using obit::GridHostPlan;
+using obit::kGridHalfWidth;
+using obit::kGridTableRows;
+using obit::kGridTaps;
+
+struct ObitDFTGrid {
+  int device = 0;
+  int kernel = OBIT_DFT_GRID_KERNEL_REFERENCE;
+  GridHostPlan hp;
+  float2* d_plane = nullptr;  // ny rows of hp.pitch complex values
+  float* d_table = nullptr;   // kGridTableRows x kGridTaps
+  float* d_stage = nullptr;   // records of apply_host
+  size_t stageBytes = 0;
+  float* d_fscale = nullptr;  // device copy of a host freqScale
+  size_t fscaleCount = 0;
+};
+
+namespace {
+
+int fail(int code, const std::string& msg) {
+  obit::set_last_error(msg);
+  return code;
+}
+
+#define CUDA_TRY(call)                                                              \
+  do {                                                                              \
+    cudaError_t _e = (call);                                                        \
+    if (_e != cudaSuccess)                                                          \
+      return fail(OBIT_DFT_ECUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+// ---- field set-up kernels ----------------------------------------------------
+
+__global__ void grid_scatter_kernel(const int* __restrict__ cell, const float* __restrict__ flux, int n,
+                                    float* __restrict__ grid) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) grid[cell[i]] = flux[i];  // cells are distinct: sums were formed on the host
+}
+
+struct PlaneParams {
+  const float2* fft;  // ny rows of nx/2 + 1
+  float2* plane;
+  int nx, ny, pitch, nxp;
+  int doGaus;
+  float b1, b2, b3, dV;
+  const float* UU;
+};
+
+// Tapered FFT value at centred row r (ky = r - ny/2) and half-plane column j,
+// the taper in the reference's single-precision steps (ObitSkyModel.c:4315-4331).
+__device__ __forceinline__ float2 tapered(const PlaneParams& p, int r, int j) {
+  const int nh = p.nx / 2 + 1;
+  float2 v = p.fft[(size_t)((r + p.ny / 2) % p.ny) * nh + j];
+  if (p.doGaus) {
+    const float VV = __fmul_rn(p.dV, (float)(r - p.nx / 2));
+    const float bb2 = __fmul_rn(__fmul_rn(p.b2, VV), VV);
+    const float bb3 = __fmul_rn(p.b3, VV);
+    const float UU = p.UU[j];
+    const float texp = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(p.b1, UU), UU), bb2), __fmul_rn(bb3, UU));
+    const float t = texp > -14.0f ? (float)exp((double)texp) : 0.0f;
+    v.x = __fmul_rn(v.x, t);
+    v.y = __fmul_rn(v.y, t);
+  }
+  return v;
+}
+
+__global__ void grid_plane_kernel(PlaneParams p) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (c >= p.pitch) return;
+  float2 out = make_float2(0.0f, 0.0f);
+  constexpr int H = kGridHalfWidth;
+  if (c < p.nxp) {
+    if (c >= H) {
+      out = tapered(p, r, c - H);
+    } else {
+      // conjugate columns; row 0 reads columns H + 1 .. 2H of itself (ObitCArray.c:1712-1722)
+      const float2 s = r >= 1 ? tapered(p, p.ny - r, H - c) : tapered(p, 0, 2 * H - c);
+      out = make_float2(s.x, -s.y);
+    }
+  }
+  p.plane[(size_t)r * p.pitch + c] = out;
+}
+
+// ---- the per-record kernel ------------------------------------------------------
+
+struct GridApplyParams {
+  const float2* plane;
+  int pitch, nxp, nyp;
+  float crpix0, crpix1, cdelt0, cdelt1;
+  const float* table;
+  int exact;
+  float flip;
+  int do3Dmul, doRot, doPC;
+  float um[9];
+  float ccrot, ssrot;
+  float d0, d1, d2;
+  float* vis;
+  int nvis, lrec, nrparm, ilocu, ilocv, ilocw;
+  const float* fscale;
+  int kincf, kincif;
+  int chanb, nchan, ifb, nif;
+  int incf, incif, incs;  // floats
+  int stokb, nstok;
+  int op;
+  float stokFactor;
+  int doFlip;
+  int nsel, nchunk;       // selected (IF, channel) pairs per record; 32-pair chunks
+};
+
+constexpr int kApplyWarps = 4;
+constexpr int kWX = 28;  // [0] zero, [1 .. 25] column weights, [26 ..] zero
+constexpr int kWY = 26;  // row weights, [25] zero
+
+// SetConvKernal (ObitCInterpolate.c:699-745): window start, first table tap,
+// taps and table row for a pixel (1-relative) on an axis of naxis pixels.
+__device__ __forceinline__ void conv_setup(float pix, int naxis, int* start, int* k0, int* nterm, int* itab) {
+  constexpr int hw = kGridHalfWidth, iwid = kGridTaps, ntab = kGridTableRows - 1;
+  const int ipos = (int)((double)pix + 0.5);
+  int cen = ipos - hw;
+  cen = max(1, min(cen, naxis - iwid));
+  float off = __fsub_rn(__fsub_rn(pix, (float)cen), (float)hw);
+  const double od = (double)off;
+  const int ioff = od > 0.0 ? (int)(od + 0.5) : (int)(od - 0.5);
+  off = __fsub_rn(off, (float)ioff);
+  int it = (int)(((0.5 + (double)off) * (double)ntab) + 0.5);
+  *itab = max(0, min(it, ntab));
+  *start = cen - 1;
+  *k0 = abs(ioff);
+  *nterm = iwid - abs(ioff);
+}
+
+// Reference weights from table row itab, taps k0 .. 24, into w[off + i].
+__device__ __forceinline__ float table_weights(const float* __restrict__ tab, int itab, int k0, int nterm,
+                                               float* w) {
+  float s = 0.0f;
+  for (int i = 0; i < kGridTaps; i++) {
+    const float v = i < nterm ? __ldg(tab + itab * kGridTaps + k0 + i) : 0.0f;
+    w[i] = v;
+    s += v;
+  }
+  return s;
+}
+
+// Barycentric weights (-1)^i C(24, i) of 25 equispaced nodes (integers below 2^24).
+__constant__ float kBaryLam[kGridTaps] = {
+    1.f,        -24.f,      276.f,      -2024.f,    10626.f,    -42504.f,  134596.f,
+    -346104.f,  735471.f,   -1307504.f, 1961256.f,  -2496144.f, 2704156.f, -2496144.f,
+    1961256.f,  -1307504.f, 735471.f,   -346104.f,  134596.f,   -42504.f,  10626.f,
+    -2024.f,    276.f,      -24.f,      1.f};
+
+// Exact 25-point Lagrange weights at position t (0 .. 24) of the window, by the
+// barycentric formula.
+__device__ __forceinline__ float exact_weights(float t, float* w) {
+  float s = 0.0f;
+  int hit = -1;
+  for (int i = 0; i < kGridTaps; i++) {
+    const float d = t - (float)i;
+    if (d == 0.0f) hit = i;
+    const float v = d != 0.0f ? kBaryLam[i] / d : 0.0f;
+    w[i] = v;
+    s += v;
+  }
+  if (hit >= 0) {
+    for (int i = 0; i < kGridTaps; i++) w[i] = i == hit ? 1.0f : 0.0f;
+    return 1.0f;
+  }
+  const float inv = 1.0f / s;
+  for (int i = 0; i < kGridTaps; i++) w[i] *= inv;
+  return 1.0f;
+}
+
+__global__ void __launch_bounds__(kApplyWarps * 32) grid_apply_kernel(GridApplyParams p) {
+  __shared__ float sw[kApplyWarps][32][kWX + kWY];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float* mywx = sw[wib][lane];
+  float* mywy = mywx + kWX;
+  const long long nitems = (long long)p.nvis * p.nchunk;
+  for (long long item = (long long)blockIdx.x * kApplyWarps + wib; item < nitems;
+       item += (long long)gridDim.x * kApplyWarps) {
+    const int rec = (int)(item / p.nchunk), chunk = (int)(item % p.nchunk);
+    const int fidx = chunk * 32 + lane;
+    const bool valid = fidx < p.nsel;
+    const int iIF = p.ifb + (valid ? fidx / p.nchan : 0);
+    const int iCh = p.chanb + (valid ? fidx % p.nchan : 0);
+    float* rp = p.vis + (size_t)rec * p.lrec;
+
+    // ---- phase A: this lane's (IF, channel) ----
+    float u = 0.f, v = 0.f, w = 0.f, sumwt = 0.f;
+    int sx = 0, sy = 0;
+    bool bad = true, conj = false;
+    if (valid) {
+      const float ff = __ldg(p.fscale + iIF * p.kincif + iCh * p.kincf);
+      u = __fmul_rn(ff, rp[p.ilocu]);
+      v = __fmul_rn(ff, rp[p.ilocv]);
+      w = __fmul_rn(ff, rp[p.ilocw]);
+      if (p.do3Dmul) {
+        const float* m = p.um;
+        const float ut = __fadd_rn(__fadd_rn(__fmul_rn(u, m[0]), __fmul_rn(v, m[1])), __fmul_rn(w, m[2]));
+        const float vt = __fadd_rn(__fadd_rn(__fmul_rn(u, m[3]), __fmul_rn(v, m[4])), __fmul_rn(w, m[5]));
+        const float wt = __fadd_rn(__fadd_rn(__fmul_rn(u, m[6]), __fmul_rn(v, m[7])), __fmul_rn(w, m[8]));
+        u = ut;
+        v = vt;
+        w = wt;
+      } else if (p.doRot) {
+        const float ut = __fsub_rn(__fmul_rn(p.ccrot, u), __fmul_rn(p.ssrot, v));
+        const float vt = __fadd_rn(__fmul_rn(p.ccrot, v), __fmul_rn(p.ssrot, u));
+        u = ut;
+        v = vt;
+      }
+      conj = __fmul_rn(p.flip, u) < 0.0f;
+      if (conj) {
+        u = -u;
+        v = -v;
+        w = -w;
+      }
+      const float px = __fadd_rn(p.crpix0, __fdiv_rn(u, p.cdelt0));
+      const float py = __fadd_rn(p.crpix1, __fdiv_rn(v, p.cdelt1));
+      if (px >= 1.0f && px <= (float)p.nxp && py >= 1.0f && py <= (float)p.nyp) {
+        mywx[0] = mywx[26] = mywx[27] = 0.0f;
+        mywy[25] = 0.0f;
+        if (!p.exact) {
+          int k0, nt, it;
+          conv_setup(px, p.nxp, &sx, &k0, &nt, &it);
+          const float swx = table_weights(p.table, it, k0, nt, mywx + 1);
+          conv_setup(py, p.nyp, &sy, &k0, &nt, &it);
+          const float swy = table_weights(p.table, it, k0, nt, mywy);
+          sumwt = swx * swy;
+        } else {
+          // the requested point itself: 0-relative position px (py) on the plane
+          sx = min(max((int)floorf(px + 0.5f) - kGridHalfWidth, 0), p.nxp - kGridTaps);
+          sy = min(max((int)floorf(py + 0.5f) - kGridHalfWidth, 0), p.nyp - kGridTaps);
+          exact_weights(px - (float)sx, mywx + 1);
+          sumwt = exact_weights(py - (float)sy, mywy);
+        }
+        bad = !(sumwt > 0.5f);
+      }
+    }
+    __syncwarp();
+
+    // ---- phase B: the window sums, one (IF, channel) at a time ----
+    float mr = 0.f, mi = 0.f;
+    unsigned todo = __ballot_sync(0xffffffffu, valid && !bad);
+    const int cp = lane & 15, half = lane >> 4;
+    while (todo) {
+      const int c = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int csx = __shfl_sync(0xffffffffu, sx, c);
+      const int csy = __shfl_sync(0xffffffffu, sy, c);
+      const int x0e = csx & ~1;
+      const float* cwx = sw[wib][c];
+      const float* cwy = cwx + kWX;
+      float sr = 0.f, si = 0.f;
+      if (cp < 13) {
+        const float4* row =
+            reinterpret_cast<const float4*>(p.plane + (size_t)(csy + half) * p.pitch + x0e) + cp;
+        const size_t step = (size_t)p.pitch;  // two rows, in float4
+        float a0r = 0.f, a0i = 0.f, a1r = 0.f, a1i = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < 13; jj++) {
+          const int j = 2 * jj + half;
+          if (j < kGridTaps) {
+            const float4 q = __ldg(row + jj * step);
+            const float wy = cwy[j];
+            a0r = fmaf(wy, q.x, a0r);
+            a0i = fmaf(wy, q.y, a0i);
+            a1r = fmaf(wy, q.z, a1r);
+            a1i = fmaf(wy, q.w, a1i);
+          }
+        }
+        const int rel = x0e + 2 * cp - csx;  // -1 .. 24
+        const float wa = cwx[rel + 1], wb = cwx[rel + 2];
+        sr = fmaf(wa, a0r, wb * a1r);
+        si = fmaf(wa, a0i, wb * a1i);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if (lane == c) {
+        mr = sr;
+        mi = si;
+      }
+    }
+    __syncwarp();
+
+    // ---- phase C: this lane's (IF, channel) applied to its polarizations ----
+    if (valid) {
+      float wtf = 1.0f;
+      if (!bad) {
+        mr = __fdiv_rn(mr, sumwt);
+        mi = __fdiv_rn(mi, sumwt);
+        if (p.doPC) {
+          const float pc = __fadd_rn(__fadd_rn(__fmul_rn(u, p.d0), __fmul_rn(v, p.d1)), __fmul_rn(w, p.d2));
+          double sd, cd;
+          sincos((double)pc, &sd, &cd);
+          const float cs = (float)cd, sn = (float)sd;
+          const float rt = __fsub_rn(__fmul_rn(cs, mr), __fmul_rn(sn, mi));
+          const float it = __fadd_rn(__fmul_rn(cs, mi), __fmul_rn(sn, mr));
+          mr = rt;
+          mi = it;
+        }
+        if (conj) mi = -mi;
+        if (p.doFlip) {
+          const float t = mr;
+          mr = -mi;
+          mi = t;
+        }
+        if (p.op == GPUOpTypeDiv) {
+          const float wt = __fadd_rn(__fmul_rn(mr, mr), __fmul_rn(mi, mi));
+          mr = __fdiv_rn(mr, wt);
+          mi = __fdiv_rn(mi, wt);
+          wtf = __fsqrt_rn(wt);
+        }
+      }
+      float* base = rp + p.nrparm + iIF * p.incif + iCh * p.incf;
+      for (int s = p.stokb; s < p.stokb + p.nstok; s++) {
+        float* cv = base + s * p.incs;
+        if (cv[2] <= 0.0f && p.op != GPUOpTypeRepl) continue;
+        if (bad) {
+          cv[0] = 0.0f;
+          cv[1] = 0.0f;
+          cv[2] = 0.0f;
+        } else if (p.op == GPUOpTypeDiv) {
+          const float vr = cv[0], vi = cv[1];
+          cv[0] = __fadd_rn(__fmul_rn(mr, vr), __fmul_rn(mi, vi));
+          cv[1] = __fsub_rn(__fmul_rn(mr, vi), __fmul_rn(mi, vr));
+          cv[2] = __fmul_rn(cv[2], wtf);
+        } else if (p.op == GPUOpTypeRepl) {
+          cv[0] = mr;
+          cv[1] = mi;
+        } else {
+          cv[0] = __fsub_rn(cv[0], mr);
+          cv[1] = __fsub_rn(cv[1], mi);
+        }
+        mr = __fmul_rn(mr, p.stokFactor);
+        mi = __fmul_rn(mi, p.stokFactor);
+      }
+    }
+  }
+}
+
+int apply_params(const ObitDFTGrid* g, const GPUVisInfo* v, int opType, float stokFactor, int doFlip,
+                 float* d_vis, int nvis, GridApplyParams* p) {
+  if (!v) return fail(OBIT_DFT_EBADARG, "grid apply: null GPUVisInfo");
+  if (opType < GPUOpTypeSub || opType > GPUOpTypeRepl) return fail(OBIT_DFT_EBADARG, "grid apply: bad opType");
+  if (nvis < 0 || (nvis > 0 && !d_vis)) return fail(OBIT_DFT_EBADARG, "grid apply: bad records");
+  if (!v->freqScale) return fail(OBIT_DFT_EBADARG, "grid apply: freqScale is required");
+  if (v->lenvis <= 0 || v->nrparm < 0 || v->nchan <= 0 || v->nIF <= 0 || v->nstok <= 0)
+    return fail(OBIT_DFT_EBADARG, "grid apply: bad record layout");
+  if (v->ilocu < 0 || v->ilocv < 0 || v->ilocw < 0 || v->ilocu >= v->nrparm || v->ilocv >= v->nrparm ||
+      v->ilocw >= v->nrparm)
+    return fail(OBIT_DFT_EBADARG, "grid apply: u, v, w offsets outside the random parameters");
+  if (v->chanb < 0 || v->chane < v->chanb || v->chane >= v->nchan || v->IFb < 0 || v->IFe < v->IFb ||
+      v->IFe >= v->nIF || v->stokb < 0 || v->stoke < v->stokb || v->stoke >= v->nstok)
+    return fail(OBIT_DFT_EBADARG, "grid apply: bad channel, IF or polarization selection");
+  if (v->incf <= 0 || v->incif <= 0 || v->incs <= 0 || v->kincf <= 0 || v->kincif <= 0)
+    return fail(OBIT_DFT_EBADARG, "grid apply: bad increments");
+  const long long last = (long long)v->nrparm +
+                         3LL * ((long long)v->IFe * v->incif + (long long)v->chane * v->incf +
+                                (long long)v->stoke * v->incs) + 2;
+  if (last >= v->lenvis) return fail(OBIT_DFT_EBADARG, "grid apply: selection beyond the record length");
+  const GridHostPlan& h = g->hp;
+  GridApplyParams q = {};
+  q.plane = g->d_plane;
+  q.pitch = h.pitch;
+  q.nxp = h.nxp;
+  q.nyp = h.ny;
+  q.crpix0 = h.crpix0;
+  q.crpix1 = h.crpix1;
+  q.cdelt0 = h.cdelt0;
+  q.cdelt1 = h.cdelt1;
+  q.table = g->d_table;
+  q.exact = g->kernel == OBIT_DFT_GRID_KERNEL_EXACT;
+  q.flip = h.flip;
+  q.do3Dmul = h.do3Dmul;
+  q.doRot = h.doRot;
+  q.doPC = h.doPC;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) q.um[i * 3 + j] = h.umat[i][j];
+  q.ccrot = h.ccrot;
+  q.ssrot = h.ssrot;
+  q.d0 = h.dxyzc[0];
+  q.d1 = h.dxyzc[1];
+  q.d2 = h.dxyzc[2];
+  q.vis = d_vis;
+  q.nvis = nvis;
+  q.lrec = v->lenvis;
+  q.nrparm = v->nrparm;
+  q.ilocu = v->ilocu;
+  q.ilocv = v->ilocv;
+  q.ilocw = v->ilocw;
+  q.fscale = v->freqScale;
+  q.kincf = v->kincf;
+  q.kincif = v->kincif;
+  q.chanb = v->chanb;
+  q.nchan = v->chane - v->chanb + 1;
+  q.ifb = v->IFb;
+  q.nif = v->IFe - v->IFb + 1;
+  q.incf = 3 * v->incf;
+  q.incif = 3 * v->incif;
+  q.incs = 3 * v->incs;
+  q.stokb = v->stokb;
+  q.nstok = v->stoke - v->stokb + 1;
+  q.op = opType;
+  q.stokFactor = stokFactor;
+  q.doFlip = doFlip ? 1 : 0;
+  q.nsel = q.nchan * q.nif;
+  q.nchunk = (q.nsel + 31) / 32;
+  *p = q;
+  return OBIT_DFT_OK;
+}
+
+// freqScale in host memory is copied (in order on `st`) to a device buffer of
+// the field; device or managed memory is read in place.
+int resolve_fscale(ObitDFTGrid* g, const GPUVisInfo* v, cudaStream_t st, GridApplyParams* q) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, v->freqScale) != cudaSuccess) {
+    cudaGetLastError();
+    at.type = cudaMemoryTypeUnregistered;
+  }
+  if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return OBIT_DFT_OK;
+  const size_t n = (size_t)v->IFe * v->kincif + (size_t)v->chane * v->kincf + 1;
+  if (n > g->fscaleCount) {
+    cudaFree(g->d_fscale);
+    g->d_fscale = nullptr;
+    g->fscaleCount = 0;
+    CUDA_TRY(cudaMalloc(&g->d_fscale, sizeof(float) * n));
+    g->fscaleCount = n;
+  }
+  CUDA_TRY(cudaMemcpyAsync(g->d_fscale, v->freqScale, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  q->fscale = g->d_fscale;
+  return OBIT_DFT_OK;
+}
+
+int launch_apply(const GridApplyParams& q, cudaStream_t st) {
+  if (q.nvis == 0) return OBIT_DFT_OK;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const long long items = (long long)q.nvis * q.nchunk;
+  const long long want = (items + kApplyWarps - 1) / kApplyWarps;
+  const int grid = (int)std::min<long long>(want, (long long)nsm * 8);
+  grid_apply_kernel<<<grid, kApplyWarps * 32, 0, st>>>(q);
+  CUDA_TRY(cudaGetLastError());
+  return OBIT_DFT_OK;
+}
+
+void release(ObitDFTGrid* g) {
+  if (!g) return;
+  cudaFree(g->d_plane);
+  cudaFree(g->d_table);
+  cudaFree(g->d_stage);
+  cudaFree(g->d_fscale);
+  delete g;
+}
+
+}  // namespace
+
+extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGridImage* image,
+                                    const ObitDFTCCModel* model, float maxGrid, int kernel, void* stream,
+                                    ObitDFTGrid** out) {
+  if (!out) return fail(OBIT_DFT_EBADARG, "grid create: null output");
+  *out = nullptr;
+  if (kernel != OBIT_DFT_GRID_KERNEL_REFERENCE && kernel != OBIT_DFT_GRID_KERNEL_EXACT)
+    return fail(OBIT_DFT_EBADARG, "grid create: unknown kernel");
+  ObitDFTGrid* g = new ObitDFTGrid();
+  g->kernel = kernel;
+  int rc = obit::grid_host_plan(field, image, model, maxGrid, &g->hp);
+  if (rc) {
+    delete g;
+    return rc;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const GridHostPlan& h = g->hp;
+  float* d_grid = nullptr;
+  float2* d_fft = nullptr;
+  int* d_cell = nullptr;
+  float* d_flux = nullptr;
+  float* d_UU = nullptr;
+  cufftHandle plan = 0;
+  bool havePlan = false;
+  auto cleanup = [&]() {
+    cudaFree(d_grid);
+    cudaFree(d_fft);
+    cudaFree(d_cell);
+    cudaFree(d_flux);
+    cudaFree(d_UU);
+    if (havePlan) cufftDestroy(plan);
+  };
+  auto bail = [&](int code, const std::string& msg) {
+    cleanup();
+    release(g);
+    return fail(code, msg);
+  };
+  cudaError_t e = cudaGetDevice(&g->device);
+  if (e != cudaSuccess) return bail(OBIT_DFT_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (h.ncomp == 0) {
+    *out = g;  // nothing gridded: the reference skips the field
+    return OBIT_DFT_OK;
+  }
+  const size_t nh = (size_t)h.nx / 2 + 1;
+  const size_t ncell = h.cell.size();
+  if ((e = cudaMalloc(&g->d_plane, sizeof(float2) * (size_t)h.ny * h.pitch)) != cudaSuccess ||
+      (e = cudaMalloc(&g->d_table, sizeof(float) * h.table.size())) != cudaSuccess ||
+      (e = cudaMalloc(&d_grid, sizeof(float) * (size_t)h.nx * h.ny)) != cudaSuccess ||
+      (e = cudaMalloc(&d_fft, sizeof(float2) * nh * h.ny)) != cudaSuccess ||
+      (e = cudaMalloc(&d_cell, sizeof(int) * ncell)) != cudaSuccess ||
+      (e = cudaMalloc(&d_flux, sizeof(float) * ncell)) != cudaSuccess ||
+      (e = cudaMalloc(&d_UU, sizeof(float) * std::max<size_t>(1, h.UU.size()))) != cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, std::string("grid create: cudaMalloc: ") + cudaGetErrorString(e));
+  if ((e = cudaMemcpyAsync(g->d_table, h.table.data(), sizeof(float) * h.table.size(), cudaMemcpyHostToDevice,
+                           st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(d_cell, h.cell.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(d_flux, h.flux.data(), sizeof(float) * ncell, cudaMemcpyHostToDevice, st)) !=
+          cudaSuccess ||
+      (!h.UU.empty() && (e = cudaMemcpyAsync(d_UU, h.UU.data(), sizeof(float) * h.UU.size(),
+                                             cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+      (e = cudaMemsetAsync(d_grid, 0, sizeof(float) * (size_t)h.nx * h.ny, st)) != cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, std::string("grid create: copy: ") + cudaGetErrorString(e));
+  grid_scatter_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(d_cell, d_flux, (int)ncell, d_grid);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, std::string("grid scatter: ") + cudaGetErrorString(e));
+  // ObitSkyModelFTImage: forward real-to-half-complex transform, unnormalized
+  if (cufftPlan2d(&plan, h.ny, h.nx, CUFFT_R2C) != CUFFT_SUCCESS)
+    return bail(OBIT_DFT_ECUDA, "grid create: cufftPlan2d failed");
+  havePlan = true;
+  if (cufftSetStream(plan, st) != CUFFT_SUCCESS ||
+      cufftExecR2C(plan, d_grid, reinterpret_cast<cufftComplex*>(d_fft)) != CUFFT_SUCCESS)
+    return bail(OBIT_DFT_ECUDA, "grid create: cufftExecR2C failed");
+  PlaneParams pp;
+  pp.fft = d_fft;
+  pp.plane = g->d_plane;
+  pp.nx = h.nx;
+  pp.ny = h.ny;
+  pp.pitch = h.pitch;
+  pp.nxp = h.nxp;
+  pp.doGaus = h.doGaus;
+  pp.b1 = h.b1;
+  pp.b2 = h.b2;
+  pp.b3 = h.b3;
+  pp.dV = h.dV;
+  pp.UU = d_UU;
+  grid_plane_kernel<<<dim3((unsigned)((h.pitch + 255) / 256), (unsigned)h.ny), 256, 0, st>>>(pp);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, std::string("grid plane: ") + cudaGetErrorString(e));
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, std::string("grid create: ") + cudaGetErrorString(e));
+  cleanup();
+  *out = g;
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_grid_apply(ObitDFTGrid* g, const GPUVisInfo* visInfo, int opType, float stokFactor,
+                                   int doFlip, float* d_vis, int nvis, void* stream) {
+  if (!g) return fail(OBIT_DFT_EBADARG, "grid apply: null field");
+  GridApplyParams q;
+  int rc = apply_params(g, visInfo, opType, stokFactor, doFlip, d_vis, nvis, &q);
+  if (rc) return rc;
+  if (g->hp.ncomp == 0 || nvis == 0) return OBIT_DFT_OK;
+  CUDA_TRY(cudaSetDevice(g->device));
+  rc = resolve_fscale(g, visInfo, (cudaStream_t)stream, &q);
+  if (rc) return rc;
+  return launch_apply(q, (cudaStream_t)stream);
+}
+
+extern "C" int obit_dft_grid_apply_host(ObitDFTGrid* g, const GPUVisInfo* visInfo, int opType,
+                                        float stokFactor, int doFlip, float* h_vis, int nvis, void* stream) {
+  if (!g) return fail(OBIT_DFT_EBADARG, "grid apply: null field");
+  if (nvis > 0 && !h_vis) return fail(OBIT_DFT_EBADARG, "grid apply: null records");
+  if (!visInfo) return fail(OBIT_DFT_EBADARG, "grid apply: null GPUVisInfo");
+  if (nvis == 0 || g->hp.ncomp == 0) return OBIT_DFT_OK;
+  CUDA_TRY(cudaSetDevice(g->device));
+  const size_t bytes = sizeof(float) * (size_t)nvis * (size_t)std::max(0, visInfo->lenvis);
+  if (bytes > g->stageBytes) {
+    cudaFree(g->d_stage);
+    g->d_stage = nullptr;
+    g->stageBytes = 0;
+    CUDA_TRY(cudaMalloc(&g->d_stage, bytes));
+    g->stageBytes = bytes;
+  }
+  GridApplyParams q;
+  int rc = apply_params(g, visInfo, opType, stokFactor, doFlip, g->d_stage, nvis, &q);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = resolve_fscale(g, visInfo, st, &q);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(g->d_stage, h_vis, bytes, cudaMemcpyHostToDevice, st));
+  rc = launch_apply(q, st);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(h_vis, g->d_stage, bytes, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_grid_info(const ObitDFTGrid* g, long long* info, int n) {
+  if (!g || !info) return fail(OBIT_DFT_EBADARG, "grid info: null argument");
+  const GridHostPlan& h = g->hp;
+  const long long v[10] = {h.ncomp, h.bad, h.nx, h.ny, h.nxp, h.doGaus, h.do3Dmul, h.doPC, h.doRot, g->kernel};
+  for (int i = 0; i < n && i < 10; i++) info[i] = v[i];
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_grid_plane(const ObitDFTGrid* g, float* h_plane, long long capacity) {
+  if (!g || !h_plane) return fail(OBIT_DFT_EBADARG, "grid plane: null argument");
+  const GridHostPlan& h = g->hp;
+  if (!g->d_plane) return fail(OBIT_DFT_EBADARG, "grid plane: the field has no components");
+  if (capacity < 2LL * h.nxp * h.ny) return fail(OBIT_DFT_EBADARG, "grid plane: buffer too small");
+  CUDA_TRY(cudaSetDevice(g->device));
+  CUDA_TRY(cudaMemcpy2D(h_plane, sizeof(float2) * h.nxp, g->d_plane, sizeof(float2) * h.pitch,
+                        sizeof(float2) * h.nxp, h.ny, cudaMemcpyDeviceToHost));
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_grid_destroy(ObitDFTGrid* g) {
+  if (!g) return OBIT_DFT_OK;
+  cudaSetDevice(g->device);
+  release(g);
+  return OBIT_DFT_OK;
+}

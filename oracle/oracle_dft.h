@@ -120,6 +120,33 @@ int oracle_beam_apply(const OracleJob *job, const OracleBeam *beam, float *vis, 
 void oracle_beam_coeffs(int stokType, double c2p, double s2p, const float *J1, const float *J2,
                         double *cr, double *ci);
 
+/* The reference's gridded-model loop (refcpu_grid.c): the interpolator's plane
+ * (ny rows of nxp complex values), its kernel table ((ntab + 1) x 25), the
+ * field geometry and the record layout, selection and operation.  Increments
+ * and offsets in floats. */
+typedef struct RefGridJob {
+  const float *plane;
+  int nxp, ny;
+  const float *table;
+  int ntab;
+  float crpix0, crpix1, cdelt0, cdelt1;
+  float flip;
+  int do3Dmul;
+  float umat[9];
+  int doRot;
+  float ccrot, ssrot;
+  int doPC;
+  float dxyzc[3];
+  int lrec, nrparm, ilocu, ilocv, ilocw;
+  const float *fscale;
+  int kincf, kincif;
+  int chanb, nchan, ifb, nif, incf, incif, incs, stokb, nstok;
+  int doDivide, doReplace, doFlip;
+  float stokFactor;
+} RefGridJob;
+
+int refcpu_grid_apply(const RefGridJob *job, float *vis, long nvis, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif
