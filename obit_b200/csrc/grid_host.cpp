@@ -179,7 +179,10 @@ int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, c
 
   // ---- interpolator (ObitCInterpolate.c:128-206 with ObitSkyModel.c:4354-4358) ----
   g->nxp = nx / 2 + 1 + kGridHalfWidth;
-  g->pitch = (g->nxp + 2) & ~1;  // even, one spare column: 16-byte rows for pair loads
+  // even (16-byte rows for pair loads), with zero columns past the last one for
+  // the apply kernel's window unions, which may reach 7 columns beyond it
+  g->pitch = (g->nxp + 8) & ~1;
+  g->rows = ny + kGridPadRows;
   g->crpix0 = (float)kGridHalfWidth;
   g->crpix1 = (float)(ny / 2);
   g->cdelt0 = (float)(1.0 / ((-kPi / 180.0) * (double)(float)kOverSample * (double)cdx * (double)image->nx));

@@ -10,11 +10,13 @@ namespace obit {
 constexpr int kGridHalfWidth = 12;                 // HWIDTH, ObitSkyModel.c:75
 constexpr int kGridTaps = 2 * kGridHalfWidth + 1;  // taps per axis
 constexpr int kGridTableRows = 201;                // 1 + 1 / 0.005, ObitCInterpolate.c:760
+constexpr int kGridPadRows = 6;                    // zero rows after the plane (window unions)
 
 struct GridHostPlan {
   int nx = 0, ny = 0;        // grid: OverSample x the image
   int nxp = 0;               // plane columns: nx / 2 + 1 + HWIDTH conjugate columns
-  int pitch = 0;             // complex values per plane row in device memory (even, > nxp)
+  int pitch = 0;             // complex values per plane row in device memory (even, > nxp + 6)
+  int rows = 0;              // plane rows in device memory: ny, then kGridPadRows zero rows
   std::vector<int> cell;     // distinct cells of the quadrant-swapped grid, first-touch order
   std::vector<float> flux;   // their summed fluxes
   int ncomp = 0, bad = 0;

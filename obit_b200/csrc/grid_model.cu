@@ -12,10 +12,14 @@
 // w at the channel, re-projection or rotation, the half-plane conjugation, the
 // plane pixel and the interpolation window with its 25 + 25 weights (the
 // reference's table rows, or exact Lagrange weights) into the warp's
-// shared-memory slots.  Phase B, per pair, the whole warp: 13 lanes read a row
-// of the 25 x 25 window as 16-byte column pairs, the two half-warps take
-// alternate rows, each lane sums its column pair over the rows with the row
-// weights, then weights the two columns and the warp reduces.  Phase C, a lane
+// shared-memory slots.  Phase B, the whole warp, a group of up to kGroup
+// pairs at a time whose windows fit one union of kUnion x kUnion cells
+// (channels of a record move their windows by a fraction of a cell each, so
+// neighbours share most of them): the 16 lanes of each half-warp read a row of
+// the union as 16-byte column pairs, the half-warps take alternate rows, and
+// each lane sums its column pair over the rows with every member's row
+// weights; then each member's column weights and a warp reduction.  Each union
+// row is read once per group instead of once per pair.  Phase C, a lane
 // per pair again: normalization, field-offset phase, conjugation back, doFlip,
 // and subtract / divide / replace over the selected polarizations.  Every
 // single-precision step that decides a window or a table row rounds as the
@@ -41,7 +45,7 @@ struct ObitDFTGrid {
   int device = 0;
   int kernel = OBIT_DFT_GRID_KERNEL_REFERENCE;
   GridHostPlan hp;
-  float2* d_plane = nullptr;  // ny rows of hp.pitch complex values
+  float2* d_plane = nullptr;  // hp.rows rows (ny, then zero rows) of hp.pitch complex values
   float* d_table = nullptr;   // kGridTableRows x kGridTaps
   float* d_stage = nullptr;   // records of apply_host
   size_t stageBytes = 0;
@@ -104,7 +108,7 @@ __global__ void grid_plane_kernel(PlaneParams p) {
   if (c >= p.pitch) return;
   float2 out = make_float2(0.0f, 0.0f);
   constexpr int H = kGridHalfWidth;
-  if (c < p.nxp) {
+  if (c < p.nxp && r < p.ny) {
     if (c >= H) {
       out = tapered(p, r, c - H);
     } else {
@@ -143,8 +147,14 @@ struct GridApplyParams {
 };
 
 constexpr int kApplyWarps = 4;
-constexpr int kWX = 28;  // [0] zero, [1 .. 25] column weights, [26 ..] zero
-constexpr int kWY = 26;  // row weights, [25] zero
+constexpr int kSlack = 6;                      // window starts of a group's members span at most this
+constexpr int kUnion = kGridTaps + kSlack;     // union rows and columns (31)
+constexpr int kGroup = 8;                      // members summed together (registers: 4 each)
+// A lane's weight slots, zero-padded so that a member's weight at union row r
+// (column c) is slot r - dy + kSlack (c - dx + kSlack + 1), dy, dx its window's
+// offset in the union: rows 0..kUnion-1, columns -1..kUnion.
+constexpr int kWX = kGridTaps + 2 * kSlack + 3;  // 40: [0, kSlack+1) zero, 25 weights, zeros
+constexpr int kWY = kGridTaps + 2 * kSlack + 1;  // 38: [0, kSlack) zero, 25 weights, zeros
 
 // SetConvKernal (ObitCInterpolate.c:699-745): window start, first table tap,
 // taps and table row for a pixel (1-relative) on an axis of naxis pixels.
@@ -251,70 +261,103 @@ __global__ void __launch_bounds__(kApplyWarps * 32) grid_apply_kernel(GridApplyP
       const float px = __fadd_rn(p.crpix0, __fdiv_rn(u, p.cdelt0));
       const float py = __fadd_rn(p.crpix1, __fdiv_rn(v, p.cdelt1));
       if (px >= 1.0f && px <= (float)p.nxp && py >= 1.0f && py <= (float)p.nyp) {
-        mywx[0] = mywx[26] = mywx[27] = 0.0f;
-        mywy[25] = 0.0f;
+        for (int i = 0; i < kSlack + 1; i++) mywx[i] = 0.0f;
+        for (int i = kSlack + 1 + kGridTaps; i < kWX; i++) mywx[i] = 0.0f;
+        for (int i = 0; i < kSlack; i++) mywy[i] = 0.0f;
+        for (int i = kSlack + kGridTaps; i < kWY; i++) mywy[i] = 0.0f;
+        float* wxs = mywx + kSlack + 1;
+        float* wys = mywy + kSlack;
         if (!p.exact) {
           int k0, nt, it;
           conv_setup(px, p.nxp, &sx, &k0, &nt, &it);
-          const float swx = table_weights(p.table, it, k0, nt, mywx + 1);
+          const float swx = table_weights(p.table, it, k0, nt, wxs);
           conv_setup(py, p.nyp, &sy, &k0, &nt, &it);
-          const float swy = table_weights(p.table, it, k0, nt, mywy);
+          const float swy = table_weights(p.table, it, k0, nt, wys);
           sumwt = swx * swy;
         } else {
           // the requested point itself: 0-relative position px (py) on the plane
           sx = min(max((int)floorf(px + 0.5f) - kGridHalfWidth, 0), p.nxp - kGridTaps);
           sy = min(max((int)floorf(py + 0.5f) - kGridHalfWidth, 0), p.nyp - kGridTaps);
-          exact_weights(px - (float)sx, mywx + 1);
-          sumwt = exact_weights(py - (float)sy, mywy);
+          exact_weights(px - (float)sx, wxs);
+          sumwt = exact_weights(py - (float)sy, wys);
         }
         bad = !(sumwt > 0.5f);
       }
     }
     __syncwarp();
 
-    // ---- phase B: the window sums, one (IF, channel) at a time ----
+    // ---- phase B: the window sums, a group of members per union ----
     float mr = 0.f, mi = 0.f;
     unsigned todo = __ballot_sync(0xffffffffu, valid && !bad);
     const int cp = lane & 15, half = lane >> 4;
     while (todo) {
-      const int c = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int csx = __shfl_sync(0xffffffffu, sx, c);
-      const int csy = __shfl_sync(0xffffffffu, sy, c);
-      const int x0e = csx & ~1;
-      const float* cwx = sw[wib][c];
-      const float* cwy = cwx + kWX;
-      float sr = 0.f, si = 0.f;
-      if (cp < 13) {
-        const float4* row =
-            reinterpret_cast<const float4*>(p.plane + (size_t)(csy + half) * p.pitch + x0e) + cp;
-        const size_t step = (size_t)p.pitch;  // two rows, in float4
-        float a0r = 0.f, a0i = 0.f, a1r = 0.f, a1i = 0.f;
+      // anchor: the first pending pair; the union extends from its window in the
+      // direction the last pending pair's window lies
+      const int c0 = __ffs(todo) - 1, cl = 31 - __clz(todo);
+      const int ax = __shfl_sync(0xffffffffu, sx, c0), ay = __shfl_sync(0xffffffffu, sy, c0);
+      const int lx = __shfl_sync(0xffffffffu, sx, cl), ly = __shfl_sync(0xffffffffu, sy, cl);
+      const int ux = max(lx >= ax ? ax : ax - kSlack, 0);
+      const int uy = max(ly >= ay ? ay : ay - kSlack, 0);
+      const bool fits = ((todo >> lane) & 1u) && sx >= ux && sx <= ux + kSlack && sy >= uy && sy <= uy + kSlack;
+      unsigned sel = __ballot_sync(0xffffffffu, fits);
+      int mem[kGroup], dxm[kGroup], dym[kGroup];
+      int cnt = 0;
 #pragma unroll
-        for (int jj = 0; jj < 13; jj++) {
-          const int j = 2 * jj + half;
-          if (j < kGridTaps) {
-            const float4 q = __ldg(row + jj * step);
-            const float wy = cwy[j];
-            a0r = fmaf(wy, q.x, a0r);
-            a0i = fmaf(wy, q.y, a0i);
-            a1r = fmaf(wy, q.z, a1r);
-            a1i = fmaf(wy, q.w, a1i);
+      for (int k = 0; k < kGroup; k++) {
+        mem[k] = sel ? __ffs(sel) - 1 : 0;
+        if (sel) {
+          sel &= sel - 1;
+          cnt = k + 1;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kGroup; k++) {
+        dxm[k] = __shfl_sync(0xffffffffu, sx, mem[k]) - ux;
+        dym[k] = __shfl_sync(0xffffffffu, sy, mem[k]) - uy;
+        if (k < cnt) todo &= ~(1u << mem[k]);
+      }
+      const int x0e = ux & ~1;
+      const float4* base4 = reinterpret_cast<const float4*>(p.plane + (size_t)(uy + half) * p.pitch + x0e) + cp;
+      const size_t step = (size_t)p.pitch;  // two rows, in float4
+      float4 acc[kGroup];
+#pragma unroll
+      for (int k = 0; k < kGroup; k++) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+      for (int rr = 0; rr < (kUnion + 1) / 2; rr++) {
+        const int r = 2 * rr + half;
+        if (r < kUnion) {
+          const float4 q = __ldg(base4 + rr * step);
+#pragma unroll
+          for (int k = 0; k < kGroup; k++) {
+            if (k < cnt) {
+              const float w = sw[wib][mem[k]][kWX + r - dym[k] + kSlack];
+              acc[k].x = fmaf(w, q.x, acc[k].x);
+              acc[k].y = fmaf(w, q.y, acc[k].y);
+              acc[k].z = fmaf(w, q.z, acc[k].z);
+              acc[k].w = fmaf(w, q.w, acc[k].w);
+            }
           }
         }
-        const int rel = x0e + 2 * cp - csx;  // -1 .. 24
-        const float wa = cwx[rel + 1], wb = cwx[rel + 2];
-        sr = fmaf(wa, a0r, wb * a1r);
-        si = fmaf(wa, a0i, wb * a1i);
       }
+      const int cc = x0e + 2 * cp - ux;  // union column of this lane's first value: -1 .. kUnion
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-        si += __shfl_xor_sync(0xffffffffu, si, o);
-      }
-      if (lane == c) {
-        mr = sr;
-        mi = si;
+      for (int k = 0; k < kGroup; k++) {
+        if (k < cnt) {
+          const float* wxk = sw[wib][mem[k]];
+          const int i0 = cc - dxm[k] + kSlack + 1;
+          const float wa = wxk[i0], wb = wxk[i0 + 1];
+          float sr = fmaf(wa, acc[k].x, wb * acc[k].z);
+          float si = fmaf(wa, acc[k].y, wb * acc[k].w);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+            si += __shfl_xor_sync(0xffffffffu, si, o);
+          }
+          if (lane == mem[k]) {
+            mr = sr;
+            mi = si;
+          }
+        }
       }
     }
     __syncwarp();
@@ -536,7 +579,7 @@ extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGr
   }
   const size_t nh = (size_t)h.nx / 2 + 1;
   const size_t ncell = h.cell.size();
-  if ((e = cudaMalloc(&g->d_plane, sizeof(float2) * (size_t)h.ny * h.pitch)) != cudaSuccess ||
+  if ((e = cudaMalloc(&g->d_plane, sizeof(float2) * (size_t)h.rows * h.pitch)) != cudaSuccess ||
       (e = cudaMalloc(&g->d_table, sizeof(float) * h.table.size())) != cudaSuccess ||
       (e = cudaMalloc(&d_grid, sizeof(float) * (size_t)h.nx * h.ny)) != cudaSuccess ||
       (e = cudaMalloc(&d_fft, sizeof(float2) * nh * h.ny)) != cudaSuccess ||
@@ -577,7 +620,7 @@ extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGr
   pp.b3 = h.b3;
   pp.dV = h.dV;
   pp.UU = d_UU;
-  grid_plane_kernel<<<dim3((unsigned)((h.pitch + 255) / 256), (unsigned)h.ny), 256, 0, st>>>(pp);
+  grid_plane_kernel<<<dim3((unsigned)((h.pitch + 255) / 256), (unsigned)h.rows), 256, 0, st>>>(pp);
   if ((e = cudaGetLastError()) != cudaSuccess)
     return bail(OBIT_DFT_ECUDA, std::string("grid plane: ") + cudaGetErrorString(e));
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
