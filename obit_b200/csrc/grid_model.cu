@@ -51,6 +51,11 @@ struct ObitDFTGrid {
   size_t stageBytes = 0;
   float* d_fscale = nullptr;  // device copy of a host freqScale
   size_t fscaleCount = 0;
+  // apply_host: copy/compute streams of the chunked pipeline and their events
+  static constexpr int kHostStreams = 3;
+  cudaStream_t hs[kHostStreams] = {};
+  cudaEvent_t hev[kHostStreams + 1] = {};
+  bool haveStreams = false;
 };
 
 namespace {
@@ -340,23 +345,60 @@ __global__ void __launch_bounds__(kApplyWarps * 32) grid_apply_kernel(GridApplyP
         }
       }
       const int cc = x0e + 2 * cp - ux;  // union column of this lane's first value: -1 .. kUnion
+      float V[2 * kGroup];                // each member's column-weighted (re, im) of this lane
 #pragma unroll
       for (int k = 0; k < kGroup; k++) {
+        V[2 * k] = V[2 * k + 1] = 0.f;
         if (k < cnt) {
           const float* wxk = sw[wib][mem[k]];
           const int i0 = cc - dxm[k] + kSlack + 1;
           const float wa = wxk[i0], wb = wxk[i0 + 1];
-          float sr = fmaf(wa, acc[k].x, wb * acc[k].z);
-          float si = fmaf(wa, acc[k].y, wb * acc[k].w);
+          V[2 * k] = fmaf(wa, acc[k].x, wb * acc[k].z);
+          V[2 * k + 1] = fmaf(wa, acc[k].y, wb * acc[k].w);
+        }
+      }
+      int myk = -1;
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            sr += __shfl_xor_sync(0xffffffffu, sr, o);
-            si += __shfl_xor_sync(0xffffffffu, si, o);
+      for (int k = 0; k < kGroup; k++)
+        if (k < cnt && mem[k] == lane) myk = k;
+      if (cnt <= 2) {
+        // few members: one warp sum each
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          if (k < cnt) {
+            float sr = V[2 * k], si = V[2 * k + 1];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              sr += __shfl_xor_sync(0xffffffffu, sr, o);
+              si += __shfl_xor_sync(0xffffffffu, si, o);
+            }
+            if (myk == k) {
+              mr = sr;
+              mi = si;
+            }
           }
-          if (lane == mem[k]) {
-            mr = sr;
-            mi = si;
+        }
+      } else {
+        // the 16 values summed over the warp by recursive halving: after the
+        // steps of 16, 8, 4, 2 lanes each lane holds the partial sum of value
+        // lane >> 1 over 16 lanes, and the step of 1 completes it
+#pragma unroll
+        for (int m = kGroup, o = 16; m >= 1; m >>= 1, o >>= 1) {
+          const bool upper = (lane & o) != 0;
+#pragma unroll
+          for (int j = 0; j < m; j++) {
+            const float send = upper ? V[j] : V[j + m];
+            const float keep = upper ? V[j + m] : V[j];
+            V[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
           }
+        }
+        V[0] += __shfl_xor_sync(0xffffffffu, V[0], 1);
+        const int src = myk < 0 ? 0 : 4 * myk;
+        const float sr = __shfl_sync(0xffffffffu, V[0], src);
+        const float si = __shfl_sync(0xffffffffu, V[0], src + 2);
+        if (myk >= 0) {
+          mr = sr;
+          mi = si;
         }
       }
     }
@@ -530,6 +572,10 @@ void release(ObitDFTGrid* g) {
   cudaFree(g->d_table);
   cudaFree(g->d_stage);
   cudaFree(g->d_fscale);
+  if (g->haveStreams) {
+    for (cudaStream_t st : g->hs) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : g->hev) cudaEventDestroy(ev);
+  }
   delete g;
 }
 
@@ -650,7 +696,8 @@ extern "C" int obit_dft_grid_apply_host(ObitDFTGrid* g, const GPUVisInfo* visInf
   if (!visInfo) return fail(OBIT_DFT_EBADARG, "grid apply: null GPUVisInfo");
   if (nvis == 0 || g->hp.ncomp == 0) return OBIT_DFT_OK;
   CUDA_TRY(cudaSetDevice(g->device));
-  const size_t bytes = sizeof(float) * (size_t)nvis * (size_t)std::max(0, visInfo->lenvis);
+  const size_t lrec = (size_t)std::max(0, visInfo->lenvis);
+  const size_t bytes = sizeof(float) * (size_t)nvis * lrec;
   if (bytes > g->stageBytes) {
     cudaFree(g->d_stage);
     g->d_stage = nullptr;
@@ -661,13 +708,40 @@ extern "C" int obit_dft_grid_apply_host(ObitDFTGrid* g, const GPUVisInfo* visInf
   GridApplyParams q;
   int rc = apply_params(g, visInfo, opType, stokFactor, doFlip, g->d_stage, nvis, &q);
   if (rc) return rc;
+  if (!g->haveStreams) {
+    for (cudaStream_t& hs : g->hs) CUDA_TRY(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
+    for (cudaEvent_t& ev : g->hev) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    g->haveStreams = true;
+  }
   cudaStream_t st = (cudaStream_t)stream;
   rc = resolve_fscale(g, visInfo, st, &q);
   if (rc) return rc;
-  CUDA_TRY(cudaMemcpyAsync(g->d_stage, h_vis, bytes, cudaMemcpyHostToDevice, st));
-  rc = launch_apply(q, st);
-  if (rc) return rc;
-  CUDA_TRY(cudaMemcpyAsync(h_vis, g->d_stage, bytes, cudaMemcpyDeviceToHost, st));
+  // chunks of about 64 MB, round-robin over the streams: the upload of one
+  // chunk, the kernel of another and the download of a third overlap (pinned
+  // records); everything is ordered after the caller's stream and before its
+  // return
+  constexpr int S = ObitDFTGrid::kHostStreams;
+  const int per = (int)std::max<size_t>(1, std::min<size_t>((size_t)nvis, (64u << 20) / (sizeof(float) * lrec)));
+  CUDA_TRY(cudaEventRecord(g->hev[S], st));
+  for (int i = 0; i < S; i++) CUDA_TRY(cudaStreamWaitEvent(g->hs[i], g->hev[S], 0));
+  int k = 0;
+  for (int r0 = 0; r0 < nvis; r0 += per, k++) {
+    const int n = std::min(per, nvis - r0);
+    cudaStream_t cs = g->hs[k % S];
+    float* dv = g->d_stage + (size_t)r0 * lrec;
+    const size_t cb = sizeof(float) * (size_t)n * lrec;
+    CUDA_TRY(cudaMemcpyAsync(dv, h_vis + (size_t)r0 * lrec, cb, cudaMemcpyHostToDevice, cs));
+    GridApplyParams qc = q;
+    qc.vis = dv;
+    qc.nvis = n;
+    rc = launch_apply(qc, cs);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h_vis + (size_t)r0 * lrec, dv, cb, cudaMemcpyDeviceToHost, cs));
+  }
+  for (int i = 0; i < S; i++) {
+    CUDA_TRY(cudaEventRecord(g->hev[i], g->hs[i]));
+    CUDA_TRY(cudaStreamWaitEvent(st, g->hev[i], 0));
+  }
   CUDA_TRY(cudaStreamSynchronize(st));
   return OBIT_DFT_OK;
 }

@@ -14,15 +14,18 @@ from obit_b200.comps import CCField, CCModel, load_comps
 
 def field_case(N: int = 64, ncomp: int = 150, seed: int = 3, gauss=None, shift3d: bool = False,
                nchan: int = 8, nif: int = 2, nint: int = 4, reach: float = 0.8, cell_asec: float = 2.0,
-               neg_frac: float = 0.0, nstok: int = 2, flag_frac: float = 0.0):
+               neg_frac: float = 0.0, nstok: int = 2, flag_frac: float = 0.0, Ny: int | None = None,
+               rotation: float = 0.0, uv_rotation: float = 0.0):
     """Returns (CCField, GridImage, CCModel, UVData).  Components on cells
     within the central half of an N x N image of cell_asec pixels; baselines
     reach `reach` x a quarter of the grid's uv half-width.  gauss: (maj, min
-    arcsec, PA deg) of every component."""
+    arcsec, PA deg) of every component.  Ny: image rows (default N); rotation,
+    uv_rotation: the image's and the uv data's CROTA (a 3-D field)."""
     rng = np.random.default_rng(seed)
     cell = cell_asec / 3600.0
+    Ny = Ny or N
     ix = rng.integers(-N // 4, N // 4, ncomp)
-    iy = rng.integers(-N // 4, N // 4, ncomp)
+    iy = rng.integers(-Ny // 4, Ny // 4, ncomp)
     flux = rng.uniform(0.01, 1.0, ncomp).astype(np.float32)
     if neg_frac > 0:
         flux[rng.random(ncomp) < neg_frac] *= -0.1
@@ -36,11 +39,12 @@ def field_case(N: int = 64, ncomp: int = 150, seed: int = 3, gauss=None, shift3d
         parms[:, 3] = 1.0
     f = CCField(flux=flux, deltaX=(ix * cdx).astype(np.float32), deltaY=(iy * cdy).astype(np.float32),
                 crvalRA=150.0, crvalDec=45.0, do3D=shift3d, cdeltX=cdx, cdeltY=cdy, parms=parms)
-    m = CCModel(uvRA=150.0, uvDec=45.0, do3D=shift3d)
+    m = CCModel(uvRA=150.0, uvDec=45.0, do3D=shift3d, uvRotation=uv_rotation)
+    f.rotation = rotation
     if shift3d:
         f.crvalRA = 150.0 + 0.05 / math.cos(math.radians(45.0))
         f.crvalDec = 45.03
-    img = G.GridImage(N, N, N / 2 + 1, N / 2 + 1)
+    img = G.GridImage(N, Ny, N / 2 + 1, Ny / 2 + 1)
     umax = 1.0 / (cell * math.pi / 180.0) / 4.0
     freq = 1.4e9
     lam = 299792458.0 / freq

@@ -186,3 +186,36 @@ def test_vis_info_of_a_selection():
     assert (vi.chanb, vi.chane, vi.IFb, vi.IFe, vi.stokb, vi.stoke) == (2, 31, 1, 2, 1, 3)
     assert (vi.incs, vi.incf, vi.incif) == (1, 4, 160) and vi.lenvis == uv.lrec
     assert vi.freqScale == fs.ctypes.data and fs.dtype == np.float32
+
+
+def test_rotated_3d_field_equals_the_dft():
+    """A 3-D field off the phase centre with an image rotation and a uv
+    rotation: re-projection, rotated field offset and phase."""
+    f, img, m, uv = field_case(seed=14, shift3d=True, rotation=12.0, uv_rotation=-5.0)
+    e, gm = _dft_err(f, img, m, uv, exact=True)
+    assert gm.geom.do3Dmul and gm.geom.doPC
+    assert e < TOL, e
+
+
+def test_rotation_without_reprojection_equals_the_dft():
+    """A 3-D field image with a rotation while the sky model is 2-D (no
+    re-projection): u, v rotated by uv minus map rotation."""
+    f, img, m, uv = field_case(seed=15, shift3d=True, rotation=10.0)
+    m.do3D = False
+    gm = G.build(f, img, m)
+    assert gm.geom.doRot and not gm.geom.do3Dmul and gm.geom.doPC
+    # the DFT loader re-projects 3-D fields regardless of the model's flag, so
+    # compare with the oracle's own C restatement instead
+    a = G.apply_c(gm, uv, SkyModelParams(op=2))
+    b = G.apply(gm, uv, SkyModelParams(op=2))
+    va = a[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    vb = b[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    assert np.abs(va[..., :2] - vb[..., :2]).max() / _l1(f) < 2e-6
+
+
+def test_non_square_image():
+    """nx != ny: the taper's rows use nx / 2 as the reference's loop does;
+    point fields equal the DFT."""
+    f, img, m, uv = field_case(N=64, Ny=48, seed=16)
+    e, _ = _dft_err(f, img, m, uv, exact=True)
+    assert e < TOL, e

@@ -54,16 +54,21 @@ def test_plane_matches_the_oracle(gauss):
     assert err < TOL, err
 
 
-@pytest.mark.parametrize("case", ["point", "gauss", "shift3d"])
+REF_CASES = {"point": {}, "gauss": {"gauss": (6.0, 3.0, 30.0)}, "shift3d": {"shift3d": True},
+             "rot3d": {"shift3d": True, "rotation": 12.0, "uv_rotation": -5.0},
+             "nonsquare_gauss": {"Ny": 64, "gauss": (5.0, 4.0, -40.0)}}
+
+
+@pytest.mark.parametrize("case", list(REF_CASES))
 def test_reference_kernel_matches_the_oracle(case):
-    kw = {"point": {}, "gauss": {"gauss": (6.0, 3.0, 30.0)}, "shift3d": {"shift3d": True}}[case]
-    f, img, m, uv = field_case(N=96, seed=22, nint=6, **kw)
+    f, img, m, uv = field_case(N=96, seed=22, nint=6, **REF_CASES[case])
     got, info, _ = _gpu_model(f, img, m, uv)
     want = G.model_values(G.build(f, img, m), uv, SkyModelParams())
     assert not np.isnan(want).any()
     err = np.abs(got - want).max() / _l1(f)
     assert err < TOL, err
-    assert info["doPC"] == int(case == "shift3d") and info["do3Dmul"] == int(case == "shift3d")
+    off = case in ("shift3d", "rot3d")
+    assert info["doPC"] == int(off) and info["do3Dmul"] == int(off)
 
 
 @pytest.mark.parametrize("case", ["point", "shift3d", "gauss"])
