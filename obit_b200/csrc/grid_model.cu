@@ -219,7 +219,31 @@ __device__ __forceinline__ float exact_weights(float t, float* w) {
   return 1.0f;
 }
 
-__global__ void __launch_bounds__(kApplyWarps * 32) grid_apply_kernel(GridApplyParams p) {
+// Rows of a window union summed for G members: this lane's column pair of
+// rows half, half + 2, ... (the other half-warp takes the rest), each row
+// weighted by every member's row weight; members beyond G are zero.
+template <int G>
+__device__ __forceinline__ void union_rows(const float4* __restrict__ base4, size_t step, int half,
+                                           const float* swb, const int* wo, float4* acc) {
+#pragma unroll
+  for (int k = 0; k < kGroup; k++) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int rr = 0; rr < (kUnion + 1) / 2; rr++) {
+    if (2 * rr + half < kUnion) {
+      const float4 q = __ldg(base4 + rr * step);
+#pragma unroll
+      for (int k = 0; k < G; k++) {
+        const float w = swb[wo[k] + 2 * rr];
+        acc[k].x = fmaf(w, q.x, acc[k].x);
+        acc[k].y = fmaf(w, q.y, acc[k].y);
+        acc[k].z = fmaf(w, q.z, acc[k].z);
+        acc[k].w = fmaf(w, q.w, acc[k].w);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kApplyWarps * 32, 3) grid_apply_kernel(GridApplyParams p) {
   __shared__ float sw[kApplyWarps][32][kWX + kWY];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   float* mywx = sw[wib][lane];
@@ -324,26 +348,17 @@ __global__ void __launch_bounds__(kApplyWarps * 32) grid_apply_kernel(GridApplyP
       const int x0e = ux & ~1;
       const float4* base4 = reinterpret_cast<const float4*>(p.plane + (size_t)(uy + half) * p.pitch + x0e) + cp;
       const size_t step = (size_t)p.pitch;  // two rows, in float4
+      // each member's row weight of this lane's first row (slot offsets in the warp's slots)
+      const float* swb = &sw[wib][0][0];
+      int wo[kGroup];
+#pragma unroll
+      for (int k = 0; k < kGroup; k++)  // members beyond cnt read lane 0's slots (in range; unused)
+        wo[k] = k < cnt ? mem[k] * (kWX + kWY) + kWX + kSlack - dym[k] + half : kWX;
       float4 acc[kGroup];
-#pragma unroll
-      for (int k = 0; k < kGroup; k++) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
-      for (int rr = 0; rr < (kUnion + 1) / 2; rr++) {
-        const int r = 2 * rr + half;
-        if (r < kUnion) {
-          const float4 q = __ldg(base4 + rr * step);
-#pragma unroll
-          for (int k = 0; k < kGroup; k++) {
-            if (k < cnt) {
-              const float w = sw[wib][mem[k]][kWX + r - dym[k] + kSlack];
-              acc[k].x = fmaf(w, q.x, acc[k].x);
-              acc[k].y = fmaf(w, q.y, acc[k].y);
-              acc[k].z = fmaf(w, q.z, acc[k].z);
-              acc[k].w = fmaf(w, q.w, acc[k].w);
-            }
-          }
-        }
-      }
+      if (cnt <= kGroup / 2)
+        union_rows<kGroup / 2>(base4, step, half, swb, wo, acc);
+      else
+        union_rows<kGroup>(base4, step, half, swb, wo, acc);
       const int cc = x0e + 2 * cp - ux;  // union column of this lane's first value: -1 .. kUnion
       float V[2 * kGroup];                // each member's column-weighted (re, im) of this lane
 #pragma unroll
