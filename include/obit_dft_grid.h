@@ -64,6 +64,20 @@ int obit_dft_grid_create(const ObitDFTCCField *field, const ObitDFTGridImage *im
                          const ObitDFTCCModel *model, float maxGrid, int kernel, void *stream,
                          ObitDFTGrid **out);
 
+/* ObitSkyModelLoadImage (ObitSkyModel.c:2163-2260), the image model
+ * (OBIT_SkyModel_Image, which the reference always grids): a model image of
+ * image->nx x image->ny pixels (square; row-major, nx per row; host or device
+ * memory) instead of components.  Pixels below model->minFlux (or above 1e20)
+ * and blanked pixels (value fblank) are zero, the rest times model->factor
+ * (ObitFArrayClip and ObitFArrayPad); the image is centred in the grid of
+ * twice its size by pixel nx / 2, then transformed and interpolated as the
+ * component model is (no taper).  field gives the image's geometry only
+ * (crval, rotation, do3D, pixel offsets, cdelt, shifts, projection); its rows
+ * are not read.  Primary-beam correction (doPBCor) is not applied. */
+int obit_dft_grid_create_image(const float *pixels, float fblank, const ObitDFTCCField *field,
+                               const ObitDFTGridImage *image, const ObitDFTCCModel *model, int kernel,
+                               void *stream, ObitDFTGrid **out);
+
 /* ThreadSkyModelFTGrid on nvis records at d_vis (device, lenvis floats each,
  * updated in place, asynchronously on `stream`).  visInfo gives the layout and
  * selection (its freqScale, the FP32 nu / nu_uvref per (channel, IF) as

@@ -190,6 +190,9 @@ SIGNATURES = {
     "obit_dft_grid_create": (C.c_int, [C.POINTER(ObitDFTCCField), C.POINTER(ObitDFTGridImage),
                                        C.POINTER(ObitDFTCCModel), C.c_float, C.c_int, C.c_void_p,
                                        C.POINTER(C.c_void_p)]),
+    "obit_dft_grid_create_image": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(ObitDFTCCField),
+                                             C.POINTER(ObitDFTGridImage), C.POINTER(ObitDFTCCModel), C.c_int,
+                                             C.c_void_p, C.POINTER(C.c_void_p)]),
     "obit_dft_grid_apply": (C.c_int, [C.c_void_p, C.POINTER(GPUVisInfo), C.c_int, C.c_float, C.c_int,
                                       C.c_void_p, C.c_int, C.c_void_p]),
     "obit_dft_grid_apply_host": (C.c_int, [C.c_void_p, C.POINTER(GPUVisInfo), C.c_int, C.c_float, C.c_int,

@@ -62,8 +62,12 @@ void grid_kernel_table(std::vector<float>* tab) {
   }
 }
 
-int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
-                   float maxGrid, GridHostPlan* g) {
+namespace {
+
+// The plan of a field: with components (ObitSkyModelGridFTComps) or, for an
+// image model (ObitSkyModelLoadImage), everything but the gridding.
+int plan_field(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+               float maxGrid, bool withComps, GridHostPlan* g) {
   if (!field || !image || !model || !g) return fail(OBIT_DFT_EBADARG, "grid: null argument");
   const ObitDFTCCField& f = *field;
   // the conjugate columns of row 0 read columns up to 2 HWIDTH of the half plane
@@ -71,7 +75,7 @@ int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, c
     return fail(OBIT_DFT_EBADARG, "grid: image smaller than the interpolation kernel");
   if ((long long)image->nx * image->ny > (1LL << 28))
     return fail(OBIT_DFT_EBADARG, "grid: image larger than 2^28 pixels");
-  if (f.nrow < 0 || (f.nrow > 0 && (!f.flux || !f.deltaX || !f.deltaY)))
+  if (withComps && (f.nrow < 0 || (f.nrow > 0 && (!f.flux || !f.deltaX || !f.deltaY))))
     return fail(OBIT_DFT_EBADARG, "grid: missing CC columns");
   if (f.ncpProjection) return fail(OBIT_DFT_EUNSUPPORTED, "grid: -NCP fields are not supported");
   const float maprot = f.rotation, uvrot = model->uvRotation;
@@ -104,6 +108,7 @@ int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, c
   g->flux.clear();
   g->ncomp = g->bad = 0;
   std::unordered_map<long long, size_t> slot;
+  if (!withComps) last = first - 1;  // image model: no rows
   for (int j = first; j <= last; j++) {
     const size_t k = (size_t)j - 1;
     const float* pr = (f.parms && f.nparms > 0) ? f.parms + k * f.nparms : nullptr;
@@ -223,6 +228,24 @@ int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, c
     }
   }
   g->doRot = std::fabs((double)g->ssrot) > 1.0e-10 || std::fabs((double)g->ccrot - 1.0) > 1.0e-4;
+  return OBIT_DFT_OK;
+}
+
+}  // namespace
+
+int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+                   float maxGrid, GridHostPlan* g) {
+  return plan_field(field, image, model, maxGrid, true, g);
+}
+
+int grid_host_plan_image(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+                         GridHostPlan* g) {
+  if (image && image->nx != image->ny)
+    return fail(OBIT_DFT_EUNSUPPORTED, "grid: image models must be square (the reference sizes the FFT "
+                                       "output from the transposed axes)");
+  const int rc = plan_field(field, image, model, 1e20f, false, g);
+  if (rc) return rc;
+  g->ncomp = image->nx * image->ny;  // the reference always models an image field
   return OBIT_DFT_OK;
 }
 

@@ -41,4 +41,9 @@ void grid_kernel_table(std::vector<float>* tab);
 int grid_host_plan(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
                    float maxGrid, GridHostPlan* g);
 
+// The same for an image model (no components: the field's rows are not read;
+// the geometry, interpolator and table as for components; ncomp = pixels).
+int grid_host_plan_image(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+                         GridHostPlan* g);
+
 }  // namespace obit

@@ -596,27 +596,38 @@ void release(ObitDFTGrid* g) {
 
 }  // namespace
 
-extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGridImage* image,
-                                    const ObitDFTCCModel* model, float maxGrid, int kernel, void* stream,
-                                    ObitDFTGrid** out) {
-  if (!out) return fail(OBIT_DFT_EBADARG, "grid create: null output");
-  *out = nullptr;
-  if (kernel != OBIT_DFT_GRID_KERNEL_REFERENCE && kernel != OBIT_DFT_GRID_KERNEL_EXACT)
-    return fail(OBIT_DFT_EBADARG, "grid create: unknown kernel");
-  ObitDFTGrid* g = new ObitDFTGrid();
-  g->kernel = kernel;
-  int rc = obit::grid_host_plan(field, image, model, maxGrid, &g->hp);
-  if (rc) {
-    delete g;
-    return rc;
-  }
-  cudaStream_t st = (cudaStream_t)stream;
+namespace {
+
+// Pixels of an image model (ObitSkyModelLoadImage, ObitSkyModel.c:2163-2260)
+// into the zeroed, quadrant-swapped grid of twice the image: blanked pixels
+// and those below minFlux (or above 1e20) are zero (ObitFArrayClip, then the
+// blank-skipping ObitFArrayShiftAdd and ObitFArrayDeblank of ObitFArrayPad,
+// ObitFArray.c:3512-3530), the rest times factor, pixel (x, y) at grid cell
+// (x, y) + n - n/2.
+__global__ void grid_image_kernel(const float* __restrict__ pix, int n, float fblank, float minFlux,
+                                  float factor, float* __restrict__ grid) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= n) return;
+  float v = pix[(size_t)y * n + x];
+  if (v == fblank || v < minFlux || v > 1.0e20f) v = 0.0f;
+  else v = __fmul_rn(factor, v);
+  const int N = 2 * n, off = n - n / 2;
+  const int gx = (x + off + n) % N, gy = (y + off + n) % N;
+  grid[(size_t)gy * N + gx] = v;
+}
+
+// Device half of a field's set-up: the grid (component cells, or image
+// pixels when `pixels` is given), the FFT, the plane and the kernel table.
+int build_field(ObitDFTGrid* g, const float* pixels, float fblank, float minFlux, float factor,
+                cudaStream_t st) {
   const GridHostPlan& h = g->hp;
   float* d_grid = nullptr;
   float2* d_fft = nullptr;
   int* d_cell = nullptr;
   float* d_flux = nullptr;
   float* d_UU = nullptr;
+  float* d_pix = nullptr;
   cufftHandle plan = 0;
   bool havePlan = false;
   auto cleanup = [&]() {
@@ -625,42 +636,47 @@ extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGr
     cudaFree(d_cell);
     cudaFree(d_flux);
     cudaFree(d_UU);
+    cudaFree(d_pix);
     if (havePlan) cufftDestroy(plan);
   };
   auto bail = [&](int code, const std::string& msg) {
     cleanup();
-    release(g);
     return fail(code, msg);
   };
-  cudaError_t e = cudaGetDevice(&g->device);
-  if (e != cudaSuccess) return bail(OBIT_DFT_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (h.ncomp == 0) {
-    *out = g;  // nothing gridded: the reference skips the field
-    return OBIT_DFT_OK;
-  }
   const size_t nh = (size_t)h.nx / 2 + 1;
   const size_t ncell = h.cell.size();
+  const size_t npix = pixels ? (size_t)(h.nx / 2) * (h.nx / 2) : 0;
+  cudaError_t e;
   if ((e = cudaMalloc(&g->d_plane, sizeof(float2) * (size_t)h.rows * h.pitch)) != cudaSuccess ||
       (e = cudaMalloc(&g->d_table, sizeof(float) * h.table.size())) != cudaSuccess ||
       (e = cudaMalloc(&d_grid, sizeof(float) * (size_t)h.nx * h.ny)) != cudaSuccess ||
       (e = cudaMalloc(&d_fft, sizeof(float2) * nh * h.ny)) != cudaSuccess ||
-      (e = cudaMalloc(&d_cell, sizeof(int) * ncell)) != cudaSuccess ||
-      (e = cudaMalloc(&d_flux, sizeof(float) * ncell)) != cudaSuccess ||
-      (e = cudaMalloc(&d_UU, sizeof(float) * std::max<size_t>(1, h.UU.size()))) != cudaSuccess)
+      (e = cudaMalloc(&d_cell, sizeof(int) * std::max<size_t>(1, ncell))) != cudaSuccess ||
+      (e = cudaMalloc(&d_flux, sizeof(float) * std::max<size_t>(1, ncell))) != cudaSuccess ||
+      (e = cudaMalloc(&d_UU, sizeof(float) * std::max<size_t>(1, h.UU.size()))) != cudaSuccess ||
+      (pixels && (e = cudaMalloc(&d_pix, sizeof(float) * npix)) != cudaSuccess))
     return bail(OBIT_DFT_ECUDA, std::string("grid create: cudaMalloc: ") + cudaGetErrorString(e));
   if ((e = cudaMemcpyAsync(g->d_table, h.table.data(), sizeof(float) * h.table.size(), cudaMemcpyHostToDevice,
                            st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(d_cell, h.cell.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, st)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(d_flux, h.flux.data(), sizeof(float) * ncell, cudaMemcpyHostToDevice, st)) !=
-          cudaSuccess ||
+      (ncell && (e = cudaMemcpyAsync(d_cell, h.cell.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, st)) !=
+                    cudaSuccess) ||
+      (ncell && (e = cudaMemcpyAsync(d_flux, h.flux.data(), sizeof(float) * ncell, cudaMemcpyHostToDevice,
+                                     st)) != cudaSuccess) ||
       (!h.UU.empty() && (e = cudaMemcpyAsync(d_UU, h.UU.data(), sizeof(float) * h.UU.size(),
                                              cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+      (pixels && (e = cudaMemcpyAsync(d_pix, pixels, sizeof(float) * npix, cudaMemcpyDefault, st)) !=
+                     cudaSuccess) ||
       (e = cudaMemsetAsync(d_grid, 0, sizeof(float) * (size_t)h.nx * h.ny, st)) != cudaSuccess)
     return bail(OBIT_DFT_ECUDA, std::string("grid create: copy: ") + cudaGetErrorString(e));
-  grid_scatter_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(d_cell, d_flux, (int)ncell, d_grid);
+  if (pixels) {
+    const int n = h.nx / 2;
+    grid_image_kernel<<<dim3((unsigned)((n + 255) / 256), (unsigned)n), 256, 0, st>>>(d_pix, n, fblank, minFlux,
+                                                                                    factor, d_grid);
+  } else if (ncell) {
+    grid_scatter_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(d_cell, d_flux, (int)ncell, d_grid);
+  }
   if ((e = cudaGetLastError()) != cudaSuccess)
-    return bail(OBIT_DFT_ECUDA, std::string("grid scatter: ") + cudaGetErrorString(e));
+    return bail(OBIT_DFT_ECUDA, std::string("grid fill: ") + cudaGetErrorString(e));
   // ObitSkyModelFTImage: forward real-to-half-complex transform, unnormalized
   if (cufftPlan2d(&plan, h.ny, h.nx, CUFFT_R2C) != CUFFT_SUCCESS)
     return bail(OBIT_DFT_ECUDA, "grid create: cufftPlan2d failed");
@@ -687,6 +703,53 @@ extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGr
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
     return bail(OBIT_DFT_ECUDA, std::string("grid create: ") + cudaGetErrorString(e));
   cleanup();
+  return OBIT_DFT_OK;
+}
+
+int new_field(int kernel, ObitDFTGrid** out, ObitDFTGrid** g) {
+  if (!out) return fail(OBIT_DFT_EBADARG, "grid create: null output");
+  *out = nullptr;
+  if (kernel != OBIT_DFT_GRID_KERNEL_REFERENCE && kernel != OBIT_DFT_GRID_KERNEL_EXACT)
+    return fail(OBIT_DFT_EBADARG, "grid create: unknown kernel");
+  *g = new ObitDFTGrid();
+  (*g)->kernel = kernel;
+  return OBIT_DFT_OK;
+}
+
+}  // namespace
+
+extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGridImage* image,
+                                    const ObitDFTCCModel* model, float maxGrid, int kernel, void* stream,
+                                    ObitDFTGrid** out) {
+  ObitDFTGrid* g = nullptr;
+  int rc = new_field(kernel, out, &g);
+  if (rc) return rc;
+  rc = obit::grid_host_plan(field, image, model, maxGrid, &g->hp);
+  if (!rc && cudaGetDevice(&g->device) != cudaSuccess) rc = fail(OBIT_DFT_ECUDA, "grid create: no device");
+  if (!rc && g->hp.ncomp > 0)  // nothing gridded: the reference skips the field
+    rc = build_field(g, nullptr, 0.0f, 0.0f, 1.0f, (cudaStream_t)stream);
+  if (rc) {
+    release(g);
+    return rc;
+  }
+  *out = g;
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_grid_create_image(const float* pixels, float fblank, const ObitDFTCCField* field,
+                                          const ObitDFTGridImage* image, const ObitDFTCCModel* model, int kernel,
+                                          void* stream, ObitDFTGrid** out) {
+  if (!pixels) return fail(OBIT_DFT_EBADARG, "grid create: null image");
+  ObitDFTGrid* g = nullptr;
+  int rc = new_field(kernel, out, &g);
+  if (rc) return rc;
+  rc = obit::grid_host_plan_image(field, image, model, &g->hp);
+  if (!rc && cudaGetDevice(&g->device) != cudaSuccess) rc = fail(OBIT_DFT_ECUDA, "grid create: no device");
+  if (!rc) rc = build_field(g, pixels, fblank, model->minFlux, model->factor, (cudaStream_t)stream);
+  if (rc) {
+    release(g);
+    return rc;
+  }
   *out = g;
   return OBIT_DFT_OK;
 }

@@ -80,6 +80,27 @@ class GridField:
                                                   C.c_void_p(stream), C.byref(h)))
         self._h = h
 
+    @classmethod
+    def from_image(cls, pixels: np.ndarray, fblank: float, field: CCField, image: GridImage, model: CCModel,
+                   kernel: int = KERNEL_REFERENCE, stream: int = 0) -> "GridField":
+        """An image model (ObitSkyModelLoadImage): pixels (ny, nx) float32 in
+        place of components; field gives the geometry only."""
+        self = cls.__new__(cls)
+        self._lib = _lib.load()
+        keep: list = []
+        arr = _field_array([field], keep)
+        m = _model(model)
+        im = ObitDFTGridImage(image.nx, image.ny, image.crpixX, image.crpixY)
+        pix = np.ascontiguousarray(pixels, dtype=np.float32)
+        if pix.shape != (image.ny, image.nx):
+            raise ValueError("pixels must be (ny, nx)")
+        h = C.c_void_p()
+        _lib.check(self._lib.obit_dft_grid_create_image(pix.ctypes.data_as(C.c_void_p), float(fblank), arr,
+                                                        C.byref(im), C.byref(m), int(kernel), C.c_void_p(stream),
+                                                        C.byref(h)))
+        self._h = h
+        return self
+
     def info(self) -> dict:
         a = (C.c_longlong * 10)()
         _lib.check(self._lib.obit_dft_grid_info(self._h, a, 10))

@@ -130,6 +130,25 @@ def grid_comps(field, image: GridImage, factor: float = 1.0, minFlux: float = 0.
     return grid, count, gparm, bad
 
 
+def grid_image(pixels: np.ndarray, fblank: float, factor: float = 1.0, minFlux: float = 0.0) -> np.ndarray:
+    """ObitSkyModelLoadImage's grid (ObitSkyModel.c:2163-2260): ObitFArrayClip
+    (values below minFlux or above 1e20 to 0, blanks kept), then ObitFArrayPad
+    (ObitFArray.c:3512-3530: zero grid of twice the size, the image times
+    factor added with pixel n/2 on grid pixel n by the blank-skipping
+    ObitFArrayShiftAdd, then blanks to 0).  float32 (2n, 2n)."""
+    p = np.asarray(pixels, F32)
+    n = p.shape[0]
+    assert p.shape == (n, n)
+    blank = p == F32(fblank)
+    clip = (~blank) & ((p < F32(minFlux)) | (p > F32(1e20)))
+    v = np.where(clip, F32(0.0), p)
+    v = np.where(blank, F32(0.0), (F32(factor) * v).astype(F32))
+    g = np.zeros((2 * n, 2 * n), F32)
+    off = n - n // 2
+    g[off:off + n, off:off + n] = v
+    return g
+
+
 # ---- ObitSkyModelFTImage / GridFTComps ---------------------------------------
 
 
@@ -435,6 +454,14 @@ def build(field, image: GridImage, model, maxGrid: float = 1e20) -> GridModel:
     grid, ncomp, gparm, _ = grid_comps(field, image, model.factor, model.minFlux, maxGrid, model.noNeg)
     plane = ft_plane(grid, gparm, field, image)
     return GridModel(make_interp(plane, field, image), field_geometry(field, model), ncomp,
+                     float(np.abs(grid.astype(np.float64)).sum()))
+
+
+def build_image(pixels, fblank, field, image: GridImage, model) -> GridModel:
+    """ObitSkyModelLoadImage for one field: the image model's interpolator."""
+    grid = grid_image(pixels, fblank, model.factor, model.minFlux)
+    plane = ft_plane(grid, np.full(3, -1.0, F32), field, image)
+    return GridModel(make_interp(plane, field, image), field_geometry(field, model), grid.size // 4,
                      float(np.abs(grid.astype(np.float64)).sum()))
 
 

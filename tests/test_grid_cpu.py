@@ -219,3 +219,59 @@ def test_non_square_image():
     f, img, m, uv = field_case(N=64, Ny=48, seed=16)
     e, _ = _dft_err(f, img, m, uv, exact=True)
     assert e < TOL, e
+
+
+def test_mixed_mode_partition():
+    """OBIT_SkyModel_Mixed: the DFT takes the merged components above minDFT
+    (ObitSkyModel.c:1861, 1959) and the grid the rows at or below maxGrid
+    (:4421); with both at one threshold and distinct positions the two models
+    partition the field, and together equal the DFT of all (exact kernel)."""
+    from obit_b200.comps import CCModel
+    f, img, m, uv = field_case(seed=17, ncomp=120)
+    # distinct cells, so that merging cannot move flux across the threshold
+    cells = {}
+    keep = [i for i, (x, y) in enumerate(zip(f.deltaX, f.deltaY)) if cells.setdefault((x, y), i) == i]
+    f.flux, f.deltaX, f.deltaY = f.flux[keep], f.deltaX[keep], f.deltaY[keep]
+    T = 0.4
+    mdft = CCModel(**{**m.__dict__, "minDFT": T})
+    part_dft, _ = oracle.model_fp64(uv, dft_sky(f, mdft), SkyModelParams(op=OP_REPL), exact=False)
+    gm = G.build(f, img, m, maxGrid=T)
+    part_grid = G.model_values(gm, uv, SkyModelParams(), exact=True)
+    full, l1 = oracle.model_fp64(uv, dft_sky(f, m), SkyModelParams(op=OP_REPL), exact=False)
+    n_dft = int(np.sum(np.abs(f.flux) > T))
+    assert 0 < n_dft < len(f.flux) and gm.ncomp == len(f.flux) - n_dft
+    assert float(np.max(np.abs(part_dft + part_grid - full) / l1)) < TOL
+
+
+def _image_of(field, image):
+    """The image whose pixels hold the field's components (row-order sums)."""
+    n = image.nx
+    pix = np.zeros((n, n), np.float32)
+    ix = np.rint(np.asarray(field.deltaX, np.float64) / field.cdeltX).astype(int) + n // 2
+    iy = np.rint(np.asarray(field.deltaY, np.float64) / field.cdeltY).astype(int) + n // 2
+    for x, y, fl in zip(ix, iy, np.asarray(field.flux, np.float32)):
+        pix[y, x] = np.float32(pix[y, x] + fl)
+    return pix
+
+
+def test_image_model_grid_equals_the_component_grid():
+    """An image holding the components on their pixels grids to the same
+    cells as the components (ObitSkyModelLoadImage vs ObitTableCCUtilGrid)."""
+    f, img, m, uv = field_case(seed=18)
+    pix = _image_of(f, img)
+    gi = G.grid_image(pix, -12345.0)
+    gc, _, _, _ = G.grid_comps(f, img)
+    np.testing.assert_array_equal(gi, gc)
+
+
+def test_image_model_clip_blank_and_factor():
+    f, img, m, uv = field_case(N=48, seed=19)
+    pix = _image_of(f, img)
+    pix[5, 7] = -0.3   # below minFlux: zero
+    pix[9, 11] = -999.0  # blank
+    g = G.grid_image(pix, -999.0, factor=2.0, minFlux=0.0)
+    n = 48
+    off = n - n // 2
+    assert g[off + 5, off + 7] == 0.0 and g[off + 9, off + 11] == 0.0
+    keep = (pix >= 0.0) & (pix != -999.0)
+    np.testing.assert_array_equal(g[off:off + n, off:off + n][keep], (np.float32(2.0) * pix)[keep])

@@ -181,3 +181,64 @@ def test_larger_field_exact_kernel_against_the_dft():
     mod, l1 = oracle.model_fp64(sub, dft_sky(f, m), SkyModelParams(op=OP_REPL), exact=False)
     err = float(np.max(np.abs(got[idx] - mod) / l1))
     assert err < TOL, err
+
+
+def test_mixed_mode_dft_then_grid():
+    """OBIT_SkyModel_Mixed through both GPU paths: the DFT of the components
+    above minDFT subtracted, then the gridded model of the rest (maxGrid, exact
+    kernel); equals subtracting the DFT of the whole field."""
+    from helpers import run_gpu
+    from obit_b200.comps import CCModel
+    f, img, m, uv = field_case(N=96, seed=30, ncomp=200, nint=6)
+    cells = {}
+    keep = [i for i, (x, y) in enumerate(zip(f.deltaX, f.deltaY)) if cells.setdefault((x, y), i) == i]
+    f.flux, f.deltaX, f.deltaY = f.flux[keep], f.deltaX[keep], f.deltaY[keep]
+    T = 0.4
+    p = SkyModelParams(op=OP_SUB)
+    after_dft = run_gpu(uv, dft_sky(f, CCModel(**{**m.__dict__, "minDFT": T})), p, exact=False)
+    with GR.GridField(f, GR.GridImage(img.nx, img.ny, img.crpixX, img.crpixY), m, maxGrid=T,
+                      kernel=GR.KERNEL_EXACT) as gf:
+        assert 0 < gf.info()["ncomp"] < len(f.flux)
+        got = gf.FTGrid(after_dft, p).vis
+    want = oracle.apply_fp64(uv, dft_sky(f, m), p, exact=False)
+    _, l1 = oracle.model_fp64(uv, dft_sky(f, m), p, exact=False)
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+    b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+    d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1])) / l1[..., None]
+    assert float(d.max()) < TOL
+
+
+def _image_of(field, image):
+    n = image.nx
+    pix = np.zeros((n, n), np.float32)
+    ix = np.rint(np.asarray(field.deltaX, np.float64) / field.cdeltX).astype(int) + n // 2
+    iy = np.rint(np.asarray(field.deltaY, np.float64) / field.cdeltY).astype(int) + n // 2
+    for x, y, fl in zip(ix, iy, np.asarray(field.flux, np.float32)):
+        pix[y, x] = np.float32(pix[y, x] + fl)
+    return pix
+
+
+def test_image_model_matches_the_oracle_and_the_components():
+    """obit_dft_grid_create_image (ObitSkyModelLoadImage): an image holding the
+    components gives the component model's plane; a clipped, blanked, scaled
+    image matches the oracle's image model."""
+    f, img, m, uv = field_case(N=96, seed=31, nint=6, shift3d=True)
+    gimg = GR.GridImage(img.nx, img.ny, img.crpixX, img.crpixY)
+    pix = _image_of(f, img)
+    with GR.GridField(f, gimg, m) as gc, GR.GridField.from_image(pix, -999.0, f, gimg, m) as gi:
+        np.testing.assert_array_equal(gi.plane(), gc.plane())
+        assert gi.info()["ncomp"] == 96 * 96
+    pix[3, 4] = -0.5
+    pix[10, 12] = -999.0
+    pix[40:44, 50:52] = 0.7
+    from obit_b200.comps import CCModel
+    m2 = CCModel(**{**m.__dict__, "factor": 0.5, "minFlux": 0.0})
+    want_gm = G.build_image(pix, -999.0, f, img, m2)
+    p = SkyModelParams(op=OP_SUB)
+    want = G.apply(want_gm, uv, p)
+    with GR.GridField.from_image(pix, -999.0, f, gimg, m2) as gi:
+        got = gi.FTGrid(uv, p).vis
+    a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1]))
+    assert float(d.max()) / want_gm.l1 < TOL
