@@ -91,10 +91,11 @@ int obit_dft_grid_apply(ObitDFTGrid *grid, const GPUVisInfo *visInfo, int opType
                         int doFlip, float *d_vis, int nvis, void *stream);
 
 /* The same on records in host memory: h_vis (pinned, for the copies to
- * overlap) passes through a device buffer held by the field in chunks of about
- * 64 MB on three streams of the field, the upload, kernel and download of
+ * overlap) passes through three device slots of about 64 MB held by the field,
+ * in chunks on three streams of the field, the upload, kernel and download of
  * different chunks overlapping, all ordered after the work queued on `stream`;
- * returns when h_vis holds the result. */
+ * any number of records (device memory does not grow with nvis); returns when
+ * h_vis holds the result. */
 int obit_dft_grid_apply_host(ObitDFTGrid *grid, const GPUVisInfo *visInfo, int opType,
                              float stokFactor, int doFlip, float *h_vis, int nvis, void *stream);
 

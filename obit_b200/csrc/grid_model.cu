@@ -774,8 +774,15 @@ extern "C" int obit_dft_grid_apply_host(ObitDFTGrid* g, const GPUVisInfo* visInf
   if (!visInfo) return fail(OBIT_DFT_EBADARG, "grid apply: null GPUVisInfo");
   if (nvis == 0 || g->hp.ncomp == 0) return OBIT_DFT_OK;
   CUDA_TRY(cudaSetDevice(g->device));
-  const size_t lrec = (size_t)std::max(0, visInfo->lenvis);
-  const size_t bytes = sizeof(float) * (size_t)nvis * lrec;
+  const size_t lrec = (size_t)std::max(1, visInfo->lenvis);
+  // chunks of about 64 MB, round-robin over the streams, each stream reusing
+  // its own staging slot in order: the upload of one chunk, the kernel of
+  // another and the download of a third overlap (pinned records), and the
+  // device holds S chunks whatever the size of the host buffer
+  constexpr int S = ObitDFTGrid::kHostStreams;
+  const int per = (int)std::max<size_t>(1, std::min<size_t>((size_t)nvis, (64u << 20) / (sizeof(float) * lrec)));
+  const size_t slot = (size_t)per * lrec;
+  const size_t bytes = sizeof(float) * slot * (size_t)std::min(S, (nvis + per - 1) / per);
   if (bytes > g->stageBytes) {
     cudaFree(g->d_stage);
     g->d_stage = nullptr;
@@ -794,19 +801,13 @@ extern "C" int obit_dft_grid_apply_host(ObitDFTGrid* g, const GPUVisInfo* visInf
   cudaStream_t st = (cudaStream_t)stream;
   rc = resolve_fscale(g, visInfo, st, &q);
   if (rc) return rc;
-  // chunks of about 64 MB, round-robin over the streams: the upload of one
-  // chunk, the kernel of another and the download of a third overlap (pinned
-  // records); everything is ordered after the caller's stream and before its
-  // return
-  constexpr int S = ObitDFTGrid::kHostStreams;
-  const int per = (int)std::max<size_t>(1, std::min<size_t>((size_t)nvis, (64u << 20) / (sizeof(float) * lrec)));
   CUDA_TRY(cudaEventRecord(g->hev[S], st));
   for (int i = 0; i < S; i++) CUDA_TRY(cudaStreamWaitEvent(g->hs[i], g->hev[S], 0));
   int k = 0;
   for (int r0 = 0; r0 < nvis; r0 += per, k++) {
     const int n = std::min(per, nvis - r0);
     cudaStream_t cs = g->hs[k % S];
-    float* dv = g->d_stage + (size_t)r0 * lrec;
+    float* dv = g->d_stage + (size_t)(k % S) * slot;
     const size_t cb = sizeof(float) * (size_t)n * lrec;
     CUDA_TRY(cudaMemcpyAsync(dv, h_vis + (size_t)r0 * lrec, cb, cudaMemcpyHostToDevice, cs));
     GridApplyParams qc = q;
