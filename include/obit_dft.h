@@ -412,6 +412,35 @@ int obit_dft_batch_info(ObitDFTBatch *batch, long long *info, int n);
 /* Releases the batch's device memory, graph and streams. */
 int obit_dft_batch_destroy(ObitDFTBatch *batch);
 
+/* ---- records resident across CLEAN major cycles ----------------------------
+ * No counterpart in the reference, which re-reads the data and copies every
+ * buffer to the GPU and back each major cycle (ObitDConCleanVisMF.c:907,
+ * ObitGPUSkyModel.c:510-517).  The records are uploaded once; each cycle
+ * resets a device work copy to them, applies its models to that copy with the
+ * device-resident calls (obit_dft_calc_device, obit_dft_batch_run on facets
+ * pointing into it, obit_dft_grid_apply), and downloads the residual.  Device
+ * memory: twice the records. */
+typedef struct ObitDFTResident ObitDFTResident;
+
+/* Uploads nvis records of lenvis floats from h_vis (pinned for speed) on the
+ * current device; returns when they are resident. */
+int obit_dft_resident_create(const float *h_vis, int nvis, int lenvis, void *stream, ObitDFTResident **out);
+
+/* Resets the work copy to the uploaded records (device-to-device, ordered on
+ * `stream`). */
+int obit_dft_resident_reset(ObitDFTResident *r, void *stream);
+
+/* Device pointer of the work copy (nvis records), for the device-resident
+ * calls; NULL for a NULL handle. */
+float *obit_dft_resident_records(ObitDFTResident *r);
+
+/* Copies the work copy to h_out (nvis x lenvis floats) after the work queued
+ * on `stream`; returns when h_out holds it. */
+int obit_dft_resident_download(ObitDFTResident *r, float *h_out, void *stream);
+
+/* Releases the device copies. */
+int obit_dft_resident_destroy(ObitDFTResident *r);
+
 /* Reads and clears the kernels' device error flag (synchronizes the device):
  * OBIT_DFT_OK or OBIT_DFT_EKERNEL. */
 int obit_dft_check(GPUInfo *gpuInfo);

@@ -202,6 +202,12 @@ SIGNATURES = {
     "obit_dft_grid_destroy": (C.c_int, [C.c_void_p]),
     "obit_dft_choose_mode": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_int), C.c_int, C.c_longlong, C.c_int]),
+    # records resident across major cycles
+    "obit_dft_resident_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "obit_dft_resident_reset": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "obit_dft_resident_records": (C.c_void_p, [C.c_void_p]),
+    "obit_dft_resident_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "obit_dft_resident_destroy": (C.c_int, [C.c_void_p]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),

@@ -23,7 +23,8 @@ LIB = PKG / "libobit_dft.so"
 OBJ = PKG / "_build"
 
 CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "dft_beam.cu", "beam_jones.cu", "abi_layout.cu",
-              "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu", "grid_model.cu"]
+              "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu", "grid_model.cu",
+              "resident.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
 CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp", "grid_host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
