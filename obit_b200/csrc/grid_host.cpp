@@ -10,7 +10,6 @@
 
 #include <cmath>
 #include <string>
-#include <unordered_map>
 
 #include "abi_internal.h"
 #include "sky_geom.h"
@@ -104,11 +103,13 @@ int plan_field(const ObitDFTCCField* field, const ObitDFTGridImage* image, const
   last = std::min(last, f.nrow);
   g->gparm[0] = g->gparm[1] = g->gparm[2] = -1.0f;
   bool isGauss = false;
-  g->cell.clear();
-  g->flux.clear();
   g->ncomp = g->bad = 0;
-  std::unordered_map<long long, size_t> slot;
   if (!withComps) last = first - 1;  // image model: no rows
+  // The reference's row loop up to the point where each row's cell is found:
+  // the model type of the first row, one Gaussian size for all, and the stop
+  // at the first negative flux (noNeg).  The rows' cells and sums are formed
+  // on the device (grid_rows_kernel) with the constants below.
+  int stop = last;
   for (int j = first; j <= last; j++) {
     const size_t k = (size_t)j - 1;
     const float* pr = (f.parms && f.nparms > 0) ? f.parms + k * f.nparms : nullptr;
@@ -127,38 +128,27 @@ int plan_field(const ObitDFTCCField* field, const ObitDFTGridImage* image, const
     } else if (isGauss && (pr[0] != g->gparm[0] || pr[1] != g->gparm[1] || pr[2] != g->gparm[2])) {
       return fail(OBIT_DFT_EBADARG, "grid: all Gaussians of a field must have the same size");
     }
-    if (model->noNeg && f.flux[k] < 0.0f) break;
-    const float flux = f.flux[k] * model->factor;
-    float dx = f.deltaX[k] + xpoff, dy = f.deltaY[k] + ypoff;
-    if (std::fabs((double)flux) < (double)model->minFlux || flux == 0.0f) continue;
-    if (std::fabs((double)flux) > (double)maxGrid) continue;
-    const float tx = dx * iCellX, ty = dy * iCellY;
-    const int ix = tx > 0.0f ? (int)((double)tx + 0.5) : (int)((double)tx - 0.5);
-    const int iy = ty > 0.0f ? (int)((double)ty + 0.5) : (int)((double)ty - 0.5);
-    if (tx - (float)ix > 0.1f || ty - (float)iy > 0.1f) g->bad++;  // the reference's test has no abs
-    dx = std::min(maxX, std::max(dx, minX));
-    dy = std::min(maxY, std::max(dy, minY));
-    dx *= iCellX;
-    dy *= iCellY;
-    int xPix = (int)((double)(dx + (float)(nx / 2)) + 0.5);
-    int yPix = (int)((double)(dy + (float)(ny / 2)) + 0.5);
-    // the reference's clip admits one cell past the last column or row (cdelt < 0),
-    // where it would write outside its grid; such a component stays on the edge
-    xPix = std::min(std::max(xPix, 0), nx - 1);
-    yPix = std::min(std::max(yPix, 0), ny - 1);
-    // ObitFArray2DCenter's quadrant swap folded into the cell index
-    const int sx = (xPix + nx / 2) % nx, sy = (yPix + ny / 2) % ny;
-    const long long idx = (long long)sy * nx + sx;
-    auto it = slot.find(idx);
-    if (it == slot.end()) {
-      slot.emplace(idx, g->flux.size());
-      g->cell.push_back((int)idx);
-      g->flux.push_back(flux);
-    } else {
-      g->flux[it->second] = g->flux[it->second] + flux;  // row order, as the reference sums
+    if (model->noNeg && f.flux[k] < 0.0f) {
+      stop = j - 1;
+      break;
     }
-    g->ncomp++;
   }
+  GridRows& r = g->rowsDesc;
+  r.first = first - 1;
+  r.count = std::max(0, stop - first + 1);
+  r.factor = model->factor;
+  r.minFlux = model->minFlux;
+  r.maxGrid = maxGrid;
+  r.xpoff = xpoff;
+  r.ypoff = ypoff;
+  r.minX = minX;
+  r.maxX = maxX;
+  r.minY = minY;
+  r.maxY = maxY;
+  r.iCellX = iCellX;
+  r.iCellY = iCellY;
+  r.nx = nx;
+  r.ny = ny;
 
   // ---- taper constants (ObitSkyModel.c:4291-4310) ----
   g->doGaus = g->gparm[0] > 0.0f || g->gparm[1] > 0.0f;
@@ -246,6 +236,7 @@ int grid_host_plan_image(const ObitDFTCCField* field, const ObitDFTGridImage* im
   const int rc = plan_field(field, image, model, 1e20f, false, g);
   if (rc) return rc;
   g->ncomp = image->nx * image->ny;  // the reference always models an image field
+  g->rowsDesc.count = 0;
   return OBIT_DFT_OK;
 }
 

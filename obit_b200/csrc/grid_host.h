@@ -12,14 +12,24 @@ constexpr int kGridTaps = 2 * kGridHalfWidth + 1;  // taps per axis
 constexpr int kGridTableRows = 201;                // 1 + 1 / 0.005, ObitCInterpolate.c:760
 constexpr int kGridPadRows = 6;                    // zero rows after the plane (window unions)
 
+// ObitTableCCUtilGrid's per-row constants (ObitTableCCUtil.c:140-176) for the
+// device pass over a field's rows first .. first + count - 1 (0-relative, after
+// the noNeg stop).
+struct GridRows {
+  int first = 0, count = 0;
+  float factor = 1.f, minFlux = 0.f, maxGrid = 1e20f;
+  float xpoff = 0.f, ypoff = 0.f, minX = 0.f, maxX = 0.f, minY = 0.f, maxY = 0.f;
+  float iCellX = 1.f, iCellY = 1.f;
+  int nx = 0, ny = 0;
+};
+
 struct GridHostPlan {
   int nx = 0, ny = 0;        // grid: OverSample x the image
   int nxp = 0;               // plane columns: nx / 2 + 1 + HWIDTH conjugate columns
   int pitch = 0;             // complex values per plane row in device memory (even, > nxp + 6)
   int rows = 0;              // plane rows in device memory: ny, then kGridPadRows zero rows
-  std::vector<int> cell;     // distinct cells of the quadrant-swapped grid, first-touch order
-  std::vector<float> flux;   // their summed fluxes
-  int ncomp = 0, bad = 0;
+  GridRows rowsDesc;         // the component rows, gridded on the device
+  int ncomp = 0, bad = 0;    // components gridded, off-cell warnings (set by the device pass)
   float gparm[3] = {-1.f, -1.f, -1.f};
   bool doGaus = false;
   float b1 = 0.f, b2 = 0.f, b3 = 0.f, dV = 0.f;

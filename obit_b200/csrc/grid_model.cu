@@ -1,7 +1,9 @@
 // Device half of the gridded model FT (include/obit_dft_grid.h).
 //
-// Per field (obit_dft_grid_create): the distinct grid cells from the host plan
-// are stored into a zeroed, quadrant-swapped grid of nx x ny floats; cuFFT
+// Per field (obit_dft_grid_create): one thread per CC row finds its cell in the
+// zeroed, quadrant-swapped grid of nx x ny floats (grid_rows_kernel), a stable
+// radix sort by cell keeps each cell's rows in row order, and the first row of
+// each cell sums them (grid_cells_kernel), as the reference adds them; cuFFT
 // transforms it to ny rows of nx/2 + 1 complex values; one kernel then writes
 // the interpolator's plane -- rows swapped (ObitCArray2DCenter), the Gaussian
 // taper applied, HWIDTH conjugate columns in front (ObitCArrayAddConjg) -- in
@@ -26,9 +28,11 @@
 // reference's code does (no contraction), so the windows and rows are the
 // reference's.
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 #include <cufft.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <string>
 
@@ -74,10 +78,62 @@ int fail(int code, const std::string& msg) {
 
 // ---- field set-up kernels ----------------------------------------------------
 
-__global__ void grid_scatter_kernel(const int* __restrict__ cell, const float* __restrict__ flux, int n,
-                                    float* __restrict__ grid) {
+struct RowGridParams {
+  const float *flux, *dx, *dy;
+  int n;
+  obit::GridRows r;
+  int* keys;       // cell of each row in the quadrant-swapped grid, INT_MAX when the row is not gridded
+  float* vals;     // its flux times factor
+  int* counters;   // [0] rows gridded, [1] rows off a cell centre by more than 0.1
+};
+
+// ObitTableCCUtilGrid's row body (ObitTableCCUtil.c:230-290) for one row, in
+// its single-precision steps: Factor, the reference-pixel offset, the flux
+// window, the off-cell warning, the clip, the nearest cell.
+__global__ void grid_rows_kernel(RowGridParams p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) grid[cell[i]] = flux[i];  // cells are distinct: sums were formed on the host
+  if (i >= p.n) return;
+  const obit::GridRows& r = p.r;
+  const float flux = __fmul_rn(p.flux[i], r.factor);
+  float dx = __fadd_rn(p.dx[i], r.xpoff), dy = __fadd_rn(p.dy[i], r.ypoff);
+  int key = INT_MAX;
+  const double af = fabs((double)flux);
+  if (!(af < (double)r.minFlux || flux == 0.0f) && !(af > (double)r.maxGrid)) {
+    const float tx = __fmul_rn(dx, r.iCellX), ty = __fmul_rn(dy, r.iCellY);
+    const int ix = tx > 0.0f ? (int)((double)tx + 0.5) : (int)((double)tx - 0.5);
+    const int iy = ty > 0.0f ? (int)((double)ty + 0.5) : (int)((double)ty - 0.5);
+    if (__fsub_rn(tx, (float)ix) > 0.1f || __fsub_rn(ty, (float)iy) > 0.1f) atomicAdd(&p.counters[1], 1);
+    dx = dx < r.minX ? r.minX : dx;  // MIN (maxX, MAX (dx, minX))
+    dx = r.maxX < dx ? r.maxX : dx;
+    dy = dy < r.minY ? r.minY : dy;
+    dy = r.maxY < dy ? r.maxY : dy;
+    dx = __fmul_rn(dx, r.iCellX);
+    dy = __fmul_rn(dy, r.iCellY);
+    int xPix = (int)((double)__fadd_rn(dx, (float)(r.nx / 2)) + 0.5);
+    int yPix = (int)((double)__fadd_rn(dy, (float)(r.ny / 2)) + 0.5);
+    // the reference's clip admits one cell past the last column or row (cdelt < 0),
+    // where it would write outside its grid; such a component stays on the edge
+    xPix = min(max(xPix, 0), r.nx - 1);
+    yPix = min(max(yPix, 0), r.ny - 1);
+    // ObitFArray2DCenter's quadrant swap folded into the cell index
+    key = ((yPix + r.ny / 2) % r.ny) * r.nx + (xPix + r.nx / 2) % r.nx;
+    atomicAdd(&p.counters[0], 1);
+  }
+  p.keys[i] = key;
+  p.vals[i] = flux;
+}
+
+// After a stable sort by cell: the first row of each cell sums the cell's
+// fluxes in row order, as the reference adds them into its grid.
+__global__ void grid_cells_kernel(const int* __restrict__ keys, const float* __restrict__ vals, int n,
+                                  float* __restrict__ grid) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int k = keys[j];
+  if (k == INT_MAX || (j > 0 && keys[j - 1] == k)) return;
+  float s = 0.0f;
+  for (int t = j; t < n && keys[t] == k; t++) s = __fadd_rn(s, vals[t]);
+  grid[k] = s;
 }
 
 struct PlaneParams {
@@ -619,24 +675,28 @@ __global__ void grid_image_kernel(const float* __restrict__ pix, int n, float fb
 
 // Device half of a field's set-up: the grid (component cells, or image
 // pixels when `pixels` is given), the FFT, the plane and the kernel table.
-int build_field(ObitDFTGrid* g, const float* pixels, float fblank, float minFlux, float factor,
-                cudaStream_t st) {
-  const GridHostPlan& h = g->hp;
+int build_field(ObitDFTGrid* g, const ObitDFTCCField* field, const float* pixels, float fblank, float minFlux,
+                float factor, cudaStream_t st) {
+  GridHostPlan& h = g->hp;
   float* d_grid = nullptr;
   float2* d_fft = nullptr;
-  int* d_cell = nullptr;
-  float* d_flux = nullptr;
   float* d_UU = nullptr;
   float* d_pix = nullptr;
+  float* d_rows = nullptr;   // flux, dx, dy of the rows
+  int* d_keys = nullptr;     // keys in, keys out, counters
+  float* d_vals = nullptr;   // values in, values out
+  void* d_sort = nullptr;
   cufftHandle plan = 0;
   bool havePlan = false;
   auto cleanup = [&]() {
     cudaFree(d_grid);
     cudaFree(d_fft);
-    cudaFree(d_cell);
-    cudaFree(d_flux);
     cudaFree(d_UU);
     cudaFree(d_pix);
+    cudaFree(d_rows);
+    cudaFree(d_keys);
+    cudaFree(d_vals);
+    cudaFree(d_sort);
     if (havePlan) cufftDestroy(plan);
   };
   auto bail = [&](int code, const std::string& msg) {
@@ -644,39 +704,83 @@ int build_field(ObitDFTGrid* g, const float* pixels, float fblank, float minFlux
     return fail(code, msg);
   };
   const size_t nh = (size_t)h.nx / 2 + 1;
-  const size_t ncell = h.cell.size();
   const size_t npix = pixels ? (size_t)(h.nx / 2) * (h.nx / 2) : 0;
+  const int nrow = pixels ? 0 : h.rowsDesc.count;
+  size_t sortBytes = 0;
   cudaError_t e;
+  if (nrow > 0 && cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, (const int*)nullptr, (int*)nullptr,
+                                                  (const float*)nullptr, (float*)nullptr, nrow, 0, 31, st) !=
+                      cudaSuccess)
+    return bail(OBIT_DFT_ECUDA, "grid create: sort sizing failed");
   if ((e = cudaMalloc(&g->d_plane, sizeof(float2) * (size_t)h.rows * h.pitch)) != cudaSuccess ||
       (e = cudaMalloc(&g->d_table, sizeof(float) * h.table.size())) != cudaSuccess ||
       (e = cudaMalloc(&d_grid, sizeof(float) * (size_t)h.nx * h.ny)) != cudaSuccess ||
       (e = cudaMalloc(&d_fft, sizeof(float2) * nh * h.ny)) != cudaSuccess ||
-      (e = cudaMalloc(&d_cell, sizeof(int) * std::max<size_t>(1, ncell))) != cudaSuccess ||
-      (e = cudaMalloc(&d_flux, sizeof(float) * std::max<size_t>(1, ncell))) != cudaSuccess ||
       (e = cudaMalloc(&d_UU, sizeof(float) * std::max<size_t>(1, h.UU.size()))) != cudaSuccess ||
-      (pixels && (e = cudaMalloc(&d_pix, sizeof(float) * npix)) != cudaSuccess))
+      (pixels && (e = cudaMalloc(&d_pix, sizeof(float) * npix)) != cudaSuccess) ||
+      (nrow && (e = cudaMalloc(&d_rows, sizeof(float) * 3 * (size_t)nrow)) != cudaSuccess) ||
+      (nrow && (e = cudaMalloc(&d_keys, sizeof(int) * (2 * (size_t)nrow + 2))) != cudaSuccess) ||
+      (nrow && (e = cudaMalloc(&d_vals, sizeof(float) * 2 * (size_t)nrow)) != cudaSuccess) ||
+      (nrow && (e = cudaMalloc(&d_sort, std::max<size_t>(16, sortBytes))) != cudaSuccess))
     return bail(OBIT_DFT_ECUDA, std::string("grid create: cudaMalloc: ") + cudaGetErrorString(e));
+  const size_t r0 = (size_t)h.rowsDesc.first;
   if ((e = cudaMemcpyAsync(g->d_table, h.table.data(), sizeof(float) * h.table.size(), cudaMemcpyHostToDevice,
                            st)) != cudaSuccess ||
-      (ncell && (e = cudaMemcpyAsync(d_cell, h.cell.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice, st)) !=
-                    cudaSuccess) ||
-      (ncell && (e = cudaMemcpyAsync(d_flux, h.flux.data(), sizeof(float) * ncell, cudaMemcpyHostToDevice,
-                                     st)) != cudaSuccess) ||
       (!h.UU.empty() && (e = cudaMemcpyAsync(d_UU, h.UU.data(), sizeof(float) * h.UU.size(),
                                              cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
       (pixels && (e = cudaMemcpyAsync(d_pix, pixels, sizeof(float) * npix, cudaMemcpyDefault, st)) !=
                      cudaSuccess) ||
+      (nrow && (e = cudaMemcpyAsync(d_rows, field->flux + r0, sizeof(float) * nrow, cudaMemcpyDefault, st)) !=
+                   cudaSuccess) ||
+      (nrow && (e = cudaMemcpyAsync(d_rows + nrow, field->deltaX + r0, sizeof(float) * nrow, cudaMemcpyDefault,
+                                    st)) != cudaSuccess) ||
+      (nrow && (e = cudaMemcpyAsync(d_rows + 2 * (size_t)nrow, field->deltaY + r0, sizeof(float) * nrow,
+                                    cudaMemcpyDefault, st)) != cudaSuccess) ||
+      (nrow && (e = cudaMemsetAsync(d_keys + 2 * (size_t)nrow, 0, 2 * sizeof(int), st)) != cudaSuccess) ||
       (e = cudaMemsetAsync(d_grid, 0, sizeof(float) * (size_t)h.nx * h.ny, st)) != cudaSuccess)
     return bail(OBIT_DFT_ECUDA, std::string("grid create: copy: ") + cudaGetErrorString(e));
   if (pixels) {
     const int n = h.nx / 2;
     grid_image_kernel<<<dim3((unsigned)((n + 255) / 256), (unsigned)n), 256, 0, st>>>(d_pix, n, fblank, minFlux,
                                                                                     factor, d_grid);
-  } else if (ncell) {
-    grid_scatter_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(d_cell, d_flux, (int)ncell, d_grid);
+  } else if (nrow) {
+    RowGridParams rp;
+    rp.flux = d_rows;
+    rp.dx = d_rows + nrow;
+    rp.dy = d_rows + 2 * (size_t)nrow;
+    rp.n = nrow;
+    rp.r = h.rowsDesc;
+    rp.keys = d_keys;
+    rp.vals = d_vals;
+    rp.counters = d_keys + 2 * (size_t)nrow;
+    grid_rows_kernel<<<(unsigned)((nrow + 255) / 256), 256, 0, st>>>(rp);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+      return bail(OBIT_DFT_ECUDA, std::string("grid rows: ") + cudaGetErrorString(e));
+    // stable radix sort by cell: each cell's rows stay in row order
+    if (cub::DeviceRadixSort::SortPairs(d_sort, sortBytes, d_keys, d_keys + nrow, d_vals, d_vals + nrow, nrow, 0,
+                                        31, st) != cudaSuccess)
+      return bail(OBIT_DFT_ECUDA, "grid create: sort failed");
+    grid_cells_kernel<<<(unsigned)((nrow + 255) / 256), 256, 0, st>>>(d_keys + nrow, d_vals + nrow, nrow, d_grid);
   }
   if ((e = cudaGetLastError()) != cudaSuccess)
     return bail(OBIT_DFT_ECUDA, std::string("grid fill: ") + cudaGetErrorString(e));
+  if (nrow) {
+    int counters[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(counters, d_keys + 2 * (size_t)nrow, sizeof(counters), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return bail(OBIT_DFT_ECUDA, std::string("grid create: ") + cudaGetErrorString(e));
+    h.ncomp = counters[0];
+    h.bad = counters[1];
+    if (h.ncomp == 0) {  // nothing gridded: the reference skips the field
+      cleanup();
+      cudaFree(g->d_plane);
+      cudaFree(g->d_table);
+      g->d_plane = nullptr;
+      g->d_table = nullptr;
+      return OBIT_DFT_OK;
+    }
+  }
   // ObitSkyModelFTImage: forward real-to-half-complex transform, unnormalized
   if (cufftPlan2d(&plan, h.ny, h.nx, CUFFT_R2C) != CUFFT_SUCCESS)
     return bail(OBIT_DFT_ECUDA, "grid create: cufftPlan2d failed");
@@ -726,8 +830,8 @@ extern "C" int obit_dft_grid_create(const ObitDFTCCField* field, const ObitDFTGr
   if (rc) return rc;
   rc = obit::grid_host_plan(field, image, model, maxGrid, &g->hp);
   if (!rc && cudaGetDevice(&g->device) != cudaSuccess) rc = fail(OBIT_DFT_ECUDA, "grid create: no device");
-  if (!rc && g->hp.ncomp > 0)  // nothing gridded: the reference skips the field
-    rc = build_field(g, nullptr, 0.0f, 0.0f, 1.0f, (cudaStream_t)stream);
+  if (!rc && g->hp.rowsDesc.count > 0)  // no rows: nothing gridded, the reference skips the field
+    rc = build_field(g, field, nullptr, 0.0f, 0.0f, 1.0f, (cudaStream_t)stream);
   if (rc) {
     release(g);
     return rc;
@@ -745,7 +849,7 @@ extern "C" int obit_dft_grid_create_image(const float* pixels, float fblank, con
   if (rc) return rc;
   rc = obit::grid_host_plan_image(field, image, model, &g->hp);
   if (!rc && cudaGetDevice(&g->device) != cudaSuccess) rc = fail(OBIT_DFT_ECUDA, "grid create: no device");
-  if (!rc) rc = build_field(g, pixels, fblank, model->minFlux, model->factor, (cudaStream_t)stream);
+  if (!rc) rc = build_field(g, field, pixels, fblank, model->minFlux, model->factor, (cudaStream_t)stream);
   if (rc) {
     release(g);
     return rc;

@@ -268,3 +268,26 @@ def test_host_records_in_many_chunks():
     assert uv.vis.nbytes > 3 * (64 << 20)
     np.testing.assert_array_equal(host, dev)
     assert not np.array_equal(host, uv.vis)
+
+
+def test_many_rows_per_cell():
+    """A CLEAN-like table: 60,000 rows on 1,500 cells (each cell's rows spread
+    over the table), a negative row late in the table with noNeg, factor and
+    minFlux: the device pass (cells per row, stable sort by cell, row-order
+    sums) gives the oracle's grid, so the planes agree."""
+    from obit_b200.comps import CCModel
+    f, img, m, uv = field_case(N=96, seed=33, ncomp=1500, nint=2)
+    rng = np.random.default_rng(9)
+    pick = rng.integers(0, 1500, 60000)
+    f.flux = rng.uniform(-0.01, 0.2, 60000).astype(np.float32)
+    f.flux[:50000] = np.abs(f.flux[:50000])
+    f.deltaX, f.deltaY = f.deltaX[pick], f.deltaY[pick]
+    m2 = CCModel(**{**m.__dict__, "factor": 0.8, "minFlux": 0.001, "noNeg": True})
+    grid, n, gparm, bad = G.grid_comps(f, img, factor=0.8, minFlux=0.001, noNeg=True)
+    want = G.ft_plane(grid, gparm, f, img)
+    with GR.GridField(f, GR.GridImage(img.nx, img.ny, img.crpixX, img.crpixY), m2) as gf:
+        info = gf.info()
+        got = gf.plane()
+    assert info["ncomp"] == n and info["bad"] == bad and 40000 < n < 60000
+    err = np.abs(got.astype(np.complex128) - want).max() / float(np.abs(grid.astype(np.float64)).sum())
+    assert err < TOL, err
