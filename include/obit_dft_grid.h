@@ -126,6 +126,19 @@ int obit_dft_grid_destroy(ObitDFTGrid *grid);
 int obit_dft_choose_mode(int modelMode, int modelType, const int *ncc, const int *nx, const int *ny,
                          int nfield, long long nvis, int nchan);
 
+/* The same choice from this library's own rates on a B200 (no counterpart):
+ * the DFT costs ncc x nvis x nchan / dftRate seconds per field, the gridded
+ * model nvis x nchan / gridRate plus gridSetup seconds per field; returns 1
+ * (DFT) or 2 (grid) for the cheaper in total (2 for image models, 1 for point
+ * models).  A rate or set-up of 0 takes the value measured on one B200 with
+ * the default kernels: 4.5e12 component-visibility evaluations/s, 3.5e9 model
+ * visibilities/s, 0.01 s per field.  The gridded model's accuracy is the
+ * reference's table offset (see OBIT_DFT_GRID_KERNEL_REFERENCE) unless the
+ * exact kernel is used; the DFT is exact to 1e-7 of the model's L1 norm. */
+int obit_dft_choose_mode_measured(int modelType, const int *ncc, const int *nx, const int *ny, int nfield,
+                                  long long nvis, int nchan, double dftRate, double gridRate,
+                                  double gridSetup);
+
 #ifdef __cplusplus
 }
 #endif

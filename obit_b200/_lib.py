@@ -208,6 +208,9 @@ SIGNATURES = {
     "obit_dft_resident_records": (C.c_void_p, [C.c_void_p]),
     "obit_dft_resident_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "obit_dft_resident_destroy": (C.c_int, [C.c_void_p]),
+    "obit_dft_choose_mode_measured": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                                C.POINTER(C.c_int), C.c_int, C.c_longlong, C.c_int, C.c_double,
+                                                C.c_double, C.c_double]),
     "obit_dft_check": (C.c_int, [_GPUINFO_P]),
     "obit_dft_set_wait_limit": (C.c_int, [_GPUINFO_P, C.c_int]),
     "obit_dft_last_error": (C.c_char_p, []),

@@ -266,3 +266,24 @@ extern "C" int obit_dft_choose_mode(int modelMode, int modelType, const int* ncc
   if (modelType == 1) mode = 2;
   return mode;
 }
+
+extern "C" int obit_dft_choose_mode_measured(int modelType, const int* ncc, const int* nx, const int* ny,
+                                             int nfield, long long nvis, int nchan, double dftRate,
+                                             double gridRate, double gridSetup) {
+  (void)nx;
+  (void)ny;
+  if (modelType == 1) return 2;
+  if (modelType == 2) return 1;
+  if (dftRate <= 0.0) dftRate = 4.5e12;
+  if (gridRate <= 0.0) gridRate = 3.5e9;
+  if (gridSetup <= 0.0) gridSetup = 0.01;
+  double tdft = 0.0, tgrid = 0.0;
+  const double vis = (double)nvis * (double)nchan;
+  for (int i = 0; i < nfield; i++) {
+    const int n = ncc ? ncc[i] : 0;
+    if (n <= 0) continue;
+    tdft += (double)n * vis / dftRate;
+    tgrid += vis / gridRate + gridSetup;
+  }
+  return tdft <= tgrid ? 1 : 2;
+}

@@ -170,3 +170,16 @@ def choose_mode(model_mode: int, model_type: int, ncc, nx, ny, nvis: int, nchan:
     b = (C.c_int * max(1, n))(*[int(x) for x in nx])
     c = (C.c_int * max(1, n))(*[int(x) for x in ny])
     return int(lib.obit_dft_choose_mode(int(model_mode), int(model_type), a, b, c, n, int(nvis), int(nchan)))
+
+
+def choose_mode_measured(model_type: int, ncc, nx, ny, nvis: int, nchan: int, dft_rate: float = 0.0,
+                         grid_rate: float = 0.0, grid_setup: float = 0.0) -> int:
+    """MODE_DFT or MODE_GRID from this library's own rates (0: the measured
+    B200 defaults); obit_dft_choose_mode_measured."""
+    lib = _lib.load()
+    n = len(ncc)
+    a = (C.c_int * max(1, n))(*[int(x) for x in ncc])
+    b = (C.c_int * max(1, n))(*[int(x) for x in nx])
+    c = (C.c_int * max(1, n))(*[int(x) for x in ny])
+    return int(lib.obit_dft_choose_mode_measured(int(model_type), a, b, c, n, int(nvis), int(nchan),
+                                                 float(dft_rate), float(grid_rate), float(grid_setup)))

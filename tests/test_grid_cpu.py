@@ -275,3 +275,20 @@ def test_image_model_clip_blank_and_factor():
     assert g[off + 5, off + 7] == 0.0 and g[off + 9, off + 11] == 0.0
     keep = (pix >= 0.0) & (pix != -999.0)
     np.testing.assert_array_equal(g[off:off + n, off:off + n][keep], (np.float32(2.0) * pix)[keep])
+
+
+def test_choose_mode_measured_crossover():
+    """With the B200 rates the DFT stays the cheaper mode up to about
+    dftRate / gridRate components (1,300), far above the reference's
+    time model's crossover (a few components for such data)."""
+    _lib.load()
+    nvis, nchan = 2_000_000, 1024
+    assert GR.choose_mode(0, 0, [50], [4096], [4096], nvis, nchan) == 2
+    assert GR.choose_mode_measured(0, [50], [4096], [4096], nvis, nchan) == 1
+    assert GR.choose_mode_measured(0, [1000], [4096], [4096], nvis, nchan) == 1
+    assert GR.choose_mode_measured(0, [2000], [4096], [4096], nvis, nchan) == 2
+    # little data: the grid's set-up dominates and the DFT is cheaper even for many components
+    assert GR.choose_mode_measured(0, [20000], [4096], [4096], 1000, 1) == 1
+    assert GR.choose_mode_measured(1, [5], [64], [64], 10, 1) == 2
+    assert GR.choose_mode_measured(2, [5000], [64], [64], 10 ** 6, 64) == 1
+    assert GR.choose_mode_measured(0, [2000], [4096], [4096], nvis, nchan, dft_rate=1e14) == 1
