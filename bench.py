@@ -52,12 +52,16 @@ ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per
 #   config4: dft_recur_kernel<32, 0> at 23,808 records (296.35 MB read + 240.85 MB written)
 #   config5: dft_recur_batch_kernel<32, 0> over the 96-facet draw at 189,029 records
 #            (rows x 0.001; 3,668.0 MB read + 3,567.0 MB written)
+#   beam:    dft_beam_recur_kernel<PointSpec, 4> at 4,032 records (200.9 MB read + 147.5 MB written)
+#   grid:    grid_apply_kernel at 4,032 records (215.87 MB read + 144.40 MB written)
 NCU_DRAM_BYTES_PER_RECORD = {
     "config1": ((65.61e6 + 13.73e6) / 42120, "42,120-record capture (the whole configuration)"),
     "config2": ((499.44e6 + 443.81e6) / 10080, "10,080-record capture"),
     "config3": ((202.13e6 + 150.94e6) / 4032, "4,032-record capture"),
     "config4": ((296.35e6 + 240.85e6) / 23808, "23,808-record capture"),
     "config5": ((3668.0e6 + 3567.0e6) / 189029, "189,029-record capture of the same facet draw"),
+    "beam": ((200.9e6 + 147.5e6) / 4032, "4,032-record capture"),
+    "grid": ((215.87e6 + 144.40e6) / 4032, "4,032-record capture"),
 }
 
 
@@ -722,7 +726,9 @@ def run_beam(args):
                    "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024,
                    "correlations": ncorr, "l2": "inputs larger than L2", "timing": "CUDA events around all steps"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": NCU_DRAM_BYTES_PER_RECORD["beam"][0] * rows,
+                     "traffic_source": "ncu dram__bytes_read + dram__bytes_write of a " +
+                                       NCU_DRAM_BYTES_PER_RECORD["beam"][1] + ", scaled by records",
                      "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
                      "flops_per_eval": flops},
         "comparators": comp, "host": host_info(), "cpu_baseline": None, "e2e": None,
@@ -857,7 +863,10 @@ def run_grid(args):
                            "what": "components x model visibilities per second: the DFT metric for the same "
                                    "model and records (one set-up per step counted in the second figure)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                     "traffic": NCU_DRAM_BYTES_PER_RECORD["grid"][0] * rows,
+                     "traffic_source": "ncu dram__bytes_read + dram__bytes_write of a " +
+                                       NCU_DRAM_BYTES_PER_RECORD["grid"][1] + ", scaled by records",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs",
                      "note": "algorithmic bytes are the records' selected correlations read and written; the "
                              "kernel's limit is its window gathers through L1/L2 (25 rows x 13 16-byte pairs "
                              "per model visibility)",
