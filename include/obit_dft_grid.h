@@ -49,7 +49,10 @@ enum {
                                          model is the one at a point 0.005 cell
                                          (+- 0.0025) below the requested one */
   OBIT_DFT_GRID_KERNEL_EXACT = 1      /* 25-point Lagrange weights at the requested
-                                         point itself (no counterpart) */
+                                         point itself, on a window centred on it (no
+                                         counterpart); a point within 12 cells of the
+                                         plane's edge, whose window would leave the
+                                         plane, is blanked as off the plane */
 };
 
 typedef struct ObitDFTGrid ObitDFTGrid;

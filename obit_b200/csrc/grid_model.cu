@@ -361,11 +361,15 @@ __global__ void __launch_bounds__(kApplyWarps * 32, 3) grid_apply_kernel(GridApp
           const float swy = table_weights(p.table, it, k0, nt, wys);
           sumwt = swx * swy;
         } else {
-          // the requested point itself: 0-relative position px (py) on the plane
-          sx = min(max((int)floorf(px + 0.5f) - kGridHalfWidth, 0), p.nxp - kGridTaps);
-          sy = min(max((int)floorf(py + 0.5f) - kGridHalfWidth, 0), p.nyp - kGridTaps);
-          exact_weights(px - (float)sx, wxs);
-          sumwt = exact_weights(py - (float)sy, wys);
+          // the requested point itself: 0-relative position px (py) on the plane, a
+          // window centred on it; a point whose window would leave the plane is
+          // blanked as off the plane (an edge window would extrapolate)
+          sx = (int)floorf(px + 0.5f) - kGridHalfWidth;
+          sy = (int)floorf(py + 0.5f) - kGridHalfWidth;
+          if (sx >= 0 && sx + kGridTaps <= p.nxp && sy >= 0 && sy + kGridTaps <= p.nyp) {
+            exact_weights(px - (float)sx, wxs);
+            sumwt = exact_weights(py - (float)sy, wys);
+          }
         }
         bad = !(sumwt > 0.5f);
       }

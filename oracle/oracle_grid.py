@@ -294,7 +294,8 @@ def interpolate(ip: Interp, u: np.ndarray, v: np.ndarray, chunk: int = 8192, exa
     NaN where the reference returns its blank (outside the plane, or weight
     sum <= 0.5).  exact: 25-point Lagrange weights at the requested point
     itself (0-relative plane position = the reference's 1-relative pixel),
-    the window centred on it and clamped to the plane."""
+    the window centred on it; a point whose window would leave the plane is
+    blanked."""
     ny, nxp = ip.plane.shape
     ntab = ip.table.shape[0] - 1
     px = (ip.crpix[0] + (u / ip.cdelt[0]).astype(F32)).astype(F32)
@@ -308,10 +309,12 @@ def interpolate(ip: Interp, u: np.ndarray, v: np.ndarray, chunk: int = 8192, exa
         ii = idx[s:s + chunk]
         if exact:
             X, Y = px[ii].astype(np.float64), py[ii].astype(np.float64)
-            sx = np.clip(np.floor(X + 0.5).astype(np.int64) - HWIDTH, 0, nxp - IWID)
-            sy = np.clip(np.floor(Y + 0.5).astype(np.int64) - HWIDTH, 0, ny - IWID)
-            wx = lagrange_weights(X - sx)
-            wy = lagrange_weights(Y - sy)
+            sx = np.floor(px[ii].astype(np.float32) + np.float32(0.5)).astype(np.int64) - HWIDTH
+            sy = np.floor(py[ii].astype(np.float32) + np.float32(0.5)).astype(np.int64) - HWIDTH
+            fits = (sx >= 0) & (sx + IWID <= nxp) & (sy >= 0) & (sy + IWID <= ny)
+            sx, sy = np.clip(sx, 0, nxp - IWID), np.clip(sy, 0, ny - IWID)
+            wx = lagrange_weights(X - sx) * fits[:, None]
+            wy = lagrange_weights(Y - sy) * fits[:, None]
         else:
             sx, k0x, ntx, tx = conv_setup(px[ii], nxp, ntab)
             sy, k0y, nty, ty = conv_setup(py[ii], ny, ntab)

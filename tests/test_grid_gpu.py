@@ -120,13 +120,15 @@ def test_selection_leaves_the_rest_untouched():
     np.testing.assert_array_equal(got[:, :uv.nrparm], uv.vis[:, :uv.nrparm])
 
 
-def test_points_off_the_plane_are_blanked():
+@pytest.mark.parametrize("kernel", [GR.KERNEL_REFERENCE, GR.KERNEL_EXACT])
+def test_points_off_the_plane_are_blanked(kernel):
     """Baselines beyond the plane: the reference zeroes data and weight; near
-    its edge, the reference's clamped windows are followed."""
+    its edge, the reference's clamped windows (or the exact kernel's clamped,
+    centred ones) are followed."""
     f, img, m, uv = field_case(N=48, seed=26, reach=6.0, nint=8)
     p = SkyModelParams(op=OP_SUB)
-    want = G.apply(G.build(f, img, m), uv, p)
-    with GR.GridField(f, GR.GridImage(img.nx, img.ny, img.crpixX, img.crpixY), m) as gf:
+    want = G.apply(G.build(f, img, m), uv, p, exact=(kernel == GR.KERNEL_EXACT))
+    with GR.GridField(f, GR.GridImage(img.nx, img.ny, img.crpixX, img.crpixY), m, kernel=kernel) as gf:
         got = gf.FTGrid(uv, p).vis
     a = got[:, uv.nrparm:].reshape(uv.vis_view().shape)
     b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)
