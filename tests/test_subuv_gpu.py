@@ -1,0 +1,46 @@
+"""The SubUV pass structure over the GPU paths (obit_b200.subuv.sub_uv): a
+two-field model (one 2-D field at the phase centre, one 3-D field off it)
+applied by the DFT (all fields in one pass) and by the gridded model (a pass
+per field, exact kernel) gives the oracle's result; the chosen mode follows
+ObitSkyModelChose."""
+import numpy as np
+import pytest
+
+import oracle
+from grid_helpers import dft_sky, field_case
+from obit_b200 import grid as GR
+from obit_b200.comps import load_comps
+from obit_b200.skymodel import OP_SUB, SkyModelParams
+from obit_b200.subuv import sub_uv
+
+pytestmark = pytest.mark.gpu
+
+
+def test_two_fields_by_dft_and_by_grid():
+    f1, img1, m, uv = field_case(N=96, seed=50, ncomp=120, nint=5)
+    f2, img2, m3, _ = field_case(N=96, seed=51, ncomp=80, nint=5, shift3d=True)
+    m.do3D = True  # the model's flag: 3-D re-projection for the shifted field
+    fields, images = [f1, f2], [img1, img2]
+    gimages = [GR.GridImage(i.nx, i.ny, i.crpixX, i.crpixY) for i in images]
+    p = SkyModelParams(op=OP_SUB)
+    sky, _ = load_comps(fields, m)
+    want = oracle.apply_fp64(uv, sky, p, exact=False)
+    _, l1 = oracle.model_fp64(uv, sky, p, exact=False)
+    for mode, kernel in ((GR.MODE_DFT, GR.KERNEL_REFERENCE), (GR.MODE_GRID, GR.KERNEL_EXACT)):
+        r = sub_uv(uv, fields, gimages, m, p, mode=mode, kernel=kernel)
+        assert r.mode == mode
+        a = r.uv.vis[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+        b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+        d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1])) / l1[..., None]
+        assert float(d.max()) < 1e-5, (mode, float(d.max()))
+    np.testing.assert_array_equal(uv.vis, field_case(N=96, seed=50, ncomp=120, nint=5)[3].vis)
+
+
+def test_fastest_follows_the_reference_choice():
+    f1, img1, m, uv = field_case(N=64, seed=52, ncomp=200, nint=3)
+    gim = [GR.GridImage(img1.nx, img1.ny, img1.crpixX, img1.crpixY)]
+    want = GR.choose_mode(GR.MODE_FASTEST, GR.TYPE_COMPS, [200], [64], [64], uv.nvis, uv.nchan * uv.nif)
+    r = sub_uv(uv, [f1], gim, m, SkyModelParams(op=OP_SUB))
+    assert r.mode == want
+    r2 = sub_uv(uv, [f1], gim, m, SkyModelParams(op=OP_SUB), measured=True)
+    assert r2.mode == GR.MODE_DFT  # 200 components: the DFT on the B200
