@@ -29,7 +29,7 @@ def _case(seed):
     return kw, kernel, op
 
 
-@pytest.mark.parametrize("seed", range(16))
+@pytest.mark.parametrize("seed", range(32))
 def test_random_case(seed):
     kw, kernel, op = _case(seed)
     f, img, m, uv = field_case(**kw)
