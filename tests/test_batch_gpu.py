@@ -58,7 +58,10 @@ def _check_facet(uv, sky, p, got):
         # weights become weight x |M| (input weights are 1 or flagged)
         assert float(np.max(np.abs(a[..., :2, 2] - b[..., :2, 2]) / l1[..., None])) < 2 * TOL_REL
     else:
-        assert float(np.max(d / l1[..., None])) < TOL_REL
+        # the records are FP32: the result of a subtraction is rounded to the
+        # data's precision, which a heavily tapered model's L1 norm may not reach
+        ulp = 2.0 ** -22 * np.abs(b[..., 0] + 1j * b[..., 1])[..., :2]
+        assert float(np.max((d - ulp) / l1[..., None])) < TOL_REL
     assert np.array_equal(a[..., 2:, :], b[..., 2:, :])  # unselected polarizations
 
 

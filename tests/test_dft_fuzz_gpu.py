@@ -70,6 +70,9 @@ def test_random_case(seed):
         assert float(np.max(np.where(ok, rel, 0))) < TOL_REL, (mod, kw, p)
         return
     d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1]))
+    # the records are FP32: a subtraction's result is rounded to the data's
+    # precision, which a heavily tapered model's L1 norm may not reach
+    d = np.maximum(d - 2.0 ** -22 * np.abs(b[..., 0] + 1j * b[..., 1]), 0.0)
     rel = d / np.broadcast_to(np.where(sel, l1, 1.0)[..., None], d.shape)
     assert float(np.max(np.where(mask, rel, 0))) < TOL_REL, (mod, kw, p, float(np.max(rel)))
     np.testing.assert_array_equal(a[..., 2], b[..., 2])
