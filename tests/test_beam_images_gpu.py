@@ -100,3 +100,31 @@ def test_beam_dft_from_images(circular):
     for p_ in range(4):
         d = np.abs((a[..., p_, 0] - b[..., p_, 0]) + 1j * (a[..., p_, 1] - b[..., p_, 1]))
         assert np.nanmax(d / np.maximum(l1[..., model_of[p_]], 1e-30)) < TOL_REL + 1e-6
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_images(seed):
+    """Seeded random grids: antenna types, planes, image size, projection,
+    interpolation half-width, cell, parallactic angle and component positions
+    (some off the grid)."""
+    torch = pytest.importorskip("torch")
+    r = np.random.default_rng(13000 + seed)
+    ntype, nplane = int(r.integers(1, 4)), int(r.integers(1, 5))
+    n = int(r.choice([21, 40, 61]))
+    im = _images(ntype, nplane, n=n, projection=int(r.integers(0, 2)), seed=int(r.integers(0, 10 ** 6)))
+    im.hwidth = int(r.integers(1, 5))
+    im.cdelt = (float(r.uniform(0.02, 0.08)), float(r.uniform(0.02, 0.08)))
+    ncomp = int(r.integers(1, 400))
+    half = 0.5 * n * max(im.cdelt)
+    pos = r.uniform(-1.2 * half, 1.2 * half, (ncomp, 2)).astype(np.float32)
+    par = float(r.uniform(-1.5, 1.5))
+    d_px = torch.from_numpy(im.pixels).cuda()
+    d_pos = torch.from_numpy(pos).cuda()
+    d_j = torch.zeros((ntype, ncomp, nplane, 8), dtype=torch.float32, device="cuda")
+    jones_from_images(im, d_px.data_ptr(), d_pos.data_ptr(), ncomp, par, d_j.data_ptr())
+    torch.cuda.synchronize()
+    got = d_j.cpu().numpy()
+    want = oracle.beam_jones_fp64(im, pos, par)
+    unit = np.array([1, 0, 0, 0, 0, 0, 1, 0], np.float32)
+    np.testing.assert_array_equal(np.all(got == unit, axis=-1), np.all(want == unit, axis=-1))
+    assert np.max(np.abs(got - want)) < 2e-5
