@@ -694,6 +694,7 @@ def run_beam(args):
     ncorr = 4
     flops = 6.0 + 8.0 * ncorr
     run = lambda: gm.calc_device(d_vis.data_ptr(), rows, sp)  # noqa: E731
+    form = gm.beam_info()
     with torch.cuda.stream(stream):
         sampler = ClockSampler(0)
         for _ in range(args.warmup):
@@ -704,13 +705,18 @@ def run_beam(args):
             t_ms, launch_ms = _timed_on(torch, stream, run, args.steps, 0, gm.check)
         comp = None
         if not args.no_compare:
-            gm.set_kernel(_lib.OBIT_DFT_PLAIN)
-            gm.set_beam(beam, d_jones.data_ptr())
-            pt_ms, _ = _timed_on(torch, stream, run, 1, 1, gm.check)
-            pl = evals / (pt_ms * 1e-3) / 1e9
-            comp = {"per_channel_form_gevals_s": pl, "recur_vs_per_channel": evals * args.steps / (t_ms * 1e-3) / 1e9 / pl,
-                    "what": "the beam kernel's per-channel form (one thread per record and channel, FP64 "
-                            "phase, one sin/cos per component-visibility), same records, 1 launch"}
+            rate = evals * args.steps / (t_ms * 1e-3) / 1e9
+            comp = {}
+            for name, flavor, what in (
+                    ("block_form", _lib.OBIT_DFT_RECUR_CHAIN,
+                     "8-channel blocks on the FP32 pipe (packed complex multiply-accumulate per correlation)"),
+                    ("per_channel_form", _lib.OBIT_DFT_PLAIN,
+                     "one thread per record and channel, FP64 phase, one sin/cos per component-visibility")):
+                gm.set_kernel(flavor)
+                gm.set_beam(beam, d_jones.data_ptr())
+                c_ms, _ = _timed_on(torch, stream, run, 1, 1, gm.check)
+                cr = evals / (c_ms * 1e-3) / 1e9
+                comp[name] = {"gevals_s": cr, "speedup": rate / cr, "what": what + "; same records, 1 launch"}
     value = evals * args.steps / (t_ms * 1e-3)
     peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
     achieved = evals * flops / (statistics.mean(launch_ms) * 1e-3) / 1e12
@@ -724,7 +730,9 @@ def run_beam(args):
                                f"correlations, {sky.ncomp} point components with spectral index, "
                                f"{ntype} antenna types, {njc} Jones planes, Stokes I sky",
                    "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024,
-                   "correlations": ncorr, "l2": "inputs larger than L2", "timing": "CUDA events around all steps"},
+                   "correlations": ncorr, "l2": "inputs larger than L2", "timing": "CUDA events around all steps",
+                   "beam_form": {0: "blocks, FP32 pipe", 1: "tensor-core (mma.sync TF32, 3-product split)",
+                                 2: "per channel"}[form["form"]], "components_per_tile": form["ct"]},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": NCU_DRAM_BYTES_PER_RECORD["beam"][0] * rows,
                      "traffic_source": "ncu dram__bytes_read + dram__bytes_write of a " +

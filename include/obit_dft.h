@@ -222,6 +222,15 @@ typedef struct ObitDFTBeam {
 } ObitDFTBeam;
 int obit_dft_set_beam(GPUInfo *gpuInfo, const ObitDFTBeam *beam);
 
+/* The beam kernel the next call will use (building the plan if needed):
+ * info[0] = form (0: blocks of at most 8 channels on the FP32 pipe, 1: the
+ * tensor-core form -- point families on uniformly spaced channels with the
+ * default flavor; OBIT_DFT_RECUR_CHAIN keeps the block form -- 2: one thread
+ * per channel, OBIT_DFT_PLAIN), info[1] = components per tile, info[2] =
+ * channel runs (form 1) or blocks per record (forms 0 and 2).  Writes
+ * min(n, 3) entries; OBIT_DFT_EBADARG when no beam is set. */
+int obit_dft_beam_info(GPUInfo *gpuInfo, int *info, int n);
+
 /* Beam images from which the Jones table is interpolated: for every antenna
  * type the 8 images of GetJonesKernel's interpolators
  * (ObitCUDABeamModel.cu:1228-1299): P1 re, P1 im, P2 re, P2 im, X1 re, X1 im,

@@ -160,6 +160,7 @@ SIGNATURES = {
     "obit_dft_set_tile": (C.c_int, [_GPUINFO_P, C.c_int, C.c_int]),
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),
     "obit_dft_plan_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
+    "obit_dft_beam_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
     "obit_dft_calc_noalloc": (C.c_int, [C.POINTER(GPUVisInfo), C.POINTER(GPUModelInfo),
                                         C.POINTER(C.c_double), C.c_double, C.c_double,
                                         C.POINTER(C.c_double), C.c_int, C.c_void_p, C.c_int,

@@ -22,7 +22,7 @@ INCLUDE = ROOT / "include"
 LIB = PKG / "libobit_dft.so"
 OBJ = PKG / "_build"
 
-CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "dft_beam.cu", "beam_jones.cu", "abi_layout.cu",
+CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "dft_beam.cu", "dft_beam_mma.cu", "beam_jones.cu", "abi_layout.cu",
               "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu", "grid_model.cu",
               "resident.cu"]
 C_SOURCES = ["gpu_skymodel.c"]

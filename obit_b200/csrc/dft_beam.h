@@ -13,6 +13,27 @@ namespace obit {
 // Channels per block of the beam recurrence kernel.
 constexpr int kBeamK = 8;
 
+// Tensor-core form: records per CTA item (one per warp), channels per matrix
+// tile (the 16 rows of an m16n8k8 product) and tiles per run.
+constexpr int kBeamMmaWarps = 8;
+constexpr int kBeamMmaRows = 16;
+constexpr int kBeamMmaTiles = 16;
+constexpr int kBeamMmaMaxChan = kBeamMmaRows * kBeamMmaTiles;
+
+// A run of uniformly spaced channels of one IF within one Jones plane (at most
+// kBeamMmaMaxChan): channel k has frequency ratio f0 + k df (df: increment
+// class dfc of KParams), table index ifq0 + k kincf and record offset
+// off0 + k incf.
+struct BeamSeg {
+  float f0_hi, f0_lo;
+  int dfc;
+  int off0;
+  int ifq0;
+  int nch;
+  int jplane;
+  int pad;
+};
+
 struct BeamKParams {
   // Records, layout, channel blocks (at most kBeamK channels, never spanning a
   // change of Jones plane), tile shape R x Bt, component table and tile ct,
@@ -36,6 +57,17 @@ struct BeamKParams {
   int circular;                  // 1: circular feeds (RR, LL, RL, LR), 0: linear
   float c2p, s2p;                // cos, sin of twice the parallactic angle (linear Q, U)
   int flavor;                    // kFlavorRecur (blocks) or kFlavorPlain (one thread per channel)
+  // tensor-core form (point families on uniformly spaced channels): runs of
+  // channels, their count, and 1 to launch it instead of the block form
+  const BeamSeg* segs;
+  int nseg;
+  int mma;
+  // coefficient fragments of the tensor-core form, written by its prologue:
+  // [plane][type pair][component group of 4][column 8][component in group 4]
+  // float4 {b0 hi, b1 hi, b0 lo, b1 lo}; ncompPad components per (plane, pair),
+  // a multiple of the component tile, zero past the model
+  float4* coefTab;
+  int ncompPad;
 };
 
 // Correlation slots the recurrence kernel accumulates: XX and YY, or all four.
@@ -50,5 +82,16 @@ int beam_fit_tile(BeamKParams* p, std::string* err);
 
 // One launch over all records of kp (stream-ordered, asynchronous).
 int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);
+
+// Tensor-core form.  Whether the model family has it; the bytes of its
+// coefficient-fragment table (p.ncompPad set); the dynamic shared memory of a
+// launch with component tile p.k.ct; the largest tile (<= 64, a multiple of 4)
+// that fits one CTA per SM, set in p->k.ct (0 when none fits: the caller keeps
+// the block form); the launch (the fragment prologue, then the kernel).
+bool beam_mma_supported(int mode);
+size_t beam_mma_coef_bytes(const BeamKParams& p);
+size_t beam_mma_smem_bytes(const BeamKParams& p);
+int beam_mma_fit_tile(BeamKParams* p);
+int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err);
 
 }  // namespace obit

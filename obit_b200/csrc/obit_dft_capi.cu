@@ -53,16 +53,55 @@ struct BeamState {
   double* d_lnspec = nullptr;
   int* d_plane = nullptr;
   BlockDesc* d_blocks = nullptr;  // channel blocks of the beam plan
+  BeamSeg* d_segs = nullptr;      // channel runs of the tensor-core form
+  float4* d_coef = nullptr;       // its coefficient fragments (written per launch)
   BeamKParams kp{};
 };
 
 void free_beam_tables(BeamState& b) {
-  for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane, (void*)b.d_blocks})
+  for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane, (void*)b.d_blocks, (void*)b.d_segs,
+                  (void*)b.d_coef})
     if (q) cudaFree(q);
+  b.d_coef = nullptr;
   b.d_fscale = nullptr;
   b.d_lnspec = nullptr;
   b.d_plane = nullptr;
   b.d_blocks = nullptr;
+  b.d_segs = nullptr;
+}
+
+// Runs of the tensor-core beam form from a plan of kBeamMmaRows-channel
+// blocks: consecutive full blocks of one IF, one channel-increment class and
+// one Jones plane, at most kBeamMmaMaxChan channels each.
+std::vector<BeamSeg> beam_segments(const Plan& plan, const LayoutDesc& L, const std::vector<int>& jchan) {
+  std::vector<BeamSeg> segs;
+  const std::vector<BlockDesc>& bl = plan.blocks;
+  for (size_t i = 0; i < bl.size(); i++) {
+    const BlockDesc& b = bl[i];
+    const int jp = jchan[b.ifq0];
+    bool extend = false;
+    if (!segs.empty()) {
+      const BeamSeg& sg = segs.back();
+      const BlockDesc& pb = bl[i - 1];
+      extend = pb.len == kBeamMmaRows && sg.nch % kBeamMmaRows == 0 && sg.nch + b.len <= kBeamMmaMaxChan &&
+               b.ifq0 == pb.ifq0 + kBeamMmaRows * L.kincf && b.off0 == pb.off0 + kBeamMmaRows * L.incf &&
+               b.dfc == sg.dfc && jp == sg.jplane;
+    }
+    if (extend) {
+      segs.back().nch += b.len;
+    } else {
+      BeamSeg sg{};
+      sg.f0_hi = b.f0_hi;
+      sg.f0_lo = b.f0_lo;
+      sg.dfc = b.dfc;
+      sg.off0 = b.off0;
+      sg.ifq0 = b.ifq0;
+      sg.nch = b.len;
+      sg.jplane = jp;
+      segs.push_back(sg);
+    }
+  }
+  return segs;
 }
 
 struct State {
@@ -288,27 +327,62 @@ int ensure_plan(GPUInfo* g, State* s) {
     if ((int)L.specIndex.size() >= nfreq &&
         (rc = upload(L.specIndex.data(), sizeof(int) * nfreq, (void**)&b.d_plane)))
       return rc;
-    // channel blocks of at most kBeamK channels that never span a change of
-    // Jones plane (recurrence form), from the same planner
+    // Channel blocks that never span a change of Jones plane, from the same
+    // planner: 16-channel blocks joined into runs for the tensor-core form
+    // (point families on uniformly spaced channels, runs of 4 channels or more
+    // on average), else blocks of at most kBeamK channels for the block form.
     LayoutDesc LB = L;
     LB.blockKey = b.jchan;
     TuneDesc TB;
     TB.flavor = kFlavorRecur;
-    TB.K = kBeamK;
     TB.threads = kThreads;
     TB.specFactor = 0;
-    Plan bplan;
-    rc = plan_layout(LB, s->mc.model, A, TB, &bplan, &err);
-    if (rc) return fail(rc, err);
-    const int nb = (int)bplan.blocks.size();
-    CUDA_TRY(cudaMalloc(&b.d_blocks, sizeof(BlockDesc) * (size_t)std::max(1, nb)));
-    if (nb)
-      CUDA_TRY(cudaMemcpy(b.d_blocks, bplan.blocks.data(), sizeof(BlockDesc) * (size_t)nb,
-                          cudaMemcpyHostToDevice));
+    Plan mplan, bplan;
+    std::vector<BeamSeg> segs;
+    bool mma = false;
+    if (s->tune.flavor == kFlavorRecur && s->tune.specFactor && beam_mma_supported(s->mc.model.kind)) {
+      TB.K = kBeamMmaRows;
+      rc = plan_layout(LB, s->mc.model, A, TB, &mplan, &err);
+      if (rc) return fail(rc, err);
+      if (mplan.linear) {
+        segs = beam_segments(mplan, L, b.jchan);
+        long long nch = 0;
+        for (const BeamSeg& sg : segs) nch += sg.nch;
+        mma = !segs.empty() && nch >= 4LL * (long long)segs.size();
+      }
+      if (mma) {  // the tile must fit shared memory with this many antenna types
+        BeamKParams trial{};
+        trial.k = mplan.kp;
+        trial.mode = s->mc.model.kind;
+        trial.numAntType = b.numAntType;
+        mma = beam_mma_fit_tile(&trial) > 0;
+      }
+    }
+    if (!mma) {
+      TB.K = kBeamK;
+      rc = plan_layout(LB, s->mc.model, A, TB, &bplan, &err);
+      if (rc) return fail(rc, err);
+    }
+    const Plan& used = mma ? mplan : bplan;
     BeamKParams& k = b.kp;
     k = BeamKParams{};
-    k.k = bplan.kp;
-    k.k.blocks = b.d_blocks;
+    k.k = used.kp;
+    if (mma) {
+      CUDA_TRY(cudaMalloc(&b.d_segs, sizeof(BeamSeg) * segs.size()));
+      CUDA_TRY(cudaMemcpy(b.d_segs, segs.data(), sizeof(BeamSeg) * segs.size(), cudaMemcpyHostToDevice));
+      k.segs = b.d_segs;
+      k.nseg = (int)segs.size();
+      k.mma = 1;
+      k.k.blocks = nullptr;
+      k.k.R = kBeamMmaWarps;
+    } else {
+      const int nb = (int)bplan.blocks.size();
+      CUDA_TRY(cudaMalloc(&b.d_blocks, sizeof(BlockDesc) * (size_t)std::max(1, nb)));
+      if (nb)
+        CUDA_TRY(cudaMemcpy(b.d_blocks, bplan.blocks.data(), sizeof(BlockDesc) * (size_t)nb,
+                            cudaMemcpyHostToDevice));
+      k.k.blocks = b.d_blocks;
+    }
     k.k.comps = s->d_comps;
     k.k.ncomp = s->mc.model.ncomp;
     k.k.errFlag = s->d_err;
@@ -346,7 +420,14 @@ int ensure_plan(GPUInfo* g, State* s) {
     k.c2p = b.c2p;
     k.s2p = b.s2p;
     k.flavor = (s->tune.flavor == kFlavorPlain) ? kFlavorPlain : kFlavorRecur;
-    if ((rc = beam_fit_tile(&k, &err))) return fail(rc, err);
+    if (k.mma) {
+      beam_mma_fit_tile(&k);
+      k.ncompPad = (k.k.ncomp + k.k.ct - 1) / k.k.ct * k.k.ct;
+      CUDA_TRY(cudaMalloc(&b.d_coef, std::max<size_t>(16, beam_mma_coef_bytes(k))));
+      k.coefTab = b.d_coef;
+    } else if ((rc = beam_fit_tile(&k, &err))) {
+      return fail(rc, err);
+    }
   }
   s->planValid = true;
   return OBIT_DFT_OK;
@@ -633,6 +714,21 @@ int obit_dft_plan_info(GPUInfo* g, int* info, int n) {
                      pl.kp.nblocks, pl.kp.ndf, pl.specFactored ? 1 : 0, pl.mixed ? 1 : 0,
                      pl.mixed ? pl.model.ncompPt : 0};
   for (int i = 0; i < n && i < 11; i++) info[i] = v[i];
+  return OBIT_DFT_OK;
+}
+
+int obit_dft_beam_info(GPUInfo* g, int* info, int n) {
+  set_last_error("");
+  State* s;
+  int rc = ensure_state(g, &s);
+  if (rc) return rc;
+  if (!info || n < 1) return fail(OBIT_DFT_EBADARG, "beam info needs an output array");
+  if (!s->beam.on) return fail(OBIT_DFT_EBADARG, "no beam is set");
+  rc = ensure_plan(g, s);
+  if (rc) return rc;
+  const BeamKParams& k = s->beam.kp;
+  const int v[3] = {k.mma ? 1 : (k.flavor == kFlavorPlain ? 2 : 0), k.k.ct, k.mma ? k.nseg : k.k.nblocks};
+  for (int i = 0; i < n && i < 3; i++) info[i] = v[i];
   return OBIT_DFT_OK;
 }
 

@@ -192,6 +192,14 @@ class GPUSkyModel:
                 "ncompPoint")
         return dict(zip(keys, list(arr)))
 
+    def beam_info(self) -> dict:
+        """The beam kernel the next call uses: form 0 (blocks on the FP32
+        pipe), 1 (tensor-core form) or 2 (one thread per channel), components
+        per tile, channel runs or blocks per record."""
+        arr = (C.c_int * 3)()
+        _lib.check(self._lib.obit_dft_beam_info(self.gpuinfo, arr, 3))
+        return dict(zip(("form", "ct", "units"), list(arr)))
+
     def calc_device(self, d_vis_ptr: int, nvis: int, stream_ptr: int = 0) -> None:
         """Apply the model to nvis records already in device memory (async)."""
         _lib.check(self._lib.obit_dft_calc_device(self.gpuinfo, C.c_void_p(d_vis_ptr), nvis,

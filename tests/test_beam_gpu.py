@@ -3,7 +3,9 @@ oracle: random Jones matrices per antenna type, component and Jones plane,
 2 or 4 correlations, subtract / replace / divide with flags, every model
 family, Stokes I, Q, U and V skies; unit Jones matrices reproduce the plain
 sky model; a record whose antennas fall outside the table is reported and
-left untouched."""
+left untouched.  Point families on uniformly spaced channels run the
+tensor-core form by default and the FP32 block form under
+OBIT_DFT_RECUR_CHAIN: both are checked."""
 import numpy as np
 import pytest
 
@@ -17,7 +19,10 @@ from test_beam_oracle_cpu import beam_case
 pytestmark = pytest.mark.gpu
 
 
-def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None):
+FORMS = [_lib.OBIT_DFT_RECUR, _lib.OBIT_DFT_RECUR_CHAIN]
+
+
+def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None, info=None):
     out = uv.copy()
     d_jones = torch.from_numpy(np.ascontiguousarray(jones if jones is not None else beam.jones)).cuda()
     gm = GPUSkyModel("beam")
@@ -27,6 +32,8 @@ def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None):
             gm.set_kernel(flavor)
         gm.set_beam(beam, d_jones.data_ptr())
         gm.DFTSetMod(sky)
+        if info is not None:
+            info.update(gm.beam_info())
         gm.DFTCalc(out)
         gm.DFTShutdown()
     finally:
@@ -55,9 +62,10 @@ def _check(uv, got, want, l1, op):
             assert np.nanmax(d / np.maximum(L, 1e-30)) < TOL_REL + 1e-6
 
 
+@pytest.mark.parametrize("flavor", FORMS)
 @pytest.mark.parametrize("nstok", [2, 4])
 @pytest.mark.parametrize("op", [OP_SUB, OP_REPL, OP_DIV])
-def test_beam_matches_oracle(op, nstok):
+def test_beam_matches_oracle(op, nstok, flavor):
     torch = pytest.importorskip("torch")
     uv, sky, beam = beam_case(nstok=nstok, nrow=70, nchan=24, nif=2, ncomp=150, seed=3 + op,
                               flag_frac=0.1)
@@ -66,18 +74,24 @@ def test_beam_matches_oracle(op, nstok):
         c[..., 0] = 1.0
         c[..., 1] = 0.0
     p = SkyModelParams(op=op)
-    got = _run_beam(uv, sky, p, beam, torch)
+    info = {}
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor, info=info)
+    assert info["form"] == (1 if flavor == _lib.OBIT_DFT_RECUR else 0)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, op)
 
 
+@pytest.mark.parametrize("flavor", FORMS)
 @pytest.mark.parametrize("mt", [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC, U.MOD_GAUSS,
                                 U.MOD_GAUSS_SPEC, U.MOD_GAUSS_TSPEC])
-def test_beam_every_family(mt):
+def test_beam_every_family(mt, flavor):
     torch = pytest.importorskip("torch")
     uv, sky, beam = beam_case(mt=mt, nstok=4, nrow=40, nchan=20, nif=2, ncomp=90, seed=11 + mt)
     p = SkyModelParams(op=OP_SUB)
-    got = _run_beam(uv, sky, p, beam, torch)
+    info = {}
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor, info=info)
+    point = mt in (U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC)
+    assert info["form"] == (1 if point and flavor == _lib.OBIT_DFT_RECUR else 0)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
 
@@ -140,24 +154,25 @@ def test_beam_nonuniform_channels_take_the_direct_form():
     _check(uv, got, want, l1, OP_SUB)
 
 
+@pytest.mark.parametrize("flavor", FORMS)
 @pytest.mark.parametrize("stok", [2, 3, 4])
-def test_beam_polarized_skies(stok):
+def test_beam_polarized_skies(stok, flavor):
     """Stokes Q, U (with a parallactic angle) and V skies."""
     torch = pytest.importorskip("torch")
     uv, sky, beam = beam_case(nstok=4, nrow=50, nchan=20, nif=2, ncomp=110, seed=23 + stok, flag_frac=0.1,
                               stok=stok, par_ang=0.61)
     p = SkyModelParams(op=OP_SUB)
-    got = _run_beam(uv, sky, p, beam, torch)
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
 
 
-@pytest.mark.parametrize("flavor", [_lib.OBIT_DFT_RECUR, _lib.OBIT_DFT_PLAIN])
+@pytest.mark.parametrize("flavor", FORMS + [_lib.OBIT_DFT_PLAIN])
 @pytest.mark.parametrize("mt", [U.MOD_POINT_SPEC, U.MOD_GAUSS_TSPEC])
 def test_beam_jones_planes_inside_blocks(flavor, mt):
     """Seven Jones planes over 2 x 27 channels: plane changes fall inside the
-    recurrence form's 8-channel blocks, which the planner cuts there; the
-    recurrence form and the per-channel comparator both match the oracle."""
+    block form's 8-channel blocks and the tensor-core form's 16-channel
+    tiles, which the planner cuts there; every form matches the oracle."""
     torch = pytest.importorskip("torch")
     uv, sky, beam = beam_case(mt=mt, nstok=4, nrow=45, nchan=27, nif=2, ncomp=140, seed=41, njc=7,
                               flag_frac=0.1)
@@ -184,8 +199,9 @@ def test_beam_selection_and_one_correlation():
     assert np.max(d / np.maximum(l1[:, 1:3, 3:22, 0], 1e-30)) < TOL_REL + 1e-6
 
 
+@pytest.mark.parametrize("flavor", FORMS)
 @pytest.mark.parametrize("stok", [1, 2, 3, 4])
-def test_beam_circular_feeds(stok):
+def test_beam_circular_feeds(stok, flavor):
     """Circular feeds (records RR, LL, RL, LR; Jones matrices in the R, L basis),
     Stokes I, Q, U and V skies: the model J1 M J2^H of the CPU path's circular
     branch."""
@@ -193,6 +209,42 @@ def test_beam_circular_feeds(stok):
     uv, sky, beam = beam_case(nstok=4, nrow=45, nchan=20, nif=2, ncomp=110, seed=51 + stok, flag_frac=0.1,
                               stok=stok, circular=True)
     p = SkyModelParams(op=OP_SUB)
-    got = _run_beam(uv, sky, p, beam, torch)
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
+
+
+@pytest.mark.parametrize("mt", [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC])
+@pytest.mark.parametrize("nstok", [1, 2, 4])
+def test_beam_tensor_form_long_runs(mt, nstok):
+    """The tensor-core form over runs longer than one 256-channel run (300
+    channels: a full run and a 44-channel run ending in a partial tile), three
+    antenna types, five Jones planes and enough components for several
+    64-component tiles with a ragged last one."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(mt=mt, nstok=nstok, nrow=37, nchan=300, nif=2, ncomp=333, seed=61 + mt,
+                              ntype=3, njc=5, flag_frac=0.1)
+    p = SkyModelParams(op=OP_SUB)
+    info = {}
+    got = _run_beam(uv, sky, p, beam, torch, info=info)
+    assert info["form"] == 1 and info["units"] >= 2 * 2
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
+
+
+def test_beam_form_choice():
+    """Irregular channels and single-channel selections keep the block form."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(nstok=4, nrow=20, nchan=24, nif=2, ncomp=40, seed=71)
+    rng = np.random.default_rng(5)
+    uv2 = uv.copy()
+    uv2.freqArr = np.sort(uv2.freqArr + rng.uniform(-3e5, 3e5, uv2.freqArr.shape))
+    info = {}
+    _run_beam(uv2, sky, SkyModelParams(op=OP_SUB), beam, torch, info=info)
+    assert info["form"] == 0
+    info = {}
+    _run_beam(uv, sky, SkyModelParams(op=OP_SUB, startChannel=5, numberChannel=1), beam, torch, info=info)
+    assert info["form"] == 0
+    info = {}
+    _run_beam(uv, sky, SkyModelParams(op=OP_SUB), beam, torch, flavor=_lib.OBIT_DFT_PLAIN, info=info)
+    assert info["form"] == 2
