@@ -68,6 +68,11 @@ struct BeamKParams {
   // a multiple of the component tile, zero past the model
   float4* coefTab;
   int ncompPad;
+  // spectral amplitudes of the tensor-core form (point families with a
+  // spectrum), written by its prologue: [run][component group of 4][matrix
+  // tile 16][lane group 8][component in group 4] float2 {A(16 m + g),
+  // A(16 m + g + 8)}, zero past the run and the model
+  float2* ampTab;
 };
 
 // Correlation slots the recurrence kernel accumulates: XX and YY, or all four.
@@ -84,12 +89,14 @@ int beam_fit_tile(BeamKParams* p, std::string* err);
 int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);
 
 // Tensor-core form.  Whether the model family has it; the bytes of its
-// coefficient-fragment table (p.ncompPad set); the dynamic shared memory of a
+// coefficient-fragment and amplitude tables (p.ncompPad, p.nseg set; no
+// amplitude table for point models); the dynamic shared memory of a
 // launch with component tile p.k.ct; the largest tile (<= 64, a multiple of 4)
 // that fits one CTA per SM, set in p->k.ct (0 when none fits: the caller keeps
-// the block form); the launch (the fragment prologue, then the kernel).
+// the block form); the launch (the prologue kernels, then the kernel).
 bool beam_mma_supported(int mode);
 size_t beam_mma_coef_bytes(const BeamKParams& p);
+size_t beam_mma_amp_bytes(const BeamKParams& p);
 size_t beam_mma_smem_bytes(const BeamKParams& p);
 int beam_mma_fit_tile(BeamKParams* p);
 int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err);

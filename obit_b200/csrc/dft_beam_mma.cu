@@ -26,14 +26,15 @@
 // performance", 2022): the dropped lo lo term and the truncation of lo are
 // below 2^-20 of each term.
 //
-// Per launch, a prologue kernel forms the coefficient fragments of every
-// (Jones plane, antenna-type pair, component), split, in the lanes' order.
-// Per component tile (ct components and the fragments of the run's plane for
-// every type pair, staged by bulk copies on one mbarrier):
+// Per launch, prologue kernels form the coefficient fragments of every
+// (Jones plane, antenna-type pair, component), split, and the spectral
+// amplitudes of every (run, component, channel), both in the order the lanes
+// read them.  Per component tile (ct components, the fragments of the run's
+// plane for every type pair and the run's amplitudes, staged by bulk copies on
+// one mbarrier):
 //   (record, component)        phase turns P (split-FP32) and the step of one
 //                              matrix tile s16 = exp(2 pi i P 16 df) (accurate
 //                              sin/cos);
-//   (component, channel)       spectral amplitudes, shared by the CTA's records;
 //   (record, component, lane)  anchors at channels g and g + 8 (MUFU sin/cos of
 //                              the range-reduced split-FP32 phase), then per
 //                              matrix tile of the run the amplitude, the split,
@@ -56,10 +57,9 @@ constexpr int kMmaThreads = kBeamMmaWarps * 32;
 // Matrix tiles per branch-free group of the run (their three dependent
 // products per tile interleave); runs are padded to a multiple of it.
 constexpr int kMmaChunk = 4;
-// float2 entries per component row of the amplitude table: one (g, g + 8)
-// pair per lane group and matrix tile, padded by 4 entries so that the rows
-// of a warp's four components start 8 banks apart
-constexpr int kAmpStride = kBeamMmaTiles * 8 + 4;
+// float2 entries of one component group of the amplitude table: one
+// (g, g + 8) channel pair per matrix tile, lane group and component
+constexpr int kAmpGroup = kBeamMmaTiles * 32;
 // float2 entries per component of the (record, component) tables: padded so
 // that a warp's four components fall in different banks
 constexpr int kPStride = kBeamMmaWarps + 1;
@@ -67,7 +67,7 @@ constexpr int kCmpSlots = kBeamMmaTiles * 2;  // packed compensation terms per t
 
 // Shared-memory layout of one CTA (offsets in floats, each a multiple of 4).
 struct MmaLayout {
-  int comp, coef, pp, ss, amp, lsp, pl, cmp, uvw, pair, total;
+  int comp, coef, pp, ss, amp, cmp, uvw, pair, total;
 };
 
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
@@ -84,11 +84,7 @@ __host__ __device__ inline MmaLayout mma_layout(int ct, int cstride, int npair, 
   L.ss = o;
   o += pad4(ct * kPStride * 2);
   L.amp = o;
-  o += table ? ct * kAmpStride * 2 : 0;
-  L.lsp = o;
-  o += table ? kBeamMmaMaxChan : 0;
-  L.pl = o;
-  o += table ? kBeamMmaMaxChan : 0;
+  o += table ? (ct / 4) * kAmpGroup * 2 : 0;
   L.cmp = o;
   o += kMmaThreads * kCmpSlots * 2;
   L.uvw = o;
@@ -167,24 +163,83 @@ __global__ void __launch_bounds__(256) beam_coef_kernel(const __grid_constant__ 
   }
 }
 
+// Prologue of point families with a spectrum: the amplitude A exp(sum_t a_t
+// L^(t+1)) (PointSpec; L the log-frequency term of the channel) or
+// A_plane exp(alpha L) (PointTSpec) of every (run, component, channel), as the
+// per-channel form computes it, in the lanes' order (BeamKParams.ampTab).
+template <int MODE>
+__global__ void __launch_bounds__(256) beam_amp_kernel(const __grid_constant__ BeamKParams bp) {
+  using F = Fields<MODE>;
+  const KParams& p = bp.k;
+  const long long n = (long long)bp.nseg * (bp.ncompPad / 4) * kAmpGroup;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i & 3);
+    const int g = (int)((i >> 2) & 7);
+    const int m = (int)((i >> 5) & (kBeamMmaTiles - 1));
+    const long long r = i / kAmpGroup;
+    const int cg = (int)(r % (bp.ncompPad / 4));
+    const int sg = (int)(r / (bp.ncompPad / 4));
+    const int c = 4 * cg + t;
+    const BeamSeg seg = bp.segs[sg];
+    float a[2] = {0.f, 0.f};
+    if (c < p.ncomp) {
+      const float* cp = p.comps + (size_t)c * p.cstride;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int k = m * kBeamMmaRows + g + 8 * h;
+        if (k < seg.nch) {
+          const int ifq = seg.ifq0 + k * bp.kincf;
+          const double L = bp.lnspec ? bp.lnspec[ifq] : 0.0;
+          double e = 0.0;
+          float A;
+          if constexpr (F::kTSpec) {
+            A = cp[F::kTabOff + (bp.plane ? bp.plane[ifq] : 0)];
+            e = (double)cp[F::kAlphaOff] * L;
+          } else {
+            A = cp[0];
+            double pw = L;
+            for (int tt = 0; tt < p.nterm && tt < kMaxNTerm; tt++) {
+              e += (double)cp[F::kSpecOff + tt] * pw;
+              pw *= L;
+            }
+          }
+          a[h] = A * expf((float)e);
+        }
+      }
+    }
+    bp.ampTab[i] = make_float2(a[0], a[1]);
+  }
+}
+
 // Stage component tile c0 and its coefficient fragments at plane jp (one
 // slice per type pair) by bulk copies on one mbarrier, with the bounded waits
 // of stage_comps.  Bulk copies need 16-byte aligned addresses and sizes:
 // cstride is a multiple of 4 floats, a slice ct * 128 bytes, the tables
 // cudaMalloc'd.
-__device__ __forceinline__ bool stage_tile(const BeamKParams& bp, float* sComp, float4* sCoef, int c0,
-                                           int jp, int npair, uint64_t* bar, uint32_t& phase) {
+template <bool kAmp>
+__device__ __forceinline__ bool stage_tile(const BeamKParams& bp, float* sComp, float4* sCoef, float2* sAmp,
+                                           int c0, int sg, int jp, int npair, uint64_t* bar, uint32_t& phase) {
   const KParams& p = bp.k;
   const int ct = p.ct;
   const int nc = min(ct, p.ncomp - c0);
   const uint32_t cbytes = (uint32_t)nc * p.cstride * 4u;
   const uint32_t fbytes = (uint32_t)ct * 128u;
+  const uint32_t abytes = kAmp ? (uint32_t)(ct / 4) * kAmpGroup * 8u : 0u;
   const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(bar);
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_s),
-                 "r"(cbytes + (uint32_t)npair * fbytes)
+                 "r"(cbytes + (uint32_t)npair * fbytes + abytes)
                  : "memory");
+    if (kAmp) {
+      const float2* src = bp.ampTab + ((size_t)sg * (bp.ncompPad / 4) + c0 / 4) * kAmpGroup;
+      asm volatile(
+          "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              (uint32_t)__cvta_generic_to_shared(sAmp)),
+          "l"(src), "r"(abytes), "r"(bar_s)
+          : "memory");
+    }
     asm volatile(
         "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
             (uint32_t)__cvta_generic_to_shared(sComp)),
@@ -241,8 +296,6 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
   float2* sP = reinterpret_cast<float2*>(smem + lay.pp);
   float2* sS = reinterpret_cast<float2*>(smem + lay.ss);
   float2* sAmp = reinterpret_cast<float2*>(smem + lay.amp);
-  float* sL = smem + lay.lsp;
-  int* sPl = reinterpret_cast<int*>(smem + lay.pl);
   f2x* sCmp = reinterpret_cast<f2x*>(smem + lay.cmp);
   float* sUVW = smem + lay.uvw;
   int* sPair = reinterpret_cast<int*>(smem + lay.pair);
@@ -255,7 +308,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
   const int nItems = ((p.nvis + kBeamMmaWarps - 1) / kBeamMmaWarps) * bp.nseg;
   for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
     const int rt = item / bp.nseg;
-    const BeamSeg seg = bp.segs[item - rt * bp.nseg];
+    const int sg = item - rt * bp.nseg;
+    const BeamSeg seg = bp.segs[sg];
     const int row0 = rt * kBeamMmaWarps;
     const int nb = (seg.nch + kBeamMmaRows - 1) / kBeamMmaRows;
     __syncthreads();  // the previous item is done with shared memory
@@ -277,13 +331,6 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
       }
       sPair[threadIdx.x] = pr;
     }
-    if constexpr (F::kTable) {  // log-frequency term (and plane) of the run's channels
-      for (int k = threadIdx.x; k < seg.nch; k += kMmaThreads) {
-        const int ifq = seg.ifq0 + k * bp.kincf;
-        sL[k] = bp.lnspec ? (float)bp.lnspec[ifq] : 0.f;
-        if constexpr (F::kTSpec) sPl[k] = bp.plane ? bp.plane[ifq] : 0;
-      }
-    }
     __syncthreads();
     const int row = row0 + warp;
     const int pr = sPair[warp];
@@ -294,15 +341,13 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
     const ds fa = ds_add(f0, ds_mul(ds{(float)g, 0.f}, dfd));
     const ds fb = ds_add(f0, ds_mul(ds{(float)(g + 8), 0.f}, dfd));
     const ds d16 = {16.f * dfd.hi, 16.f * dfd.lo};
-    // amplitude rows: the run's matrix tiles rounded up to whole groups
-    const int nrow = ((nb + kMmaChunk - 1) / kMmaChunk) * kMmaChunk * kBeamMmaRows;
     f2x tot[kBeamMmaTiles][2];
 #pragma unroll
     for (int m = 0; m < kBeamMmaTiles; m++) tot[m][0] = tot[m][1] = 0ull;
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // the previous tile's readers are done with shared memory
-      if (!stage_tile(bp, sComp, sCoef, c0, seg.jplane, npair, &bar, phase)) return;
+      if (!stage_tile<F::kTable>(bp, sComp, sCoef, sAmp, c0, sg, seg.jplane, npair, &bar, phase)) return;
       const int nc = min(ct, p.ncomp - c0);
       // (record, component): phase turns and the step of one matrix tile
       for (int idx = threadIdx.x; idx < kBeamMmaWarps * ct; idx += kMmaThreads) {
@@ -314,40 +359,6 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
         sP[c * kPStride + r] = make_float2(P.hi, P.lo);
         const ds ts = ds_mul(P, d16);
         sS[c * kPStride + r] = phasor_accurate(ds{__fsub_rn(ts.hi, rintf(ts.hi)), ts.lo});
-      }
-      if constexpr (F::kTable) {
-        // (component, channel): spectral amplitudes; entry (c, tile m, lane
-        // group gg) holds channels 16 m + gg and 16 m + gg + 8 (zero past the run)
-        float* ampF = reinterpret_cast<float*>(sAmp);
-        for (int c = warp; c < ct; c += kBeamMmaWarps) {
-          const float* cp = sComp + c * p.cstride;
-          float A = cp[0], al = 0.f;
-          float sc[kMaxNTerm];
-          if constexpr (F::kTSpec) {
-            al = cp[F::kAlphaOff];
-          } else {
-#pragma unroll
-            for (int tt = 0; tt < kMaxNTerm; tt++) sc[tt] = (tt < p.nterm) ? cp[F::kSpecOff + tt] : 0.f;
-          }
-          for (int k = lane; k < nrow; k += 32) {
-            float a = 0.f;
-            if (k < seg.nch) {
-              const float L = sL[k];
-              float e;
-              if constexpr (F::kTSpec) {
-                A = cp[F::kTabOff + sPl[k]];
-                e = al * L;
-              } else {  // sum_t a_t L^(t+1)
-                e = sc[kMaxNTerm - 1];
-#pragma unroll
-                for (int tt = kMaxNTerm - 2; tt >= 0; tt--) e = __fmaf_rn(e, L, sc[tt]);
-                e *= L;
-              }
-              a = A * exp_fast(e);
-            }
-            ampF[(c * kAmpStride + (k >> 4) * 8 + (k & 7)) * 2 + ((k >> 3) & 1)] = a;
-          }
-        }
       }
       __syncthreads();
 
@@ -375,7 +386,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
           }
           f2x ZR = pk2(za.x, zb.x), ZI = pk2(za.y, zb.y);
           const f2x SR = pk2(st.x, st.x), SI = pk2(st.y, st.y), NSI = pk2(-st.y, -st.y);
-          const float2* ap = sAmp + (size_t)c * kAmpStride + g;
+          const float2* ap = sAmp + (size_t)j * kAmpGroup + lane;
 #pragma unroll
           for (int mc = 0; mc < kBeamMmaTiles; mc += kMmaChunk) {
             if (mc < nb) {
@@ -384,7 +395,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
                 const int m = mc + i;
                 f2x VR = ZR, VI = ZI;
                 if constexpr (F::kTable) {
-                  const float2 a = ap[m * 8];
+                  const float2 a = ap[m * 32];
                   const f2x AP = pk2(a.x, a.y);
                   VR = mul2(ZR, AP);
                   VI = mul2(ZI, AP);
@@ -477,6 +488,11 @@ size_t beam_mma_coef_bytes(const BeamKParams& p) {
   return (size_t)p.numJChan * p.numAntType * p.numAntType * (size_t)p.ncompPad * 8 * sizeof(float4);
 }
 
+size_t beam_mma_amp_bytes(const BeamKParams& p) {
+  if (p.mode != kPointSpec && p.mode != kPointTSpec) return 0;
+  return (size_t)p.nseg * (size_t)(p.ncompPad / 4) * kAmpGroup * sizeof(float2);
+}
+
 size_t beam_mma_smem_bytes(const BeamKParams& p) {
   const bool table = p.mode == kPointSpec || p.mode == kPointTSpec;
   const int npair = p.numAntType * p.numAntType;
@@ -533,9 +549,23 @@ int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err
     *err = std::string("tensor-core beam kernel cannot be resident: ") + cudaGetErrorString(ce);
     return 2;
   }
-  if (!kp.coefTab || kp.ncompPad < k.ncomp || kp.ncompPad % k.ct) {
-    *err = "tensor-core beam launch without its coefficient table";
+  const bool table = kp.mode == kPointSpec || kp.mode == kPointTSpec;
+  if (!kp.coefTab || kp.ncompPad < k.ncomp || kp.ncompPad % k.ct || (table && !kp.ampTab)) {
+    *err = "tensor-core beam launch without its tables";
     return 3;
+  }
+  if (table) {  // prologue: spectral amplitudes of every (run, component, channel)
+    const long long n = (long long)kp.nseg * (kp.ncompPad / 4) * kAmpGroup;
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
+    if (kp.mode == kPointSpec)
+      beam_amp_kernel<kPointSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+    else
+      beam_amp_kernel<kPointTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) {
+      *err = std::string("beam amplitude kernel launch: ") + cudaGetErrorString(ce);
+      return 2;
+    }
   }
   {  // prologue: coefficient fragments of every (plane, type pair, component)
     const long long n = (long long)kp.numJChan * kp.numAntType * kp.numAntType * kp.ncompPad;

@@ -55,14 +55,16 @@ struct BeamState {
   BlockDesc* d_blocks = nullptr;  // channel blocks of the beam plan
   BeamSeg* d_segs = nullptr;      // channel runs of the tensor-core form
   float4* d_coef = nullptr;       // its coefficient fragments (written per launch)
+  float2* d_amp = nullptr;        // its spectral amplitudes (written per launch)
   BeamKParams kp{};
 };
 
 void free_beam_tables(BeamState& b) {
   for (void* q : {(void*)b.d_fscale, (void*)b.d_lnspec, (void*)b.d_plane, (void*)b.d_blocks, (void*)b.d_segs,
-                  (void*)b.d_coef})
+                  (void*)b.d_coef, (void*)b.d_amp})
     if (q) cudaFree(q);
   b.d_coef = nullptr;
+  b.d_amp = nullptr;
   b.d_fscale = nullptr;
   b.d_lnspec = nullptr;
   b.d_plane = nullptr;
@@ -350,12 +352,19 @@ int ensure_plan(GPUInfo* g, State* s) {
         for (const BeamSeg& sg : segs) nch += sg.nch;
         mma = !segs.empty() && nch >= 4LL * (long long)segs.size();
       }
-      if (mma) {  // the tile must fit shared memory with this many antenna types
+      if (mma) {  // the tile must fit shared memory with this many antenna types, and
+                  // the per-launch tables stay within 4 GiB
         BeamKParams trial{};
         trial.k = mplan.kp;
         trial.mode = s->mc.model.kind;
         trial.numAntType = b.numAntType;
+        trial.numJChan = b.numJChan;
+        trial.nseg = (int)segs.size();
         mma = beam_mma_fit_tile(&trial) > 0;
+        if (mma) {
+          trial.ncompPad = (trial.k.ncomp + trial.k.ct - 1) / trial.k.ct * trial.k.ct;
+          mma = beam_mma_coef_bytes(trial) + beam_mma_amp_bytes(trial) <= (size_t(4) << 30);
+        }
       }
     }
     if (!mma) {
@@ -425,6 +434,10 @@ int ensure_plan(GPUInfo* g, State* s) {
       k.ncompPad = (k.k.ncomp + k.k.ct - 1) / k.k.ct * k.k.ct;
       CUDA_TRY(cudaMalloc(&b.d_coef, std::max<size_t>(16, beam_mma_coef_bytes(k))));
       k.coefTab = b.d_coef;
+      if (const size_t ab = beam_mma_amp_bytes(k)) {
+        CUDA_TRY(cudaMalloc(&b.d_amp, ab));
+        k.ampTab = b.d_amp;
+      }
     } else if ((rc = beam_fit_tile(&k, &err))) {
       return fail(rc, err);
     }
