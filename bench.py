@@ -60,7 +60,7 @@ NCU_DRAM_BYTES_PER_RECORD = {
     "config3": ((202.13e6 + 150.94e6) / 4032, "4,032-record capture"),
     "config4": ((296.35e6 + 240.85e6) / 23808, "23,808-record capture"),
     "config5": ((3668.0e6 + 3567.0e6) / 189029, "189,029-record capture of the same facet draw"),
-    "beam": ((200.9e6 + 147.5e6) / 4032, "4,032-record capture"),
+    "beam": ((232.3e6 + 147.8e6) / 4032, "4,032-record capture of the tensor-core form"),
     "grid": ((215.87e6 + 144.40e6) / 4032, "4,032-record capture"),
 }
 
@@ -738,9 +738,17 @@ def run_beam(args):
                      "traffic_source": "ncu dram__bytes_read + dram__bytes_write of a " +
                                        NCU_DRAM_BYTES_PER_RECORD["beam"][1] + ", scaled by records",
                      "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off (best of 5)",
-                     "flops_per_eval": flops},
+                     "flops_per_eval": flops,
+                     "note": "algorithmic FP32 work of the model (complex rotate + one complex multiply-"
+                             "accumulate per correlation); the tensor-core form executes the multiply-"
+                             "accumulates as TF32 products (tensor_executed)"},
+        "tensor_executed": ({"tf32_tflops": evals * 96.0 / (statistics.mean(launch_ms) * 1e-3) / 1e12,
+                             "flops_per_eval": 96.0, "what": "3 mma.sync m16n8k8 TF32 products per 64 evaluations "
+                             "(3-product split); ncu puts the pipe at 41 % of its peak on the 4,032-record case"}
+                            if form["form"] == 1 else None),
         "comparators": comp, "host": host_info(), "cpu_baseline": None, "e2e": None,
-        "gpu_launches": args.steps, "clocks": sampler.summary(),
+        # the tensor-core form runs its coefficient and amplitude prologues before the kernel
+        "gpu_launches": args.steps * (3 if form["form"] == 1 else 1), "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)
     gm.DFTShutdown()
