@@ -91,6 +91,9 @@ def parse():
                     help="config2: one chunk of the 64-antenna dataset (default); config5: the "
                          "96-facet uneven batch; beam: the beam-corrected DFT on the config-2 "
                          "layout; grid: the gridded model FT on the config-2 layout")
+    ap.add_argument("--beam-model", default="pointspec", choices=["pointspec", "gaussspec"],
+                    help="beam workload: points with a spectral index (default) or Gaussians (1-60 arcsec) "
+                         "with one")
     ap.add_argument("--grid-kernel", default="reference", choices=["reference", "exact"],
                     help="grid: interpolation weights (the reference's table or exact Lagrange)")
     ap.add_argument("--e2e-row-scale", type=float, default=0.002,
@@ -670,7 +673,8 @@ def run_beam(args):
     freq = 1.4e9
     fa = U.freq_axis(256, 4, freq - 512e6, 1e6)
     uvw = _track(64, 36e3, 2000, freq, 2, rows, 0)
-    sky = U.make_comps(U.MOD_POINT_SPEC, args.ncomp or 4000, np.random.default_rng(4), radius_deg=1.0,
+    mtype = U.MOD_GAUSS_SPEC if args.beam_model == "gaussspec" else U.MOD_POINT_SPEC
+    sky = U.make_comps(mtype, args.ncomp or 4000, np.random.default_rng(4), radius_deg=1.0,
                        nterm=1, ref_freq=freq)
     d_vis = build_vis(torch, uvw, 4, 256, 4, device, seed=100)
     d_vis[:, 3] = torch.from_numpy(baseline_codes(64, rows)).to(device)
@@ -718,6 +722,36 @@ def run_beam(args):
                 cr = evals / (c_ms * 1e-3) / 1e9
                 comp[name] = {"gevals_s": cr, "speedup": rate / cr, "what": what + "; same records, 1 launch"}
     value = evals * args.steps / (t_ms * 1e-3)
+    # e2e: the same records from a pinned host buffer through obit_dft_calc
+    # (H2D, the beam kernels and D2H inside each synchronous call)
+    e2e = None
+    if not args.no_e2e:
+        host = d_vis.cpu()
+        # the descriptor holds all the records, so the wrapper's pinned buffer
+        # (nVisPIO records, capped at the descriptor's count) takes the chunk
+        uve = U.UVData(host.numpy(), 4, 256, 4, freq, fa)
+        ge = GPUSkyModel("beam-e2e")
+        ge.DFTInit(sky, uve, SkyModelParams(nVisPIO=rows, numberPoln=2))
+        ge.set_beam(beam, d_jones.data_ptr())
+        ge.DFTSetMod(sky)
+        gi = ge.gpuinfo
+        if gi.contents.bufferSize < rows * lrec:
+            raise RuntimeError("the pinned record buffer is smaller than the chunk")
+        C.memmove(gi.contents.h_data, host.data_ptr(), rows * lrec * 4)
+        gi.contents.nvis = rows
+        gi.contents.h_visInfo.contents.nvis = rows
+        _lib.check(ge._lib.obit_dft_calc(gi))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            _lib.check(ge._lib.obit_dft_calc(gi))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        e2e = {"value": evals * args.steps / dt / 1e9, "unit": "Gevals/s",
+               "h2d_bytes_per_step": rows * lrec * 4, "d2h_bytes_per_step": rows * lrec * 4,
+               "timing": "wall clock around the synchronous C-ABI call"}
+        ge.DFTShutdown()
+        ge.close()
     peak = float("nan") if args.no_peak else fp32_peak_tflops(torch, device)
     achieved = evals * flops / (statistics.mean(launch_ms) * 1e-3) / 1e12
     line = {
@@ -727,7 +761,9 @@ def run_beam(args):
         "data": "synthetic (seeded uvw, noise visibilities, random components and Jones matrices)",
         "accuracy": {**ACCURACY, "checked_by": "tests/test_beam_gpu.py (-m gpu)"},
         "config": {"workload": f"beam: {rows} records (64 antennas, 2016 baselines) x 4 IF x 256 ch x 4 "
-                               f"correlations, {sky.ncomp} point components with spectral index, "
+                               f"correlations, {sky.ncomp} "
+                               f"{'Gaussian' if mtype == U.MOD_GAUSS_SPEC else 'point'} components with "
+                               f"spectral index, "
                                f"{ntype} antenna types, {njc} Jones planes, Stokes I sky",
                    "rows_per_step": rows, "components": int(sky.ncomp), "channels": 1024,
                    "correlations": ncorr, "l2": "inputs larger than L2", "timing": "CUDA events around all steps",
@@ -746,7 +782,7 @@ def run_beam(args):
                              "flops_per_eval": 96.0, "what": "3 mma.sync m16n8k8 TF32 products per 64 evaluations "
                              "(3-product split); ncu puts the pipe at 41 % of its peak on the 4,032-record case"}
                             if form["form"] == 1 else None),
-        "comparators": comp, "host": host_info(), "cpu_baseline": None, "e2e": None,
+        "comparators": comp, "host": host_info(), "cpu_baseline": None, "e2e": e2e,
         # the tensor-core form runs its coefficient and amplitude prologues before the kernel
         "gpu_launches": args.steps * (3 if form["form"] == 1 else 1), "clocks": sampler.summary(),
     }

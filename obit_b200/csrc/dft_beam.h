@@ -57,7 +57,7 @@ struct BeamKParams {
   int circular;                  // 1: circular feeds (RR, LL, RL, LR), 0: linear
   float c2p, s2p;                // cos, sin of twice the parallactic angle (linear Q, U)
   int flavor;                    // kFlavorRecur (blocks) or kFlavorPlain (one thread per channel)
-  // tensor-core form (point families on uniformly spaced channels): runs of
+  // tensor-core form (uniformly spaced channels): runs of
   // channels, their count, and 1 to launch it instead of the block form
   const BeamSeg* segs;
   int nseg;
@@ -68,8 +68,8 @@ struct BeamKParams {
   // a multiple of the component tile, zero past the model
   float4* coefTab;
   int ncompPad;
-  // spectral amplitudes of the tensor-core form (point families with a
-  // spectrum), written by its prologue: [run][component group of 4][matrix
+  // spectral amplitudes of the tensor-core form (families with a spectrum),
+  // written by its prologue: [run][component group of 4][matrix
   // tile 16][lane group 8][component in group 4] float2 {A(16 m + g),
   // A(16 m + g + 8)}, zero past the run and the model
   float2* ampTab;
@@ -90,7 +90,7 @@ int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);
 
 // Tensor-core form.  Whether the model family has it; the bytes of its
 // coefficient-fragment and amplitude tables (p.ncompPad, p.nseg set; no
-// amplitude table for point models); the dynamic shared memory of a
+// amplitude table for models without a spectrum); the dynamic shared memory of a
 // launch with component tile p.k.ct; the largest tile (<= 64, a multiple of 4)
 // that fits one CTA per SM, set in p->k.ct (0 when none fits: the caller keeps
 // the block form); the launch (the prologue kernels, then the kernel).

@@ -1,5 +1,5 @@
-// Beam-corrected DFT, tensor-core form (point families on uniformly spaced
-// channels).
+// Beam-corrected DFT, tensor-core form (every model family on uniformly
+// spaced channels).
 //
 // The model of record r at channel k for correlation q is
 //   M_q(r, k) = sum_c C_q(pair(r), c, plane) A_c(k) exp(2 pi i P(r, c) f_k):
@@ -39,6 +39,10 @@
 //                              the range-reduced split-FP32 phase), then per
 //                              matrix tile of the run the amplitude, the split,
 //                              three products and one packed complex step.
+// Gaussian families carry their taper exp(Q f^2) (Q per record and component)
+// on the lane's chain as well: over one matrix tile the taper changes by
+// R = exp(Q (32 f df + 256 df^2)), and R itself by exp(512 Q df^2), so two
+// packed multiplies per tile advance it.
 // Tile partial sums are folded into compensated (Kahan) totals.
 #include <stdint.h>
 
@@ -67,12 +71,12 @@ constexpr int kCmpSlots = kBeamMmaTiles * 2;  // packed compensation terms per t
 
 // Shared-memory layout of one CTA (offsets in floats, each a multiple of 4).
 struct MmaLayout {
-  int comp, coef, pp, ss, amp, cmp, uvw, pair, total;
+  int comp, coef, pp, ss, qq, amp, cmp, uvw, pair, total;
 };
 
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
 
-__host__ __device__ inline MmaLayout mma_layout(int ct, int cstride, int npair, bool table) {
+__host__ __device__ inline MmaLayout mma_layout(int ct, int cstride, int npair, bool table, bool gauss) {
   MmaLayout L;
   int o = 0;
   L.comp = o;
@@ -83,6 +87,8 @@ __host__ __device__ inline MmaLayout mma_layout(int ct, int cstride, int npair, 
   o += pad4(ct * kPStride * 2);
   L.ss = o;
   o += pad4(ct * kPStride * 2);
+  L.qq = o;
+  o += gauss ? pad4(ct * kPStride) : 0;
   L.amp = o;
   o += table ? (ct / 4) * kAmpGroup * 2 : 0;
   L.cmp = o;
@@ -93,6 +99,14 @@ __host__ __device__ inline MmaLayout mma_layout(int ct, int cstride, int npair, 
   o += kBeamMmaWarps;
   L.total = o;
   return L;
+}
+
+// Model families: spectral amplitudes from the prologue's table; Gaussian taper.
+__host__ __device__ constexpr bool mma_amp(int mode) {
+  return mode == kPointSpec || mode == kPointTSpec || mode == kGaussSpec || mode == kGaussTSpec;
+}
+__host__ __device__ constexpr bool mma_gauss(int mode) {
+  return mode == kGauss || mode == kGaussSpec || mode == kGaussTSpec;
 }
 
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
@@ -163,9 +177,9 @@ __global__ void __launch_bounds__(256) beam_coef_kernel(const __grid_constant__ 
   }
 }
 
-// Prologue of point families with a spectrum: the amplitude A exp(sum_t a_t
-// L^(t+1)) (PointSpec; L the log-frequency term of the channel) or
-// A_plane exp(alpha L) (PointTSpec) of every (run, component, channel), as the
+// Prologue of the families with a spectrum: the amplitude A exp(sum_t a_t
+// L^(t+1)) (PointSpec, GaussSpec; L the log-frequency term of the channel) or
+// A_plane exp(alpha L) (PointTSpec, GaussTSpec) of every (run, component, channel), as the
 // per-channel form computes it, in the lanes' order (BeamKParams.ampTab).
 template <int MODE>
 __global__ void __launch_bounds__(256) beam_amp_kernel(const __grid_constant__ BeamKParams bp) {
@@ -283,18 +297,19 @@ __device__ __forceinline__ bool stage_tile(const BeamKParams& bp, float* sComp, 
 template <int MODE>
 __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __grid_constant__ BeamKParams bp) {
   using F = Fields<MODE>;
-  static_assert(!F::kGaussian, "the tensor-core form takes point families");
+  constexpr bool kAmp = mma_amp(MODE), kGau = mma_gauss(MODE);
   static_assert(kBeamMmaWarps == 8, "the (record, component) tables index records by 3 bits");
   const KParams& p = bp.k;
   extern __shared__ __align__(16) float smem[];
   __shared__ __align__(8) uint64_t bar;
   const int ct = p.ct;
   const int npair = bp.numAntType * bp.numAntType;
-  const MmaLayout lay = mma_layout(ct, p.cstride, npair, F::kTable);
+  const MmaLayout lay = mma_layout(ct, p.cstride, npair, kAmp, kGau);
   float* sComp = smem + lay.comp;
   float4* sCoef = reinterpret_cast<float4*>(smem + lay.coef);
   float2* sP = reinterpret_cast<float2*>(smem + lay.pp);
   float2* sS = reinterpret_cast<float2*>(smem + lay.ss);
+  float* sQ = smem + lay.qq;
   float2* sAmp = reinterpret_cast<float2*>(smem + lay.amp);
   f2x* sCmp = reinterpret_cast<f2x*>(smem + lay.cmp);
   float* sUVW = smem + lay.uvw;
@@ -347,7 +362,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
 
     for (int c0 = 0; c0 < p.ncomp; c0 += ct) {
       __syncthreads();  // the previous tile's readers are done with shared memory
-      if (!stage_tile<F::kTable>(bp, sComp, sCoef, sAmp, c0, sg, seg.jplane, npair, &bar, phase)) return;
+      if (!stage_tile<kAmp>(bp, sComp, sCoef, sAmp, c0, sg, seg.jplane, npair, &bar, phase)) return;
       const int nc = min(ct, p.ncomp - c0);
       // (record, component): phase turns and the step of one matrix tile
       for (int idx = threadIdx.x; idx < kBeamMmaWarps * ct; idx += kMmaThreads) {
@@ -359,6 +374,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
         sP[c * kPStride + r] = make_float2(P.hi, P.lo);
         const ds ts = ds_mul(P, d16);
         sS[c * kPStride + r] = phasor_accurate(ds{__fsub_rn(ts.hi, rintf(ts.hi)), ts.lo});
+        if constexpr (kGau) sQ[c * kPStride + r] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
       }
       __syncthreads();
 
@@ -377,12 +393,29 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
           const uint32_t bl0 = __float_as_uint(bf.z), bl1 = __float_as_uint(bf.w);
           float2 za = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, fa));
           float2 zb = phasor_fast(ds_mul_frac(ds{Pp.x, Pp.y}, fb));
-          if constexpr (!F::kTable) {  // constant amplitude: carried by the chain
+          if constexpr (!kAmp && !kGau) {  // constant amplitude: carried by the chain
             const float A = sComp[c * p.cstride];
             za.x *= A;
             za.y *= A;
             zb.x *= A;
             zb.y *= A;
+          }
+          // Gaussian taper at the lane's channels (times a constant amplitude),
+          // its ratio over one matrix tile and that ratio's own constant ratio
+          f2x TP = 0ull, RP = 0ull, CP = 0ull;
+          if constexpr (kGau) {
+            const float Q = sQ[c * kPStride + warp];
+            const float D = d16.hi;
+            float ta = exp_fast(Q * fa.hi * fa.hi), tb = exp_fast(Q * fb.hi * fb.hi);
+            if constexpr (!kAmp) {
+              const float A = sComp[c * p.cstride];
+              ta *= A;
+              tb *= A;
+            }
+            TP = pk2(ta, tb);
+            RP = pk2(exp_fast(Q * D * (2.f * fa.hi + D)), exp_fast(Q * D * (2.f * fb.hi + D)));
+            const float c2 = exp_fast(2.f * Q * D * D);
+            CP = pk2(c2, c2);
           }
           f2x ZR = pk2(za.x, zb.x), ZI = pk2(za.y, zb.y);
           const f2x SR = pk2(st.x, st.x), SI = pk2(st.y, st.y), NSI = pk2(-st.y, -st.y);
@@ -394,9 +427,13 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
               for (int i = 0; i < kMmaChunk; i++) {
                 const int m = mc + i;
                 f2x VR = ZR, VI = ZI;
-                if constexpr (F::kTable) {
-                  const float2 a = ap[m * 32];
-                  const f2x AP = pk2(a.x, a.y);
+                if constexpr (kAmp || kGau) {
+                  f2x AP = TP;
+                  if constexpr (kAmp) {
+                    const float2 a = ap[m * 32];
+                    AP = pk2(a.x, a.y);
+                    if constexpr (kGau) AP = mul2(AP, TP);
+                  }
                   VR = mul2(ZR, AP);
                   VI = mul2(ZI, AP);
                 }
@@ -416,6 +453,10 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
                 const f2x nr = fma2(ZR, SR, mul2(ZI, NSI));
                 ZI = fma2(ZR, SI, mul2(ZI, SR));
                 ZR = nr;
+                if constexpr (kGau) {
+                  TP = mul2(TP, RP);
+                  RP = mul2(RP, CP);
+                }
               }
             }
           }
@@ -482,21 +523,20 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
 
 }  // namespace
 
-bool beam_mma_supported(int mode) { return mode == kPoint || mode == kPointSpec || mode == kPointTSpec; }
+bool beam_mma_supported(int mode) { return mode >= kPoint && mode <= kGaussTSpec; }
 
 size_t beam_mma_coef_bytes(const BeamKParams& p) {
   return (size_t)p.numJChan * p.numAntType * p.numAntType * (size_t)p.ncompPad * 8 * sizeof(float4);
 }
 
 size_t beam_mma_amp_bytes(const BeamKParams& p) {
-  if (p.mode != kPointSpec && p.mode != kPointTSpec) return 0;
+  if (!mma_amp(p.mode)) return 0;
   return (size_t)p.nseg * (size_t)(p.ncompPad / 4) * kAmpGroup * sizeof(float2);
 }
 
 size_t beam_mma_smem_bytes(const BeamKParams& p) {
-  const bool table = p.mode == kPointSpec || p.mode == kPointTSpec;
   const int npair = p.numAntType * p.numAntType;
-  return sizeof(float) * (size_t)mma_layout(p.k.ct, p.k.cstride, npair, table).total;
+  return sizeof(float) * (size_t)mma_layout(p.k.ct, p.k.cstride, npair, mma_amp(p.mode), mma_gauss(p.mode)).total;
 }
 
 int beam_mma_fit_tile(BeamKParams* p) {
@@ -527,6 +567,15 @@ int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err
     case kPointTSpec:
       fn = dft_beam_mma_kernel<kPointTSpec>;
       break;
+    case kGauss:
+      fn = dft_beam_mma_kernel<kGauss>;
+      break;
+    case kGaussSpec:
+      fn = dft_beam_mma_kernel<kGaussSpec>;
+      break;
+    case kGaussTSpec:
+      fn = dft_beam_mma_kernel<kGaussTSpec>;
+      break;
     default:
       break;
   }
@@ -549,7 +598,7 @@ int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err
     *err = std::string("tensor-core beam kernel cannot be resident: ") + cudaGetErrorString(ce);
     return 2;
   }
-  const bool table = kp.mode == kPointSpec || kp.mode == kPointTSpec;
+  const bool table = mma_amp(kp.mode);
   if (!kp.coefTab || kp.ncompPad < k.ncomp || kp.ncompPad % k.ct || (table && !kp.ampTab)) {
     *err = "tensor-core beam launch without its tables";
     return 3;
@@ -557,10 +606,20 @@ int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err
   if (table) {  // prologue: spectral amplitudes of every (run, component, channel)
     const long long n = (long long)kp.nseg * (kp.ncompPad / 4) * kAmpGroup;
     const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
-    if (kp.mode == kPointSpec)
-      beam_amp_kernel<kPointSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
-    else
-      beam_amp_kernel<kPointTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+    switch (kp.mode) {
+      case kPointSpec:
+        beam_amp_kernel<kPointSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      case kPointTSpec:
+        beam_amp_kernel<kPointTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      case kGaussSpec:
+        beam_amp_kernel<kGaussSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      default:
+        beam_amp_kernel<kGaussTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+    }
     ce = cudaGetLastError();
     if (ce != cudaSuccess) {
       *err = std::string("beam amplitude kernel launch: ") + cudaGetErrorString(ce);

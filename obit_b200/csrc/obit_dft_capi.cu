@@ -331,7 +331,7 @@ int ensure_plan(GPUInfo* g, State* s) {
       return rc;
     // Channel blocks that never span a change of Jones plane, from the same
     // planner: 16-channel blocks joined into runs for the tensor-core form
-    // (point families on uniformly spaced channels, runs of 4 channels or more
+    // (uniformly spaced channels, runs of 4 channels or more
     // on average), else blocks of at most kBeamK channels for the block form.
     LayoutDesc LB = L;
     LB.blockKey = b.jchan;

@@ -3,9 +3,9 @@ oracle: random Jones matrices per antenna type, component and Jones plane,
 2 or 4 correlations, subtract / replace / divide with flags, every model
 family, Stokes I, Q, U and V skies; unit Jones matrices reproduce the plain
 sky model; a record whose antennas fall outside the table is reported and
-left untouched.  Point families on uniformly spaced channels run the
-tensor-core form by default and the FP32 block form under
-OBIT_DFT_RECUR_CHAIN: both are checked."""
+left untouched.  Uniformly spaced channels run the tensor-core form by
+default and the FP32 block form under OBIT_DFT_RECUR_CHAIN: both are
+checked."""
 import numpy as np
 import pytest
 
@@ -90,8 +90,7 @@ def test_beam_every_family(mt, flavor):
     p = SkyModelParams(op=OP_SUB)
     info = {}
     got = _run_beam(uv, sky, p, beam, torch, flavor=flavor, info=info)
-    point = mt in (U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC)
-    assert info["form"] == (1 if point and flavor == _lib.OBIT_DFT_RECUR else 0)
+    assert info["form"] == (1 if flavor == _lib.OBIT_DFT_RECUR else 0)
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
 
@@ -214,7 +213,8 @@ def test_beam_circular_feeds(stok, flavor):
     _check(uv, got, want, l1, OP_SUB)
 
 
-@pytest.mark.parametrize("mt", [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC])
+@pytest.mark.parametrize("mt", [U.MOD_POINT, U.MOD_POINT_SPEC, U.MOD_POINT_TSPEC, U.MOD_GAUSS,
+                                U.MOD_GAUSS_SPEC, U.MOD_GAUSS_TSPEC])
 @pytest.mark.parametrize("nstok", [1, 2, 4])
 def test_beam_tensor_form_long_runs(mt, nstok):
     """The tensor-core form over runs longer than one 256-channel run (300
