@@ -52,7 +52,7 @@ ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per
 #   config4: dft_recur_kernel<32, 0> at 23,808 records (296.35 MB read + 240.85 MB written)
 #   config5: dft_recur_batch_kernel<32, 0> over the 96-facet draw at 189,029 records
 #            (rows x 0.001; 3,668.0 MB read + 3,567.0 MB written)
-#   beam:    dft_beam_recur_kernel<PointSpec, 4> at 4,032 records (200.9 MB read + 147.5 MB written)
+#   beam:    dft_beam_mma_kernel<PointSpec> at 4,032 records (232.3 MB read + 147.8 MB written)
 #   grid:    grid_apply_kernel at 4,032 records (215.87 MB read + 144.40 MB written)
 NCU_DRAM_BYTES_PER_RECORD = {
     "config1": ((65.61e6 + 13.73e6) / 42120, "42,120-record capture (the whole configuration)"),
