@@ -228,7 +228,11 @@ int obit_dft_set_beam(GPUInfo *gpuInfo, const ObitDFTBeam *beam);
  * default flavor; OBIT_DFT_RECUR_CHAIN keeps the block form -- 2: one thread
  * per channel, OBIT_DFT_PLAIN), info[1] = components per tile, info[2] =
  * channel runs (form 1) or blocks per record (forms 0 and 2).  Writes
- * min(n, 3) entries; OBIT_DFT_EBADARG when no beam is set. */
+ * min(n, 3) entries; OBIT_DFT_EBADARG when no beam is set.  Form 1 keeps
+ * per-plan device tables of the split Jones coefficients and the spectral
+ * amplitudes, rewritten at the start of every call (once per obit_dft_calc,
+ * before its first chunk), so a Jones table refilled in place between calls
+ * is read afresh; calls on one GPUInfo that overlap on the GPU share them. */
 int obit_dft_beam_info(GPUInfo *gpuInfo, int *info, int n);
 
 /* Beam images from which the Jones table is interpolated: for every antenna

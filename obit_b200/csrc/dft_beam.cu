@@ -540,8 +540,8 @@ int beam_fit_tile(BeamKParams* p, std::string* err) {
   return 0;
 }
 
-int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err) {
-  if (kp.mma) return launch_beam_mma(kp, stream, err);
+int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err, bool prologue) {
+  if (kp.mma) return launch_beam_mma(kp, stream, err, prologue);
   const KParams& k = kp.k;
   if (k.nvis <= 0 || k.ncomp <= 0 || k.nblocks <= 0) return 0;
   using Fn = void (*)(const BeamKParams);

@@ -85,8 +85,11 @@ size_t beam_smem_bytes(const BeamKParams& p);
 // one CTA per SM; sets p->k.ct.  Returns 0 or an error code with err.
 int beam_fit_tile(BeamKParams* p, std::string* err);
 
-// One launch over all records of kp (stream-ordered, asynchronous).
-int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err);
+// One launch over all records of kp (stream-ordered, asynchronous).  The
+// tensor-core form runs its prologues first unless `prologue` is false (the
+// caller ran launch_beam_prologue for this call and ordered the stream after
+// it).
+int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err, bool prologue = true);
 
 // Tensor-core form.  Whether the model family has it; the bytes of its
 // coefficient-fragment and amplitude tables (p.ncompPad, p.nseg set; no
@@ -99,6 +102,9 @@ size_t beam_mma_coef_bytes(const BeamKParams& p);
 size_t beam_mma_amp_bytes(const BeamKParams& p);
 size_t beam_mma_smem_bytes(const BeamKParams& p);
 int beam_mma_fit_tile(BeamKParams* p);
-int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err);
+int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err, bool prologue = true);
+// The tensor-core form's prologues alone (the coefficient fragments and the
+// spectral amplitudes), for callers that launch the kernel on several streams.
+int launch_beam_prologue(const BeamKParams& kp, cudaStream_t stream, std::string* err);
 
 }  // namespace obit

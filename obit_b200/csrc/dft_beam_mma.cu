@@ -548,7 +548,55 @@ int beam_mma_fit_tile(BeamKParams* p) {
   return 0;
 }
 
-int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err) {
+int launch_beam_prologue(const BeamKParams& kp, cudaStream_t stream, std::string* err) {
+  const KParams& k = kp.k;
+  if (k.ncomp <= 0 || kp.nseg <= 0) return 0;
+  const bool table = mma_amp(kp.mode);
+  if (!kp.coefTab || kp.ncompPad < k.ncomp || (table && !kp.ampTab)) {
+    *err = "tensor-core beam prologue without its tables";
+    return 3;
+  }
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t ce;
+  if (table) {  // prologue: spectral amplitudes of every (run, component, channel)
+    const long long n = (long long)kp.nseg * (kp.ncompPad / 4) * kAmpGroup;
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
+    switch (kp.mode) {
+      case kPointSpec:
+        beam_amp_kernel<kPointSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      case kPointTSpec:
+        beam_amp_kernel<kPointTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      case kGaussSpec:
+        beam_amp_kernel<kGaussSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+      default:
+        beam_amp_kernel<kGaussTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
+        break;
+    }
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) {
+      *err = std::string("beam amplitude kernel launch: ") + cudaGetErrorString(ce);
+      return 2;
+    }
+  }
+  {  // prologue: coefficient fragments of every (plane, type pair, component)
+    const long long n = (long long)kp.numJChan * kp.numAntType * kp.numAntType * kp.ncompPad;
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
+    beam_coef_kernel<<<(unsigned)blocks, 256, 0, stream>>>(kp);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) {
+      *err = std::string("beam coefficient kernel launch: ") + cudaGetErrorString(ce);
+      return 2;
+    }
+  }
+  return 0;
+}
+
+int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err, bool prologue) {
   const KParams& k = kp.k;
   if (k.nvis <= 0 || k.ncomp <= 0 || kp.nseg <= 0) return 0;
   if (k.ct < 4 || (k.ct & 3) || k.R != kBeamMmaWarps) {
@@ -603,39 +651,8 @@ int launch_beam_mma(const BeamKParams& kp, cudaStream_t stream, std::string* err
     *err = "tensor-core beam launch without its tables";
     return 3;
   }
-  if (table) {  // prologue: spectral amplitudes of every (run, component, channel)
-    const long long n = (long long)kp.nseg * (kp.ncompPad / 4) * kAmpGroup;
-    const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
-    switch (kp.mode) {
-      case kPointSpec:
-        beam_amp_kernel<kPointSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
-        break;
-      case kPointTSpec:
-        beam_amp_kernel<kPointTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
-        break;
-      case kGaussSpec:
-        beam_amp_kernel<kGaussSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
-        break;
-      default:
-        beam_amp_kernel<kGaussTSpec><<<(unsigned)blocks, 256, 0, stream>>>(kp);
-        break;
-    }
-    ce = cudaGetLastError();
-    if (ce != cudaSuccess) {
-      *err = std::string("beam amplitude kernel launch: ") + cudaGetErrorString(ce);
-      return 2;
-    }
-  }
-  {  // prologue: coefficient fragments of every (plane, type pair, component)
-    const long long n = (long long)kp.numJChan * kp.numAntType * kp.numAntType * kp.ncompPad;
-    const long long blocks = std::min<long long>((n + 255) / 256, (long long)nsm * 8);
-    beam_coef_kernel<<<(unsigned)blocks, 256, 0, stream>>>(kp);
-    ce = cudaGetLastError();
-    if (ce != cudaSuccess) {
-      *err = std::string("beam coefficient kernel launch: ") + cudaGetErrorString(ce);
-      return 2;
-    }
-  }
+  if (prologue)
+    if (int rc = launch_beam_prologue(kp, stream, err)) return rc;
   const long long nItems = (long long)((k.nvis + kBeamMmaWarps - 1) / kBeamMmaWarps) * kp.nseg;
   const long long grid = std::min<long long>(nItems, (long long)perSM * nsm);
   fn<<<(unsigned)grid, kMmaThreads, smem, stream>>>(kp);

@@ -808,6 +808,21 @@ int obit_dft_calc(GPUInfo* g) {
   // quarter-buffer chunks: only the first upload and the last download are not
   // hidden behind a kernel, and they shrink with the chunk.
   std::string err;
+  // The beam's tensor-core form writes its coefficient and amplitude tables
+  // once per call, on the first stream; the other streams wait for them.
+  const bool beamPrologue = s->beam.on && s->beam.kp.mma;
+  struct EventGuard {
+    cudaEvent_t e = nullptr;
+    ~EventGuard() {
+      if (e) cudaEventDestroy(e);
+    }
+  } ready;
+  if (beamPrologue) {
+    if ((rc = launch_beam_prologue(s->beam.kp, streams[0], &err))) return fail(rc, err);
+    CUDA_TRY(cudaEventCreateWithFlags(&ready.e, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(ready.e, streams[0]));
+    for (int i = 1; i < nbuf; i++) CUDA_TRY(cudaStreamWaitEvent(streams[i], ready.e, 0));
+  }
   const int step = rowsPerBuf >= 8192 ? (rowsPerBuf + 3) / 4 : rowsPerBuf;
   int chunk = 0;
   for (int r0 = 0; r0 < nvis; r0 += step, chunk++) {
@@ -820,7 +835,7 @@ int obit_dft_calc(GPUInfo* g) {
       BeamKParams k = s->beam.kp;
       k.k.vis = bufs[b];
       k.k.nvis = nr;
-      rc = launch_beam(k, streams[b], &err);
+      rc = launch_beam(k, streams[b], &err, !beamPrologue);
     } else {
       rc = launch_plan(s->plan, bufs[b], 0, nr, s->runComps, s->d_err, streams[b], &err);
     }
