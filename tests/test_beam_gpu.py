@@ -248,3 +248,19 @@ def test_beam_form_choice():
     info = {}
     _run_beam(uv, sky, SkyModelParams(op=OP_SUB), beam, torch, flavor=_lib.OBIT_DFT_PLAIN, info=info)
     assert info["form"] == 2
+
+
+@pytest.mark.parametrize("mt", [U.MOD_POINT_SPEC, U.MOD_GAUSS])
+def test_beam_tensor_form_many_antenna_types(mt):
+    """Five antenna types (25 type pairs): the coefficient fragments of every
+    pair shrink the tensor-core form's component tile below 64; records
+    still match the oracle."""
+    torch = pytest.importorskip("torch")
+    uv, sky, beam = beam_case(mt=mt, nstok=4, nrow=30, nchan=48, nif=2, ncomp=150, seed=83, ntype=5, njc=3,
+                              flag_frac=0.1)
+    p = SkyModelParams(op=OP_SUB)
+    info = {}
+    got = _run_beam(uv, sky, p, beam, torch, info=info)
+    assert info["form"] == 1 and 8 <= info["ct"] < 64
+    want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
+    _check(uv, got, want, l1, OP_SUB)
