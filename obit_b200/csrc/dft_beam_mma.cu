@@ -11,9 +11,10 @@
 // per warp) x one run of at most 256 uniformly spaced channels in one Jones
 // plane (BeamSeg).  The warp forms its record's phasors in registers and
 // multiplies them by the coefficients with mma.sync m16n8k8 (TF32 inputs, FP32
-// accumulate): the A operand is produced per warp in registers, which the
-// register-fed product takes directly, with the coefficient matrix (8 columns)
-// as B:
+// accumulate): the A operand is produced per warp in registers and changes for
+// every 16 x 8 tile, which the register-fed product takes directly (tcgen05.mma
+// reads A from shared or tensor memory, which would add a store, a fence and a
+// CTA-wide hand-off per tile), with the coefficient matrix (8 columns) as B:
 //   rows     16 channels of the run (lane group g = lane / 4 holds g, g + 8)
 //   k        4 components: real parts at k = 0..3, imaginary parts at 4..7
 //   columns  re, im of the model correlations XX, XY, YX, YY (RR, RL, LR, LL)
@@ -26,10 +27,10 @@
 // performance", 2022): the dropped lo lo term and the truncation of lo are
 // below 2^-20 of each term.
 //
-// Per launch, prologue kernels form the coefficient fragments of every
-// (Jones plane, antenna-type pair, component), split, and the spectral
-// amplitudes of every (run, component, channel), both in the order the lanes
-// read them.  Per component tile (ct components, the fragments of the run's
+// Per call (before the first chunk of a host call), prologue kernels form the
+// coefficient fragments of every (Jones plane, antenna-type pair, component),
+// split, and the spectral amplitudes of every (run, component, channel), both
+// in the order the lanes read them.  Per component tile (ct components, the fragments of the run's
 // plane for every type pair and the run's amplitudes, staged by bulk copies on
 // one mbarrier):
 //   (record, component)        phase turns P (split-FP32) and the step of one
