@@ -199,9 +199,9 @@ void ObitCUDASkyModelDFTSetModD(GPUInfo *gpuInfo, const double *xyz, int ncomp);
  * its position, independently of the others; every selected channel of every
  * selected IF is processed.  Once set, obit_dft_calc and obit_dft_calc_device
  * apply the beam-corrected model; NULL returns to the plain sky model; the
- * multi-facet batch and obit_dft_calc_noalloc do not take a beam, and the beam
- * path forms its FP64 phase from the table's FP32 positions (an FP64 side table
- * set by obit_dft_set_mod_d is not applied to it).  A record
+ * multi-facet batch and obit_dft_calc_noalloc do not take a beam; an FP64 side
+ * table set by obit_dft_set_mod_d enters the beam path's phases as it does the
+ * plain model's.  A record
  * whose antennas fall outside antType is left untouched and the call reports
  * OBIT_DFT_EKERNEL (code 3). */
 typedef struct ObitDFTBeam {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "dft_beam.h"
+#include "ds_math.cuh"
 
 namespace obit {
 
@@ -112,6 +113,22 @@ __device__ __forceinline__ void beam_coeffs(const BeamKParams& p, const float* J
       }
     }
   }
+}
+
+// Phase turns per unit frequency ratio, (X u + Y v + Z w) / 2 pi, in split FP32
+// for component c of the table (tile entry cp); with FP64 positions
+// (KParams.compsLo, 4 floats per component: the low parts of X, Y, Z) their
+// low parts enter as in the DFT kernels.
+__device__ __forceinline__ ds beam_phase_turns(const KParams& p, const float* cp, int c, float u, float v,
+                                               float w) {
+  ds d;
+  if (p.compsLo && c < p.ncomp) {
+    const float* lo = p.compsLo + (size_t)c * 4;
+    d = ds_dot3_lo(cp[1], lo[0], u, cp[2], lo[1], v, cp[3], lo[2], w);
+  } else {
+    d = ds_dot3(cp[1], u, cp[2], v, cp[3], w);
+  }
+  return ds_mul(d, ds{kInv2PiHi, kInv2PiLo});
 }
 
 }  // namespace obit

@@ -133,7 +133,14 @@ __global__ void __launch_bounds__(256) dft_beam_plain_kernel(const __grid_consta
       }
       if constexpr (F::kGaussian) e += (double)cp[4] * u * u + (double)cp[5] * v * v + (double)cp[6] * u * v;
       if (e != 0.0) A *= expf((float)e);
-      const double t = ((double)cp[1] * u + (double)cp[2] * v + (double)cp[3] * w) * 0.15915494309189535;
+      double X = cp[1], Y = cp[2], Z = cp[3];
+      if (p.k.compsLo && c0 + c < p.k.ncomp) {  // FP64 positions: the low parts of X, Y, Z
+        const float* lo = p.k.compsLo + (size_t)(c0 + c) * 4;
+        X += lo[0];
+        Y += lo[1];
+        Z += lo[2];
+      }
+      const double t = (X * u + Y * v + Z * w) * 0.15915494309189535;
       const float rr = (float)(t - rint(t));
       float sn, cs;
       __sincosf(6.283185307179586f * rr, &sn, &cs);
@@ -298,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) dft_beam_recur_kernel(const __gri
         const int r = idx & (R - 1);
         const float* cp = sComp + c * p.cstride;
         const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-        const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
+        const ds P = beam_phase_turns(p, cp, c0 + c, u, v, w);
         sP[idx] = make_float2(P.hi, P.lo);
         if constexpr (F::kGaussian) sQ[idx] = cp[4] * u * u + cp[5] * v * v + cp[6] * u * v;
         for (int d = 0; d < p.ndf; d++) {

@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) dft_beam_mma_kernel(const __gr
         const int r = idx & 7;
         const float* cp = sComp + c * p.cstride;
         const float u = sUVW[3 * r], v = sUVW[3 * r + 1], w = sUVW[3 * r + 2];
-        const ds P = ds_mul(ds_dot3(cp[1], u, cp[2], v, cp[3], w), ds{kInv2PiHi, kInv2PiLo});
+        const ds P = beam_phase_turns(p, cp, c0 + c, u, v, w);
         sP[c * kPStride + r] = make_float2(P.hi, P.lo);
         const ds ts = ds_mul(P, d16);
         sS[c * kPStride + r] = phasor_accurate(ds{__fsub_rn(ts.hi, rintf(ts.hi)), ts.lo});

@@ -393,6 +393,7 @@ int ensure_plan(GPUInfo* g, State* s) {
       k.k.blocks = b.d_blocks;
     }
     k.k.comps = s->d_comps;
+    k.k.compsLo = s->haveLo ? s->d_lo : nullptr;  // FP64 positions, the caller's order as d_comps
     k.k.ncomp = s->mc.model.ncomp;
     k.k.errFlag = s->d_err;
     k.k.rowBase = 0;

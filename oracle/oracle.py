@@ -200,12 +200,13 @@ class OracleBeam(C.Structure):
     ]
 
 
-def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None):
+def apply_beam_fp64(uv, sky, params, beam, nthreads: int | None = None, xyz=None):
     """FP64 beam-corrected model (oracle_beam.c) applied to a copy of uv.vis:
     returns (records, l1 of shape (nvis, nif, nchan, 4) over the model
     correlations XX, XY, YX, YY).  beam: obit_b200.beam.Beam (host Jones
-    table); the first min(2, nstok) correlations, or all four, are modelled."""
-    jb = Job(uv, sky, params, exact=True)
+    table); the first min(2, nstok) correlations, or all four, are modelled.
+    xyz: optional (ncomp, 3) FP64 positions used in place of the table's."""
+    jb = Job(uv, sky, params, exact=True, xyz=xyz)
     jb.job.startPoln = 0
     jb.job.numberPoln = 4 if uv.nstok >= 4 else min(2, uv.nstok)
     for i in range(4):

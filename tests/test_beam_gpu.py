@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 FORMS = [_lib.OBIT_DFT_RECUR, _lib.OBIT_DFT_RECUR_CHAIN]
 
 
-def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None, info=None):
+def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None, info=None, xyz=None):
     out = uv.copy()
     d_jones = torch.from_numpy(np.ascontiguousarray(jones if jones is not None else beam.jones)).cuda()
     gm = GPUSkyModel("beam")
@@ -32,6 +32,8 @@ def _run_beam(uv, sky, p, beam, torch, jones=None, flavor=None, info=None):
             gm.set_kernel(flavor)
         gm.set_beam(beam, d_jones.data_ptr())
         gm.DFTSetMod(sky)
+        if xyz is not None:
+            gm.set_positions_fp64(xyz)
         if info is not None:
             info.update(gm.beam_info())
         gm.DFTCalc(out)
@@ -264,3 +266,34 @@ def test_beam_tensor_form_many_antenna_types(mt):
     assert info["form"] == 1 and 8 <= info["ct"] < 64
     want, l1 = oracle.apply_beam_fp64(uv, sky, p, beam)
     _check(uv, got, want, l1, OP_SUB)
+
+
+@pytest.mark.parametrize("flavor", FORMS + [_lib.OBIT_DFT_PLAIN])
+def test_beam_fp64_positions(flavor):
+    """FP64 component positions (obit_dft_set_mod_d) in the beam path: on the
+    22 GHz, 8000 km sample the phases reach ~1e7 rad and the FP32 table moves
+    the model far beyond the bound; with the side table every form matches
+    the oracle evaluated at the FP64 positions."""
+    torch = pytest.importorskip("torch")
+    from test_fp64_positions_gpu import _vlbi_sample
+
+    from obit_b200.beam import Beam, baseline_codes
+    uv, sky = _vlbi_sample(nrow=24, ncomp=400)
+    uv.vis[:, 3] = baseline_codes(12, uv.nvis)
+    r = np.random.default_rng(91)
+    jones = np.zeros((2, sky.ncomp, 3, 8), np.float32)
+    jones[..., 0] = 1.0
+    jones[..., 6] = 1.0
+    jones += (0.2 * r.standard_normal(jones.shape)).astype(np.float32)
+    nfreq = uv.nchan * uv.nif
+    beam = Beam(r.integers(0, 2, 12), (np.arange(nfreq) * 3 // nfreq).astype(np.int32), jones)
+    p = SkyModelParams(op=OP_REPL)
+    want64, l1 = oracle.apply_beam_fp64(uv, sky, p, beam, xyz=sky.xyz)
+    want32, _ = oracle.apply_beam_fp64(uv, sky, p, beam)
+    shape = uv.vis_view().shape
+    a = want32[:, uv.nrparm:].reshape(shape)[..., 0, :]
+    b = want64[:, uv.nrparm:].reshape(shape)[..., 0, :]
+    dev = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1])) / np.maximum(l1[..., 0], 1e-30)
+    assert float(np.nanmax(dev)) > 1e-2  # the FP32 table alone is far from the FP64-position sky
+    got = _run_beam(uv, sky, p, beam, torch, flavor=flavor, xyz=sky.xyz)
+    _check(uv, got, want64, l1, OP_REPL)
