@@ -26,7 +26,7 @@ CU_SOURCES = ["dft_plan.cu", "dft_batch_kernels.cu", "dft_beam.cu", "dft_beam_mm
               "obit_dft_capi.cu", "obit_dft_static.cu", "dft_batch.cu", "grid_model.cu",
               "resident.cu"]
 C_SOURCES = ["gpu_skymodel.c"]
-CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp", "grid_host.cpp"]
+CXX_SOURCES = ["dft_planner.cpp", "cc_loader.cpp", "grid_host.cpp", "subuv.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -44,6 +44,36 @@ def _ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+def uv_struct(uv: UVData, with_buffer: bool, exact_freq: bool, keep: list) -> ObitDFTUVData:
+    """The ObitUV / ObitUVDesc fields of uv the C mirror reads (ObitDFTUVData);
+    arrays it points to are appended to keep.  with_buffer: point at uv.vis;
+    exact_freq: pass the FP64 channel frequencies."""
+    d = ObitDFTUVData()
+    d.nvis = uv.nvis
+    d.numVisBuff = uv.nvis
+    d.lrec = uv.lrec
+    d.nrparm = uv.nrparm
+    d.ncorr = uv.ncorr
+    d.ilocu, d.ilocv, d.ilocw = uv.ilocu, uv.ilocv, uv.ilocw
+    ax = [3, uv.nstok, uv.nchan, uv.nif, 1, 1, 1]
+    for i in range(7):
+        d.inaxes[i] = ax[i]
+    d.jlocs, d.jlocf, d.jlocif = uv.jlocs, uv.jlocf, uv.jlocif
+    d.incs, d.incf, d.incif = uv.incs, uv.incf, uv.incif
+    d.crvalStokes = uv.crval_stokes
+    d.freq = uv.freq
+    fs = np.ascontiguousarray(uv.fscale, dtype=np.float32)
+    fa = np.ascontiguousarray(uv.freqArr, dtype=np.float64)
+    keep += [fs, fa]
+    d.fscale = _ptr(fs, C.c_float)
+    d.freqArr = _ptr(fa, C.c_double) if exact_freq else None
+    if with_buffer:
+        if uv.vis.dtype != np.float32 or not uv.vis.flags.c_contiguous:
+            raise DFTError(1, "uv buffer must be C-contiguous float32")
+        d.buffer = _ptr(uv.vis, C.c_float)
+    return d
+
+
 class GPUSkyModel:
     """One sky model bound to one uv layout on one GPU."""
 
@@ -92,30 +122,7 @@ class GPUSkyModel:
         return s
 
     def _uv_struct(self, uv: UVData, with_buffer: bool, exact_freq: bool) -> ObitDFTUVData:
-        d = ObitDFTUVData()
-        d.nvis = uv.nvis
-        d.numVisBuff = uv.nvis
-        d.lrec = uv.lrec
-        d.nrparm = uv.nrparm
-        d.ncorr = uv.ncorr
-        d.ilocu, d.ilocv, d.ilocw = uv.ilocu, uv.ilocv, uv.ilocw
-        ax = [3, uv.nstok, uv.nchan, uv.nif, 1, 1, 1]
-        for i in range(7):
-            d.inaxes[i] = ax[i]
-        d.jlocs, d.jlocf, d.jlocif = uv.jlocs, uv.jlocf, uv.jlocif
-        d.incs, d.incf, d.incif = uv.incs, uv.incf, uv.incif
-        d.crvalStokes = uv.crval_stokes
-        d.freq = uv.freq
-        fs = np.ascontiguousarray(uv.fscale, dtype=np.float32)
-        fa = np.ascontiguousarray(uv.freqArr, dtype=np.float64)
-        self._keep += [fs, fa]
-        d.fscale = _ptr(fs, C.c_float)
-        d.freqArr = _ptr(fa, C.c_double) if exact_freq else None
-        if with_buffer:
-            if uv.vis.dtype != np.float32 or not uv.vis.flags.c_contiguous:
-                raise DFTError(1, "uv buffer must be C-contiguous float32")
-            d.buffer = _ptr(uv.vis, C.c_float)
-        return d
+        return uv_struct(uv, with_buffer, exact_freq, self._keep)
 
     # -- class functions -----------------------------------------------------
     def DFTInit(self, sky: SkyComps, uv: UVData, params: SkyModelParams | None = None,

@@ -1,17 +1,21 @@
 """The caller of the model path: ObitSkyModelSubUV's pass structure
-(ObitSystem/Obit/src/ObitSkyModel.c:850-1087) over this library's GPU paths.
-The mode is chosen as ObitSkyModelChose does (or from the measured rates);
-the DFT loads every field's components into one table and applies them in one
-pass (nload = -1, :986-987), the gridded model applies each field in its own
-pass, in field order (:974-995); data I/O, calibration and selection of the
-reference's ObitUV layer are the caller's."""
+(ObitSystem/Obit/src/ObitSkyModel.c:850-1087) over this library's GPU paths,
+run natively by obit_dft_sub_uv (include/obit_dft_subuv.h).  The mode is chosen
+as ObitSkyModelChose does (or from the measured rates); the DFT loads every
+field's components into one table and applies them in one pass (nload = -1,
+:986-987), the gridded model applies each field in its own pass, in field order
+(:974-995); data I/O, calibration and selection of the reference's ObitUV layer
+are the caller's."""
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
+from . import _lib
 from . import grid as GR
-from .comps import CCField, CCModel, load_comps
-from .skymodel import GPUSkyModel, SkyModelParams
+from ._lib import ObitDFTErr, ObitDFTGridImage, ObitDFTSkyModel
+from .comps import CCField, CCModel, _field_array, _model
+from .skymodel import OP_DIV, OP_REPL, SkyModelParams, uv_struct
 from .uvdata import UVData
 
 
@@ -22,50 +26,53 @@ class SubUVResult:
     ncomp: int           # components applied (DFT: merged rows; grid: rows gridded)
 
 
+def _sky_fields(p: SkyModelParams, uv: UVData) -> ObitDFTSkyModel:
+    """The ObitSkyModel settings of params (operation, factor, selection); the
+    model type and spectral terms come from the loaded table."""
+    s = ObitDFTSkyModel()
+    s.factor = p.factor
+    s.doDivide = int(p.op == OP_DIV)
+    s.doReplace = int(p.op == OP_REPL)
+    s.doFlip = int(p.doFlip)
+    s.stokFactor = p.stokFactor
+    s.startChannelPB = p.startChannel if p.startChannel > 0 else 1
+    s.numberChannelPB = p.numberChannel if p.numberChannel > 0 else uv.nchan - s.startChannelPB + 1
+    s.startIFPB = p.startIF if p.startIF > 0 else 1
+    s.numberIFPB = p.numberIF if p.numberIF > 0 else uv.nif - s.startIFPB + 1
+    s.startPoln = p.startPoln if p.startPoln > 0 else 1
+    s.numberPoln = p.numberPoln if p.numberPoln > 0 else min(2, uv.nstok)
+    s.modelRefFreq = uv.freq
+    s.GPU_no = p.GPU_no
+    return s
+
+
 def sub_uv(uv: UVData, fields: list[CCField], images: list[GR.GridImage], model: CCModel,
            params: SkyModelParams | None = None, mode: int = GR.MODE_FASTEST, measured: bool = False,
            maxGrid: float = 1e20, kernel: int = GR.KERNEL_REFERENCE, exact_freq: bool = False) -> SubUVResult:
-    """Applies the CLEAN model of `fields` to uv's records (a copy) with the
-    operation of params.  mode: MODE_FASTEST chooses (the reference's time model,
-    or this library's measured rates with measured=True), MODE_DFT or MODE_GRID
-    force one.  exact_freq: the DFT forms its phase from FP64 channel
-    frequencies (the gridded model, as the reference's, uses FP32 freqScale)."""
+    """Applies the CLEAN model of `fields` to a copy of uv's records with the
+    operation of params.  mode: MODE_FASTEST chooses (the reference's time
+    model, or this library's measured rates with measured=True), MODE_DFT or
+    MODE_GRID force one.  exact_freq: the DFT forms its phase from FP64
+    channel frequencies (the gridded model, as the reference's, uses FP32
+    freqScale)."""
     p = params or SkyModelParams()
-    ncc = []
-    for f in fields:
-        first = f.startComp if f.startComp > 0 else 1
-        last = f.endComp if f.endComp > 0 else len(f.flux)
-        ncc.append(max(0, last - first + 1))
-    nx = [im.nx for im in images]
-    ny = [im.ny for im in images]
-    chan = uv.nchan * uv.nif
-    if mode == GR.MODE_FASTEST:
-        choose = GR.choose_mode_measured if measured else (lambda *a: GR.choose_mode(GR.MODE_FASTEST, *a))
-        use = choose(GR.TYPE_COMPS, ncc, nx, ny, uv.nvis, chan)
-    else:
-        use = mode
-    if use == GR.MODE_DFT:
-        sky, _ = load_comps(fields, model)
-        out = uv.copy()
-        if sky.ncomp > 0 and uv.nvis > 0:
-            q = SkyModelParams(**{**p.__dict__, "nVisPIO": max(1, uv.nvis)})
-            gm = GPUSkyModel("subuv")
-            try:
-                gm.DFTInit(sky, out, q, exact_freq=exact_freq)
-                gm.DFTSetMod(sky)
-                gm.DFTCalc(out)
-                gm.DFTShutdown()
-            finally:
-                gm.close()
-        return SubUVResult(out, GR.MODE_DFT, sky.ncomp)
-    if use != GR.MODE_GRID:
-        raise ValueError(f"mode {use} is not supported (Mixed: the DFT with minDFT plus the grid with maxGrid)")
-    out = uv
-    total = 0
-    for f, im in zip(fields, images):
-        with GR.GridField(f, im, model, maxGrid=maxGrid, kernel=kernel) as gf:
-            total += gf.info()["ncomp"]
-            out = gf.FTGrid(out, p)
-    if out is uv:
-        out = uv.copy()
-    return SubUVResult(out, GR.MODE_GRID, total)
+    if mode not in (GR.MODE_FASTEST, GR.MODE_DFT, GR.MODE_GRID):
+        raise ValueError(f"mode {mode} is not supported (Mixed: the DFT with minDFT plus the grid with maxGrid)")
+    lib = _lib.load()
+    keep: list = []
+    out = uv.copy()
+    arr = _field_array(fields, keep)
+    imgs = (ObitDFTGridImage * max(1, len(images)))()
+    for i, im in enumerate(images):
+        imgs[i] = ObitDFTGridImage(int(im.nx), int(im.ny), float(im.crpixX), float(im.crpixY))
+    m = _model(model)
+    s = _sky_fields(p, out)
+    d = uv_struct(out, True, exact_freq, keep)
+    used, ncomp = C.c_int(), C.c_int()
+    err = ObitDFTErr()
+    rc = lib.obit_dft_sub_uv(arr, len(fields), imgs if images else None, C.byref(m), C.byref(s), C.byref(d),
+                             int(mode), int(bool(measured)), float(maxGrid), int(kernel), C.byref(used),
+                             C.byref(ncomp), C.byref(err))
+    if rc:
+        raise _lib.DFTError(rc, err.message.decode(errors="replace"))
+    return SubUVResult(out, used.value, ncomp.value)
