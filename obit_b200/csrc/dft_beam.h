@@ -94,7 +94,7 @@ int launch_beam(const BeamKParams& kp, cudaStream_t stream, std::string* err, bo
 // Tensor-core form.  Whether the model family has it; the bytes of its
 // coefficient-fragment and amplitude tables (p.ncompPad, p.nseg set; no
 // amplitude table for models without a spectrum); the dynamic shared memory of a
-// launch with component tile p.k.ct; the largest tile (<= 64, a multiple of 4)
+// launch with component tile p.k.ct; the largest tile (<= 128, a multiple of 4)
 // that fits one CTA per SM, set in p->k.ct (0 when none fits: the caller keeps
 // the block form); the launch (the prologue kernels, then the kernel).
 bool beam_mma_supported(int mode);

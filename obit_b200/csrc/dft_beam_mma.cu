@@ -541,7 +541,7 @@ size_t beam_mma_smem_bytes(const BeamKParams& p) {
 }
 
 int beam_mma_fit_tile(BeamKParams* p) {
-  for (int ct = 64; ct >= 8; ct -= 4) {
+  for (int ct = 128; ct >= 8; ct -= 4) {
     p->k.ct = ct;
     if (beam_mma_smem_bytes(*p) <= 220 * 1024) return ct;
   }
