@@ -20,7 +20,11 @@ extern "C" {
  *   mode      0 chooses as ObitSkyModelChose (ObitSkyModel.c:3560-3620), or
  *             from this library's measured B200 rates when measured = 1
  *             (obit_dft_choose_mode_measured); 1 forces the DFT, 2 the
- *             gridded model;
+ *             gridded model, 3 OBIT_SkyModel_Mixed: per field, the DFT of
+ *             the components above model->minDFT, then the gridded model of
+ *             those of at most maxGrid (ObitSkyModel.c:1421-1424, 1512-1515;
+ *             the caller sets the two thresholds as the reference's
+ *             minDFT and maxGrid);
  *   DFT       every field's components in one table (ObitSkyModelLoadComps,
  *             here obit_dft_load_comps) applied in one pass (nload = -1,
  *             ObitSkyModel.c:986-987) through the ObitGPUSkyModel mirror
@@ -29,10 +33,10 @@ extern "C" {
  *   gridded   each field in its own pass, in field order (:974-995),
  *             obit_dft_grid_create / obit_dft_grid_apply_host with maxGrid
  *             and kernel (OBIT_DFT_GRID_KERNEL_*); images must be given.
- * *modeUsed (1 or 2) and *ncompUsed (DFT: merged component rows; gridded:
- * rows gridded over the fields) are written when not NULL.  Returns 0, or a
- * status code of include/obit_dft.h with the message in err (and in
- * obit_dft_last_error for the library's own failures). */
+ * *modeUsed (1, 2 or 3) and *ncompUsed (DFT: merged component rows;
+ * gridded: rows gridded over the fields; Mixed: both) are written when not
+ * NULL.  Returns 0, or a status code of include/obit_dft.h with the message in
+ * err (and in obit_dft_last_error for the library's own failures). */
 int obit_dft_sub_uv(const ObitDFTCCField *fields, int nfield, const ObitDFTGridImage *images,
                     const ObitDFTCCModel *model, const ObitDFTSkyModel *sky, ObitDFTUVData *uv, int mode,
                     int measured, float maxGrid, int kernel, int *modeUsed, int *ncompUsed, ObitDFTErr *err);

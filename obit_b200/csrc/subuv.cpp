@@ -1,7 +1,7 @@
 // ObitSkyModelSubUV's pass structure (ObitSkyModel.c:850-1087) over this
 // library's GPU paths: the mode choice, one DFT pass over every field's
-// components, or a gridded pass per field.  Host code over the C ABI; see
-// include/obit_dft_subuv.h.
+// components, a gridded pass per field, or both per field (Mixed).  Host code
+// over the C ABI; see include/obit_dft_subuv.h.
 #include "obit_dft_subuv.h"
 
 #include <stdarg.h>
@@ -47,6 +47,67 @@ struct GridDeleter {
   }
 };
 
+// One DFT pass over the components of `fields` (one table, the ObitGPUSkyModel
+// mirror); *ncomp receives the merged component rows.
+int dft_pass(const ObitDFTCCField* fields, int nfield, const ObitDFTCCModel* model, const ObitDFTSkyModel* sky,
+             ObitDFTUVData* uv, int* ncompOut, ObitDFTErr* err) {
+  int nrow = 0, ncomp = 0, lcomp = 0, modType = 0, nterm = 0;
+  int rc = obit_dft_load_comps(fields, nfield, model, nullptr, 0, &nrow, &ncomp, &lcomp, &modType, &nterm);
+  if (rc) return lib_err(err, rc, "component table");
+  std::vector<float> table((size_t)std::max(1, nrow) * std::max(1, lcomp));
+  rc = obit_dft_load_comps(fields, nfield, model, table.data(), (long long)table.size(), &nrow, &ncomp, &lcomp,
+                           &modType, &nterm);
+  if (rc) return lib_err(err, rc, "component table");
+  *ncompOut = ncomp;
+  const int nvis = uv->numVisBuff;
+  if (ncomp <= 0 || nvis <= 0) return OBIT_DFT_OK;
+  ObitDFTSkyModel s = *sky;
+  s.modType = modType;
+  s.nSpecTerm = nterm;
+  s.nVisPIO = std::max(1, nvis);
+  Mirror in(obit_gpu_skymodel_create("subuv"));
+  if (!in) return set_err(err, OBIT_DFT_ECUDA, "obit_dft_sub_uv: cannot create the GPU sky model");
+  if (obit_gpu_skymodel_dft_init(in.get(), &s, uv, err)) return OBIT_DFT_EBADARG;
+  if (obit_gpu_skymodel_dft_setmod(in.get(), &s, table.data(), lcomp, ncomp, err)) return OBIT_DFT_EBADARG;
+  if (obit_gpu_skymodel_dft_calc(in.get(), uv, err)) return OBIT_DFT_EKERNEL;
+  return OBIT_DFT_OK;
+}
+
+// The records' layout and selection as a GPUVisInfo, from a mirror instance
+// (held by `in` while the descriptor is used).
+int grid_descriptor(const ObitDFTSkyModel* sky, ObitDFTUVData* uv, Mirror* in, const GPUVisInfo** vi,
+                    ObitDFTErr* err) {
+  ObitDFTSkyModel s = *sky;
+  s.modType = 0;
+  s.nSpecTerm = 0;
+  s.nVisPIO = 1;
+  in->reset(obit_gpu_skymodel_create("subuv-grid"));
+  if (!*in) return set_err(err, OBIT_DFT_ECUDA, "obit_dft_sub_uv: cannot create the GPU sky model");
+  if (obit_gpu_skymodel_dft_init(in->get(), &s, uv, err)) return OBIT_DFT_EBADARG;
+  *vi = obit_gpu_skymodel_info(in->get())->h_visInfo;
+  return OBIT_DFT_OK;
+}
+
+// One gridded pass of a field (components of at most maxGrid); *nrow
+// receives the rows gridded.
+int grid_pass(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
+              float maxGrid, int kernel, const GPUVisInfo* vi, const ObitDFTSkyModel* sky, ObitDFTUVData* uv,
+              long long* nrow, ObitDFTErr* err) {
+  ObitDFTGrid* raw = nullptr;
+  int rc = obit_dft_grid_create(field, image, model, maxGrid, kernel, nullptr, &raw);
+  if (rc) return lib_err(err, rc, "gridded field");
+  std::unique_ptr<ObitDFTGrid, GridDeleter> grid(raw);
+  long long info[1] = {0};
+  if ((rc = obit_dft_grid_info(grid.get(), info, 1))) return lib_err(err, rc, "gridded field");
+  *nrow = info[0];
+  if (info[0] <= 0) return OBIT_DFT_OK;
+  const int opType = sky->doReplace ? 2 : (sky->doDivide ? 1 : 0);
+  rc = obit_dft_grid_apply_host(grid.get(), vi, opType, sky->stokFactor, sky->doFlip, uv->buffer,
+                                uv->numVisBuff, nullptr);
+  if (rc) return lib_err(err, rc, "gridded pass");
+  return OBIT_DFT_OK;
+}
+
 }  // namespace
 
 extern "C" int obit_dft_sub_uv(const ObitDFTCCField* fields, int nfield, const ObitDFTGridImage* images,
@@ -57,7 +118,8 @@ extern "C" int obit_dft_sub_uv(const ObitDFTCCField* fields, int nfield, const O
     return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv: NULL argument or no fields");
   if (uv->jlocf < 0 || uv->jlocf > 6 || (uv->jlocif > 6))
     return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv: uv descriptor without a frequency axis");
-  if (mode < 0 || mode > 2) return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv: mode %d is not 0, 1 or 2", mode);
+  if (mode < 0 || mode > 3)
+    return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv: mode %d is not 0, 1, 2 or 3", mode);
   const int nvis = uv->numVisBuff;
   const int nchan = uv->inaxes[uv->jlocf] * (uv->jlocif >= 0 ? uv->inaxes[uv->jlocif] : 1);
   // components per field (the selected CC rows) and image sizes for the choice
@@ -82,55 +144,28 @@ extern "C" int obit_dft_sub_uv(const ObitDFTCCField* fields, int nfield, const O
   if (ncompUsed) *ncompUsed = 0;
 
   if (use == 1) {  // DFT: all fields' components in one table, one pass
-    int nrow = 0, ncomp = 0, lcomp = 0, modType = 0, nterm = 0;
-    int rc = obit_dft_load_comps(fields, nfield, model, nullptr, 0, &nrow, &ncomp, &lcomp, &modType, &nterm);
-    if (rc) return lib_err(err, rc, "component table");
-    std::vector<float> table((size_t)std::max(1, nrow) * std::max(1, lcomp));
-    rc = obit_dft_load_comps(fields, nfield, model, table.data(), (long long)table.size(), &nrow, &ncomp,
-                             &lcomp, &modType, &nterm);
-    if (rc) return lib_err(err, rc, "component table");
-    if (ncompUsed) *ncompUsed = ncomp;
-    if (ncomp <= 0 || nvis <= 0) return OBIT_DFT_OK;
-    ObitDFTSkyModel s = *sky;
-    s.modType = modType;
-    s.nSpecTerm = nterm;
-    s.nVisPIO = std::max(1, nvis);
-    Mirror in(obit_gpu_skymodel_create("subuv"));
-    if (!in) return set_err(err, OBIT_DFT_ECUDA, "obit_dft_sub_uv: cannot create the GPU sky model");
-    if (obit_gpu_skymodel_dft_init(in.get(), &s, uv, err)) return OBIT_DFT_EBADARG;
-    if (obit_gpu_skymodel_dft_setmod(in.get(), &s, table.data(), lcomp, ncomp, err)) return OBIT_DFT_EBADARG;
-    if (obit_gpu_skymodel_dft_calc(in.get(), uv, err)) return OBIT_DFT_EKERNEL;
-    return OBIT_DFT_OK;
+    int n = 0;
+    const int rc = dft_pass(fields, nfield, model, sky, uv, &n, err);
+    if (ncompUsed) *ncompUsed = n;
+    return rc;
   }
-  if (use != 2)
-    return set_err(err, OBIT_DFT_EUNSUPPORTED,
-                   "obit_dft_sub_uv: mode %d is not supported (Mixed: the DFT with minDFT plus the grid "
-                   "with maxGrid)",
-                   use);
+  if (use != 2 && use != 3)
+    return set_err(err, OBIT_DFT_EUNSUPPORTED, "obit_dft_sub_uv: mode %d is not supported", use);
   if (!images) return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv: the gridded model needs the images");
   if (nvis <= 0) return OBIT_DFT_OK;
-  // the records' layout and selection, from a mirror instance's descriptor
-  ObitDFTSkyModel s = *sky;
-  s.modType = 0;
-  s.nSpecTerm = 0;
-  s.nVisPIO = 1;
-  Mirror in(obit_gpu_skymodel_create("subuv-grid"));
-  if (!in) return set_err(err, OBIT_DFT_ECUDA, "obit_dft_sub_uv: cannot create the GPU sky model");
-  if (obit_gpu_skymodel_dft_init(in.get(), &s, uv, err)) return OBIT_DFT_EBADARG;
-  const GPUVisInfo* vi = obit_gpu_skymodel_info(in.get())->h_visInfo;
-  const int opType = sky->doReplace ? 2 : (sky->doDivide ? 1 : 0);
+  Mirror in;
+  const GPUVisInfo* vi = nullptr;
+  if (int rc = grid_descriptor(sky, uv, &in, &vi, err)) return rc;
   long long total = 0;
   for (int f = 0; f < nfield; f++) {  // a pass per field, in field order
-    ObitDFTGrid* raw = nullptr;
-    int rc = obit_dft_grid_create(&fields[f], &images[f], model, maxGrid, kernel, nullptr, &raw);
-    if (rc) return lib_err(err, rc, "gridded field");
-    std::unique_ptr<ObitDFTGrid, GridDeleter> grid(raw);
-    long long info[1] = {0};
-    if ((rc = obit_dft_grid_info(grid.get(), info, 1))) return lib_err(err, rc, "gridded field");
-    total += info[0];
-    rc = obit_dft_grid_apply_host(grid.get(), vi, opType, sky->stokFactor, sky->doFlip, uv->buffer, nvis,
-                                  nullptr);
-    if (rc) return lib_err(err, rc, "gridded pass");
+    if (use == 3) {  // Mixed: the field's components above minDFT by the DFT first
+      int n = 0;
+      if (int rc = dft_pass(&fields[f], 1, model, sky, uv, &n, err)) return rc;
+      total += n;
+    }
+    long long n = 0;
+    if (int rc = grid_pass(&fields[f], &images[f], model, maxGrid, kernel, vi, sky, uv, &n, err)) return rc;
+    total += n;
   }
   if (ncompUsed) *ncompUsed = (int)total;
   return OBIT_DFT_OK;

@@ -22,8 +22,8 @@ from .uvdata import UVData
 @dataclass
 class SubUVResult:
     uv: UVData
-    mode: int            # grid.MODE_DFT or grid.MODE_GRID
-    ncomp: int           # components applied (DFT: merged rows; grid: rows gridded)
+    mode: int            # grid.MODE_DFT, MODE_GRID or MODE_MIXED
+    ncomp: int           # components applied (DFT: merged rows; grid: rows gridded; Mixed: both)
 
 
 def _sky_fields(p: SkyModelParams, uv: UVData) -> ObitDFTSkyModel:
@@ -52,12 +52,13 @@ def sub_uv(uv: UVData, fields: list[CCField], images: list[GR.GridImage], model:
     """Applies the CLEAN model of `fields` to a copy of uv's records with the
     operation of params.  mode: MODE_FASTEST chooses (the reference's time
     model, or this library's measured rates with measured=True), MODE_DFT or
-    MODE_GRID force one.  exact_freq: the DFT forms its phase from FP64
-    channel frequencies (the gridded model, as the reference's, uses FP32
-    freqScale)."""
+    MODE_GRID force one, MODE_MIXED runs per field the DFT of the components
+    above model.minDFT and the gridded model of those of at most maxGrid.
+    exact_freq: the DFT forms its phase from FP64 channel frequencies (the
+    gridded model, as the reference's, uses FP32 freqScale)."""
     p = params or SkyModelParams()
-    if mode not in (GR.MODE_FASTEST, GR.MODE_DFT, GR.MODE_GRID):
-        raise ValueError(f"mode {mode} is not supported (Mixed: the DFT with minDFT plus the grid with maxGrid)")
+    if mode not in (GR.MODE_FASTEST, GR.MODE_DFT, GR.MODE_GRID, GR.MODE_MIXED):
+        raise ValueError(f"unknown mode {mode}")
     lib = _lib.load()
     keep: list = []
     out = uv.copy()

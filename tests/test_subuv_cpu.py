@@ -1,6 +1,7 @@
-"""obit_dft_sub_uv argument checks that need no GPU: a call without fields, an
-unknown mode, a mode choice or gridded pass without the images are rejected
-with OBIT_DFT_EBADARG and a message, before any device work."""
+"""obit_dft_sub_uv argument checks that need no GPU: a call without fields, a
+mode choice or gridded pass without the images are rejected with
+OBIT_DFT_EBADARG and a message, before any device work; an unknown mode
+never reaches the library."""
 import numpy as np
 import pytest
 
@@ -37,7 +38,7 @@ def test_rejects_choice_and_grid_without_images():
         assert e.value.code == 1 and "images" in str(e.value)
 
 
-def test_rejects_mixed_mode():
+def test_rejects_unknown_mode():
     with pytest.raises(ValueError):
         sub_uv(_uv(), [_field()], [GR.GridImage(64, 64, 33, 33)], CCModel(uvRA=0.0, uvDec=30.0),
-               SkyModelParams(), mode=GR.MODE_MIXED)
+               SkyModelParams(), mode=7)

@@ -44,3 +44,34 @@ def test_fastest_follows_the_reference_choice():
     assert r.mode == want
     r2 = sub_uv(uv, [f1], gim, m, SkyModelParams(op=OP_SUB), measured=True)
     assert r2.mode == GR.MODE_DFT  # 200 components: the DFT on the B200
+
+
+def test_mixed_dft_above_min_then_grid():
+    """OBIT_SkyModel_Mixed: per field, the DFT of the components above minDFT,
+    then the gridded model of those of at most maxGrid (the same threshold),
+    exact kernel: the whole model is subtracted as the DFT oracle has it.  One
+    component per cell, so the split by flux is the same for the DFT's merged
+    table and the grid's rows."""
+    from obit_b200.comps import CCModel
+    fields, images = [], []
+    f0, img0, m, uv = field_case(N=96, seed=60, ncomp=200, nint=5)
+    for s_, f in ((60, f0), (61, field_case(N=96, seed=61, ncomp=150, nint=5, shift3d=True)[0])):
+        cells = {}
+        keep = [i for i, (x, y) in enumerate(zip(f.deltaX, f.deltaY)) if cells.setdefault((x, y), i) == i]
+        f.flux, f.deltaX, f.deltaY = f.flux[keep], f.deltaX[keep], f.deltaY[keep]
+        fields.append(f)
+        images.append(GR.GridImage(img0.nx, img0.ny, img0.crpixX, img0.crpixY))
+    m.do3D = True
+    T = 0.4
+    mm = CCModel(**{**m.__dict__, "minDFT": T})
+    p = SkyModelParams(op=OP_SUB)
+    r = sub_uv(uv, fields, images, mm, p, mode=GR.MODE_MIXED, maxGrid=T, kernel=GR.KERNEL_EXACT)
+    assert r.mode == GR.MODE_MIXED
+    sky, _ = load_comps(fields, m)
+    assert r.ncomp >= sky.ncomp
+    want = oracle.apply_fp64(uv, sky, p, exact=False)
+    _, l1 = oracle.model_fp64(uv, sky, p, exact=False)
+    a = r.uv.vis[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+    b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
+    d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1])) / l1[..., None]
+    assert float(d.max()) < 1e-5, float(d.max())
