@@ -142,6 +142,7 @@ int build_group(Group& g, std::vector<Facet>& fs, const float* d_comps, int* d_e
   TuneDesc T = g.tune;
   T.flavor = kFlavorRecur;
   if (T.threads != 128) T.threads = 256;
+  if (T.ct == 0) T.ct = 128;  // the batch's default tile: every facet is planned with the lead's
   {
     int lead = g.order[0];
     long long best = -1;
@@ -523,7 +524,7 @@ extern "C" int obit_dft_batch_set_tile(ObitDFTBatch* b, int K, int ct, int Bt, i
   drop_graph(b);
   for (Group& g : b->groups) {
     g.tune.K = K;
-    g.tune.ct = ct ? ct : TuneDesc().ct;
+    g.tune.ct = ct ? ct : 128;
     g.tune.Bt = Bt;
     g.tune.threads = threads ? threads : 256;
     free_group(g);

@@ -64,7 +64,9 @@ struct ApplyDesc {
 struct TuneDesc {
   int flavor = kFlavorRecur;
   int K = 0;    // channels per thread; 0 = chosen by the planner
-  int ct = 128;  // components per shared-memory tile (shrunk to fit shared memory)
+  int ct = 0;   // components per shared-memory tile (shrunk to fit shared memory); 0 = planner's
+               // choice: 160 where it fits shared memory (and the spectral-factored bound)
+               // as it is, else 128 shrunk to fit
   int Bt = 0;   // blocks per tile (power of two); 0 = chosen by the planner
   int threads = 0;  // CTA size, 128 or 256; 0 = chosen by the planner
   int specFactor = 1;  // 0: point families with a spectrum keep the chain form

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "dft_plan.h"
 
@@ -67,8 +68,8 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
     *err = "no kernel for flavor " + std::to_string(T.flavor) + " K " + std::to_string(T.K);
     return 3;
   }
-  if (T.ct < 1 || T.ct > 1024) {
-    *err = "components per tile must be in 1..1024";
+  if (T.ct < 0 || T.ct > 1024) {
+    *err = "components per tile must be in 1..1024 (0: planner's choice)";
     return 3;
   }
   const int nfreq = L.nchan * L.nif;
@@ -285,12 +286,26 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
                        : (size_t)c * kp.cstride + (size_t)((kp.R * 3 + 3) & ~3) + 4 * (size_t)c;
     return 4 * std::max(mainf + 4, smem_floats_stage(kp.R, kp.Bt, K));
   };
-  auto fit_tile = [&]() {
-    int c = (T.ct + 1) & ~1;  // even: the recurrence kernel takes components in pairs
+  auto fit_from = [&](int start) {
+    int c = (start + 1) & ~1;  // even: the recurrence kernel takes components in pairs
     while (c > 8 && need(c) > budget) c /= 2;
     return c;
   };
-  int ct = fit_tile();
+  // candidate tiles, preferred first: a requested tile shrunk to fit, or the
+  // planner's choice (160 components where shared memory holds them as they
+  // are: 1 % faster than 128 at configs 2 and 4; else 128 shrunk to fit)
+  auto candidates = [&]() {
+    std::vector<int> c;
+    if (T.ct > 0) {
+      c.push_back(fit_from(T.ct));
+    } else {
+      if (need(160) <= budget) c.push_back(160);
+      c.push_back(fit_from(128));
+    }
+    return c;
+  };
+  std::vector<int> cands = candidates();
+  int ct = cands[0];
   if (fspec || mixed) {
     // residual bound: the kernel's tile reference index is the midpoint of the
     // tile's first and last index (as floats, as the kernel forms it)
@@ -299,20 +314,31 @@ int plan_layout(const LayoutDesc& L, const ModelDesc& M, const ApplyDesc& A, con
       const double n = (double)(b.len - 1);
       quad = std::max(quad, std::fabs((double)b.l[0][2]) * n * n / 8.0);
     }
-    double spread = 0.0;
-    for (int c0 = 0; c0 < nIndexed; c0 += ct) {
-      const int nc = std::min(ct, nIndexed - c0);
-      const float at = 0.5f * (M.specIndex[c0] + M.specIndex[c0 + nc - 1]);
-      for (int c = c0; c < c0 + nc; c++)
-        spread = std::max(spread, std::fabs((double)M.specIndex[c] - (double)at));
+    auto bound_ok = [&](int tile) {
+      double spread = 0.0;
+      for (int c0 = 0; c0 < nIndexed; c0 += tile) {
+        const int nc = std::min(tile, nIndexed - c0);
+        const float at = 0.5f * (M.specIndex[c0] + M.specIndex[c0 + nc - 1]);
+        for (int c = c0; c < c0 + nc; c++)
+          spread = std::max(spread, std::fabs((double)M.specIndex[c] - (double)at));
+      }
+      return spread * quad <= kSpecResidualTol;
+    };
+    bool ok = false;
+    for (int c : cands) {  // the first candidate tile whose index spread meets the bound
+      if (bound_ok(c)) {
+        ct = c;
+        ok = true;
+        break;
+      }
     }
-    if (!(spread * quad <= kSpecResidualTol)) {
+    if (!ok) {
       if (mixed) {  // the caller rebuilds the plan from the unsplit table
         *err = "point sub-table fails the spectral-factored residual bound";
         return 4;
       }
       fspec = false;
-      ct = fit_tile();
+      ct = candidates()[0];
     }
   }
   plan->specFactored = fspec;

@@ -90,7 +90,9 @@ extern "C" int obit_dft_calc_noalloc(const GPUVisInfo* visInfo, const GPUModelIn
   if (rc) return failed(rc, err);
   if (nvis == 0 || mc.model.ncomp == 0) return OBIT_DFT_OK;
   Plan plan;
-  rc = plan_layout(L, mc.model, A, TuneDesc(), &plan, &err);
+  TuneDesc T;
+  T.ct = 128;  // the tile this entry point plans with (not the planner's 160 choice)
+  rc = plan_layout(L, mc.model, A, T, &plan, &err);
   if (rc) return failed(rc, err);
 
   // scratch layout: [error flag][channel-block table][padded component table]
