@@ -46,8 +46,8 @@ ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per
 # grows in proportion to records, so a launch's traffic is the figure times its
 # records.
 #   config1: dft_recur_kernel<32, 0> at 42,120 records (65.61 MB read + 13.73 MB written)
-#   config2: dft_recur_kernel<32, 1, ..., spectral-factored> at 10,080 records (499.44 MB read +
-#            443.81 MB written)
+#   config2: dft_recur_kernel<32, 1, ..., spectral-factored> at 10,080 records, 160-component tiles
+#            (500.25 MB read + 443.94 MB written)
 #   config3: dft_recur_kernel<32, 4, ..., mixed> at 4,032 records (202.13 MB read + 150.94 MB written)
 #   config4: dft_recur_kernel<32, 0> at 23,808 records (296.35 MB read + 240.85 MB written)
 #   config5: dft_recur_batch_kernel<32, 0> over the 96-facet draw at 189,029 records
@@ -56,7 +56,7 @@ ACCURACY = {"max_rel_err_bound": 1e-5, "metric": "|V - V_fp64| / sum_c |A_c| per
 #   grid:    grid_apply_kernel at 4,032 records (215.87 MB read + 144.40 MB written)
 NCU_DRAM_BYTES_PER_RECORD = {
     "config1": ((65.61e6 + 13.73e6) / 42120, "42,120-record capture (the whole configuration)"),
-    "config2": ((499.44e6 + 443.81e6) / 10080, "10,080-record capture"),
+    "config2": ((500.25e6 + 443.94e6) / 10080, "10,080-record capture (160-component tiles)"),
     "config3": ((202.13e6 + 150.94e6) / 4032, "4,032-record capture"),
     "config4": ((296.35e6 + 240.85e6) / 23808, "23,808-record capture"),
     "config5": ((3668.0e6 + 3567.0e6) / 189029, "189,029-record capture of the same facet draw"),
