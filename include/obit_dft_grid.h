@@ -76,7 +76,11 @@ int obit_dft_grid_create(const ObitDFTCCField *field, const ObitDFTGridImage *im
  * twice its size by pixel nx / 2, then transformed and interpolated as the
  * component model is (no taper).  field gives the image's geometry only
  * (crval, rotation, do3D, pixel offsets, cdelt, shifts, projection); its rows
- * are not read.  Primary-beam correction (doPBCor) is not applied. */
+ * are not read.  The reference's primary-beam correction of the image
+ * (doPBCor, ObitPBUtilImageCor) calls ObitPBUtilRelPB with its reference
+ * frequency and minimum gain swapped (ObitPBUtil.c:566 against
+ * ObitPBUtil.h:54-55), which clamps every gain to 1: the image is used as
+ * it is there too. */
 int obit_dft_grid_create_image(const float *pixels, float fblank, const ObitDFTCCField *field,
                                const ObitDFTGridImage *image, const ObitDFTCCModel *model, int kernel,
                                void *stream, ObitDFTGrid **out);
