@@ -41,6 +41,19 @@ int obit_dft_sub_uv(const ObitDFTCCField *fields, int nfield, const ObitDFTGridI
                     const ObitDFTCCModel *model, const ObitDFTSkyModel *sky, ObitDFTUVData *uv, int mode,
                     int measured, float maxGrid, int kernel, int *modeUsed, int *ncompUsed, ObitDFTErr *err);
 
+/* The same pass structure for image models (OBIT_SkyModel_Image, which the
+ * reference always grids: ObitSkyModelLoadImage, ObitSkyModel.c:1427-1428,
+ * 2163-2260): per field, in field order, the model image pixels[f]
+ * (images[f].nx x images[f].ny floats, square, row-major; host or device
+ * memory) with blanking value fblank, the field's geometry from fields[f]
+ * (its CC rows are not read), gridded and applied to uv->buffer with the
+ * operation and selection of `sky`.  *npixUsed (pixels gridded over the
+ * fields) is written when not NULL.  Returns 0 or a status code with the
+ * message in err. */
+int obit_dft_sub_uv_image(const float *const *pixels, float fblank, const ObitDFTCCField *fields, int nfield,
+                          const ObitDFTGridImage *images, const ObitDFTCCModel *model, const ObitDFTSkyModel *sky,
+                          ObitDFTUVData *uv, int kernel, long long *npixUsed, ObitDFTErr *err);
+
 #ifdef __cplusplus
 }
 #endif

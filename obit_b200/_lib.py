@@ -161,6 +161,10 @@ SIGNATURES = {
     "obit_dft_calc_device": (C.c_int, [_GPUINFO_P, C.c_void_p, C.c_int, C.c_void_p]),
     "obit_dft_plan_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
     "obit_dft_beam_info": (C.c_int, [_GPUINFO_P, C.POINTER(C.c_int), C.c_int]),
+    "obit_dft_sub_uv_image": (C.c_int, [C.POINTER(C.c_void_p), C.c_float, C.POINTER(ObitDFTCCField), C.c_int,
+                                        C.POINTER(ObitDFTGridImage), C.POINTER(ObitDFTCCModel),
+                                        C.POINTER(ObitDFTSkyModel), C.POINTER(ObitDFTUVData), C.c_int,
+                                        C.POINTER(C.c_longlong), C.POINTER(ObitDFTErr)]),
     "obit_dft_sub_uv": (C.c_int, [C.POINTER(ObitDFTCCField), C.c_int, C.POINTER(ObitDFTGridImage),
                                   C.POINTER(ObitDFTCCModel), C.POINTER(ObitDFTSkyModel),
                                   C.POINTER(ObitDFTUVData), C.c_int, C.c_int, C.c_float, C.c_int,

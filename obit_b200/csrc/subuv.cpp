@@ -88,13 +88,14 @@ int grid_descriptor(const ObitDFTSkyModel* sky, ObitDFTUVData* uv, Mirror* in, c
   return OBIT_DFT_OK;
 }
 
-// One gridded pass of a field (components of at most maxGrid); *nrow
-// receives the rows gridded.
+// One gridded pass of a field: its components of at most maxGrid, or, with
+// pixels, its model image; *nrow receives the rows (pixels) gridded.
 int grid_pass(const ObitDFTCCField* field, const ObitDFTGridImage* image, const ObitDFTCCModel* model,
               float maxGrid, int kernel, const GPUVisInfo* vi, const ObitDFTSkyModel* sky, ObitDFTUVData* uv,
-              long long* nrow, ObitDFTErr* err) {
+              long long* nrow, ObitDFTErr* err, const float* pixels = nullptr, float fblank = 0.0f) {
   ObitDFTGrid* raw = nullptr;
-  int rc = obit_dft_grid_create(field, image, model, maxGrid, kernel, nullptr, &raw);
+  int rc = pixels ? obit_dft_grid_create_image(pixels, fblank, field, image, model, kernel, nullptr, &raw)
+                  : obit_dft_grid_create(field, image, model, maxGrid, kernel, nullptr, &raw);
   if (rc) return lib_err(err, rc, "gridded field");
   std::unique_ptr<ObitDFTGrid, GridDeleter> grid(raw);
   long long info[1] = {0};
@@ -168,5 +169,29 @@ extern "C" int obit_dft_sub_uv(const ObitDFTCCField* fields, int nfield, const O
     total += n;
   }
   if (ncompUsed) *ncompUsed = (int)total;
+  return OBIT_DFT_OK;
+}
+
+extern "C" int obit_dft_sub_uv_image(const float* const* pixels, float fblank, const ObitDFTCCField* fields,
+                                     int nfield, const ObitDFTGridImage* images, const ObitDFTCCModel* model,
+                                     const ObitDFTSkyModel* sky, ObitDFTUVData* uv, int kernel,
+                                     long long* npixUsed, ObitDFTErr* err) {
+  if (!pixels || !fields || !images || nfield < 1 || !model || !sky || !uv || !uv->buffer)
+    return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv_image: NULL argument or no fields");
+  if (npixUsed) *npixUsed = 0;
+  for (int f = 0; f < nfield; f++)
+    if (!pixels[f]) return set_err(err, OBIT_DFT_EBADARG, "obit_dft_sub_uv_image: field %d has no pixels", f);
+  if (uv->numVisBuff <= 0) return OBIT_DFT_OK;
+  Mirror in;
+  const GPUVisInfo* vi = nullptr;
+  if (int rc = grid_descriptor(sky, uv, &in, &vi, err)) return rc;
+  long long total = 0;
+  for (int f = 0; f < nfield; f++) {  // a pass per field, in field order
+    long long n = 0;
+    if (int rc = grid_pass(&fields[f], &images[f], model, 1e20f, kernel, vi, sky, uv, &n, err, pixels[f], fblank))
+      return rc;
+    total += n;
+  }
+  if (npixUsed) *npixUsed = total;
   return OBIT_DFT_OK;
 }

@@ -77,3 +77,40 @@ def sub_uv(uv: UVData, fields: list[CCField], images: list[GR.GridImage], model:
     if rc:
         raise _lib.DFTError(rc, err.message.decode(errors="replace"))
     return SubUVResult(out, used.value, ncomp.value)
+
+
+def sub_uv_image(uv: UVData, pixels: list, fblank: float, fields: list[CCField], images: list[GR.GridImage],
+                 model: CCModel, params: SkyModelParams | None = None,
+                 kernel: int = GR.KERNEL_REFERENCE) -> SubUVResult:
+    """The pass structure for image models (obit_dft_sub_uv_image): per field
+    the model image pixels[f] ((ny, nx) float32; fields[f] gives the geometry
+    only) gridded and applied to a copy of uv's records.  ncomp of the result
+    counts the pixels gridded."""
+    import numpy as np
+
+    p = params or SkyModelParams()
+    if not (len(pixels) == len(fields) == len(images)):
+        raise ValueError("one image per field")
+    lib = _lib.load()
+    keep: list = []
+    out = uv.copy()
+    arr = _field_array(fields, keep)
+    imgs = (ObitDFTGridImage * max(1, len(images)))()
+    pix = (C.c_void_p * max(1, len(pixels)))()
+    for i, (im, px) in enumerate(zip(images, pixels)):
+        imgs[i] = ObitDFTGridImage(int(im.nx), int(im.ny), float(im.crpixX), float(im.crpixY))
+        a = np.ascontiguousarray(px, dtype=np.float32)
+        if a.shape != (im.ny, im.nx):
+            raise ValueError("pixels must be (ny, nx)")
+        keep.append(a)
+        pix[i] = a.ctypes.data
+    m = _model(model)
+    s = _sky_fields(p, out)
+    d = uv_struct(out, True, False, keep)
+    n = C.c_longlong()
+    err = ObitDFTErr()
+    rc = lib.obit_dft_sub_uv_image(pix, float(fblank), arr, len(fields), imgs, C.byref(m), C.byref(s), C.byref(d),
+                                   int(kernel), C.byref(n), C.byref(err))
+    if rc:
+        raise _lib.DFTError(rc, err.message.decode(errors="replace"))
+    return SubUVResult(out, GR.MODE_GRID, n.value)

@@ -75,3 +75,36 @@ def test_mixed_dft_above_min_then_grid():
     b = want[:, uv.nrparm:].reshape(uv.vis_view().shape)[..., :2, :]
     d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1])) / l1[..., None]
     assert float(d.max()) < 1e-5, float(d.max())
+
+
+def test_image_models_one_pass_per_field():
+    """OBIT_SkyModel_Image through the pass structure (obit_dft_sub_uv_image):
+    two fields' model images (clipped, blanked, scaled by factor) applied in
+    field order give the oracle's image model of each, subtracted in turn."""
+    import oracle_grid as G
+    from obit_b200.comps import CCModel
+    from obit_b200.subuv import sub_uv_image
+    from test_grid_gpu import _image_of
+    f1, img1, m, uv = field_case(N=96, seed=70, nint=5)
+    f2, img2, _, _ = field_case(N=96, seed=71, nint=5, shift3d=True)
+    m.do3D = True
+    pix = [_image_of(f1, img1), _image_of(f2, img2)]
+    pix[0][10, 12] = -999.0
+    pix[1][40:44, 50:52] = 0.7
+    m2 = CCModel(**{**m.__dict__, "factor": 0.5})
+    p = SkyModelParams(op=OP_SUB)
+    gims = [GR.GridImage(i.nx, i.ny, i.crpixX, i.crpixY) for i in (img1, img2)]
+    r = sub_uv_image(uv, pix, -999.0, [f1, f2], gims, m2, p)
+    assert r.ncomp == 2 * 96 * 96
+    want = uv
+    l1 = 0.0
+    for px, f, img in zip(pix, (f1, f2), (img1, img2)):
+        gm = G.build_image(px, -999.0, f, img, m2)
+        l1 += gm.l1
+        nxt = want.copy()
+        nxt.vis = G.apply(gm, want, p)
+        want = nxt
+    a = r.uv.vis[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    b = want.vis[:, uv.nrparm:].reshape(uv.vis_view().shape)
+    d = np.abs((a[..., 0] - b[..., 0]) + 1j * (a[..., 1] - b[..., 1]))
+    assert float(d.max()) / l1 < 1e-5, float(d.max()) / l1
