@@ -247,13 +247,16 @@ typedef struct ObitDFTBeamImages {
   const float *pixels;   /* device: [numAntType][8][nplane][ny][nx] */
   float fblank;          /* value of blanked pixels */
   int hwidth;            /* Lagrange interpolation half-width, 1..4 (2 hwidth + 1 taps per axis) */
-  int projection;        /* 0: linear offsets, 1: -SIN about crval */
+  int projection;        /* 0: linear offsets; about crval 1 -SIN, 2 -TAN, 3 -ARC, 4 -NCP,
+                            5 -GLS, 6 -MER, 7 -AIT, 8 -STG (CUDASkyGeom.h:91-250) */
   double crval[2];       /* reference position of the grid (deg) */
   float crpix[2];        /* reference pixel (1-relative) */
   float cdelt[2];        /* pixel increments (deg) */
   const float *planeFreq;/* host [nplane]: frequency (Hz) of each plane */
   float refSizeFact;     /* primary-beam factor of InvBeam (ObitCUDABeamModel.cu:66-72):
                             antenna size x 1.052 x DG2RAD / VELIGHT, per Hz per degree */
+  float crota;           /* rotation of the grid's y axis (deg, CROTA2); enters the -MER and
+                            -AIT scale factors only, as in CUDAPositionXYpixLM */
 } ObitDFTBeamImages;
 
 /* Fill a Jones table in the layout of ObitDFTBeam.jones ([numAntType][ncomp]

@@ -130,7 +130,7 @@ class ObitDFTBeamImages(C.Structure):
         ("numAntType", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nplane", C.c_int),
         ("pixels", C.c_void_p), ("fblank", C.c_float), ("hwidth", C.c_int), ("projection", C.c_int),
         ("crval", C.c_double * 2), ("crpix", C.c_float * 2), ("cdelt", C.c_float * 2),
-        ("planeFreq", C.POINTER(C.c_float)), ("refSizeFact", C.c_float),
+        ("planeFreq", C.POINTER(C.c_float)), ("refSizeFact", C.c_float), ("crota", C.c_float),
     ]
 
 

@@ -67,10 +67,11 @@ class BeamImages:
     crval: tuple = (0.0, 0.0)
     crpix: tuple = (1.0, 1.0)
     cdelt: tuple = (1.0, 1.0)
-    projection: int = 0            # 0 linear offsets, 1 -SIN
+    projection: int = 0            # 0 linear; 1..8 -SIN -TAN -ARC -NCP -GLS -MER -AIT -STG
     hwidth: int = 2
     fblank: float = -3.0e38
     refSizeFact: float = 0.0
+    crota: float = 0.0             # y-axis rotation (deg; -MER and -AIT scales)
     _keep: list = field(default_factory=list, repr=False)
 
     def descriptor(self, d_pixels: int) -> _lib.ObitDFTBeamImages:
@@ -80,7 +81,8 @@ class BeamImages:
         return _lib.ObitDFTBeamImages(ntype, nx, ny, nplane, C.c_void_p(d_pixels), float(self.fblank),
                                       int(self.hwidth), int(self.projection), (C.c_double * 2)(*self.crval),
                                       (C.c_float * 2)(*self.crpix), (C.c_float * 2)(*self.cdelt),
-                                      pf.ctypes.data_as(C.POINTER(C.c_float)), float(self.refSizeFact))
+                                      pf.ctypes.data_as(C.POINTER(C.c_float)), float(self.refSizeFact),
+                                      float(self.crota))
 
 
 def jones_from_images(images: BeamImages, d_pixels: int, d_pos: int, ncomp: int, par_ang: float,

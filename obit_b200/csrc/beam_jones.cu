@@ -1,7 +1,7 @@
 // Jones matrices of every (antenna type, component, beam plane) interpolated
 // from beam images: the computation of GetJonesKernel
 // (ObitCUDABeamModel.cu:1228-1299) with its pixel geometry (CUDAPositionXYpix,
-// CUDASkyGeom.h:91-286; linear and -SIN grids) and Lagrange interpolator
+// CUDASkyGeom.h:91-286; linear grids and the eight projections) and Lagrange interpolator
 // (CUDABeamInterpPixel / SetConvKernal, CUDABeamInterp.h), written anew.
 // One thread per (component, antenna type); the position, its pixel, the
 // interpolation kernels and the primary-beam factor's offset are computed
@@ -22,7 +22,7 @@ constexpr int kMaxTaps = 9;  // 2 hwidth + 1, hwidth <= 4
 
 struct JonesParams {
   int numAntType, nx, ny, nplane, ncomp, hwidth, projection;
-  float fblank, refSizeFact, parAng;
+  float fblank, refSizeFact, parAng, crota;
   double crval0, crval1;
   float crpix0, crpix1, cdelt0, cdelt1;
   const float* pixels;
@@ -32,24 +32,115 @@ struct JonesParams {
 };
 constexpr int kMaxPlanes = 64;
 
-// Pixel (1-relative) of a position (deg), or false when it cannot be
-// projected: CUDAPositionXYpixLM (linear: offsets from crval with the 0 h
-// wrap; -SIN: direction cosines about crval), then the rotation by parAng
-// and the grid's increments and reference pixel (CUDAPositionXYpix).
-__device__ bool pixel_of(const JonesParams& p, double x, double y, float& px, float& py) {
-  const double d2r = 1.745329252e-2;
-  double dx = x - p.crval0;
+// Offsets (deg) of a position (deg) from the grid's reference position in
+// the grid's projection, or false where it cannot be projected: the linear
+// offsets after the 0 h wrap, or for projections 1..8 (-SIN, -TAN, -ARC,
+// -NCP, -GLS, -MER, -AIT, -STG) the projected coordinates of the standard
+// AIPS definitions scaled back to degrees, as CUDAPositionXYpixLM
+// (CUDASkyGeom.h:91-250) forms them; crota (deg) enters only the -MER and
+// -AIT scale factors.
+__device__ bool grid_offsets(const JonesParams& p, double x, double y, double& l, double& m) {
+  const double d2r = 1.745329252e-2, halfPi = 6.28318530717959 / 4.0, eps = 1.0e-5;
+  const double dx = x - p.crval0;
   if (dx > 180.0) x -= 360.0;
   if (dx < -180.0) x += 360.0;
-  double l = x - p.crval0, m = y - p.crval1;
-  if (p.projection == 1) {
-    const double ra0 = p.crval0 * d2r, dec0 = p.crval1 * d2r, ra = x * d2r, dec = y * d2r;
-    const double cd = cos(dec), sd = sin(dec), ca = cos(ra - ra0);
-    const double sint = sd * sin(dec0) + cd * cos(dec0) * ca;
-    if (sint < 0.0) return false;
-    l = sin(ra - ra0) * cd / d2r;
-    m = (sd * cos(dec0) - cd * sin(dec0) * ca) / d2r;
+  l = x - p.crval0;
+  m = y - p.crval1;
+  if (p.projection == 0) return true;
+  const double ra0 = p.crval0 * d2r, dec0 = p.crval1 * d2r, ra = x * d2r, dec = y * d2r;
+  const double cd = cos(dec), sd = sin(dec), cd0 = cos(dec0), sd0 = sin(dec0);
+  const double da = ra - ra0, ca = cos(da);
+  const double cosAlt = sd * sd0 + cd * cd0 * ca;  // cosine of the angle from the reference
+  const double mNorth = sd * cd0 - cd * sd0 * ca;   // north component of the direction
+  double L = sin(da) * cd, M = 0.0;
+  switch (p.projection) {
+    case 1:  // -SIN: orthographic
+      if (cosAlt < 0.0) return false;
+      M = mNorth;
+      break;
+    case 2:  // -TAN: gnomonic
+      if (cosAlt <= 0.0) return false;
+      L /= cosAlt;
+      M = mNorth / cosAlt;
+      break;
+    case 3: {  // -ARC: zenithal equidistant
+      const double th = acos(fmin(1.0, fmax(-1.0, cosAlt)));
+      const double f = th != 0.0 ? th / sin(th) : 1.0;
+      L *= f;
+      M = mNorth * f;
+      break;
+    }
+    case 4:  // -NCP: north celestial pole
+      if (dec0 == 0.0) return false;
+      M = (cd0 - cd * ca) / sd0;
+      break;
+    case 5:  // -GLS: global sinusoid
+      if (fabs(dec) > halfPi || fabs(dec0) > halfPi) return false;
+      L = da * cd;
+      M = dec - dec0;
+      break;
+    case 6: {  // -MER: Mercator, scaled to the grid's increment along y
+      const double r = p.crota * d2r;
+      double step = p.cdelt1 * cos(r) + p.cdelt0 * sin(r);
+      if (step == 0.0) step = 1.0;
+      const double y0 = (p.crval1 / 2.0 + 45.0) * d2r;
+      const double ly0 = log(tan(y0)), ly1 = log(tan(y0 + step / 2.0 * d2r));
+      const double gy = step * d2r / (ly1 - ly0);
+      double gx = cos(p.crval1 * d2r);
+      if (gx <= 0.0) gx = 1.0;
+      const double t = tan(dec / 2.0 + halfPi / 2.0);
+      if (t < eps) return false;
+      L = gx * da;
+      M = gy * log(t) - gy * ly0;
+      break;
+    }
+    case 7: {  // -AIT: Hammer-Aitoff, scaled to the grid's increments
+      const double half = da / 2.0;
+      if (fabs(half) > halfPi) return false;
+      const double r = p.crota * d2r, cr = cos(r), sr = sin(r);
+      const double yc = p.crval1 * d2r;
+      double sy = p.cdelt1 * cr + p.cdelt0 * sr;
+      if (sy == 0.0) sy = 1.0;
+      sy *= d2r;
+      double ny = sin(yc + sy) / sqrt((1.0 + cos(yc + sy)) / 2.0) - sin(yc) / sqrt((1.0 + cos(yc)) / 2.0);
+      if (ny == 0.0) ny = 1.0;
+      const double gy = sy / ny;
+      double sx = p.cdelt0 * cr - p.cdelt1 * sr;
+      if (sx == 0.0) sx = 1.0;
+      sx *= d2r;
+      double nx = 2.0 * cos(yc) * sin(sx / 2.0);
+      if (nx == 0.0) nx = 1.0;
+      const double gx = sx * sqrt((1.0 + cos(yc) * cos(sx / 2.0)) / 2.0) / nx;
+      const double y0 = gy * sin(yc) / sqrt((1.0 + cos(yc)) / 2.0);
+      const double z = sqrt((1.0 + cd * cos(half)) / 2.0);
+      if (fabs(z) < eps) return false;
+      L = 2.0 * gx * cd * sin(half) / z;
+      M = gy * sd / z - y0;
+      break;
+    }
+    case 8: {  // -STG: stereographic
+      if (fabs(dec) > halfPi) return false;
+      const double den = 1.0 + cosAlt;
+      if (fabs(den) < eps) return false;
+      L *= 2.0 / den;
+      M = mNorth * 2.0 / den;
+      break;
+    }
+    default:
+      return false;
   }
+  l = L / d2r;
+  m = M / d2r;
+  return true;
+}
+
+// Pixel (1-relative) of a position (deg), or false when it cannot be
+// projected: the grid offsets rotated by the parallactic angle, then the
+// grid's increments and reference pixel (CUDAPositionXYpix,
+// CUDASkyGeom.h:266-286).
+__device__ bool pixel_of(const JonesParams& p, double x, double y, float& px, float& py) {
+  double l, m;
+  if (!grid_offsets(p, x, y, l, m)) return false;
   float sr, cr;
   sincosf(p.parAng, &sr, &cr);
   const double lr = l * cr + m * sr;
@@ -165,7 +256,7 @@ extern "C" int obit_dft_beam_jones(const ObitDFTBeamImages* im, const float* pos
   if (im->hwidth < 1 || im->hwidth > 4) return bad(OBIT_DFT_EBADARG, "interpolation half-width must be 1..4");
   if (im->nx < 2 * im->hwidth + 1 || im->ny < 2 * im->hwidth + 1)
     return bad(OBIT_DFT_EBADARG, "beam images smaller than the interpolation kernel");
-  if (im->projection != 0 && im->projection != 1) return bad(OBIT_DFT_EUNSUPPORTED, "projection must be 0 or 1");
+  if (im->projection < 0 || im->projection > 8) return bad(OBIT_DFT_EUNSUPPORTED, "projection must be 0..8");
   if (!(im->cdelt[0] != 0.0f) || !(im->cdelt[1] != 0.0f)) return bad(OBIT_DFT_EBADARG, "zero pixel increment");
   if (((uintptr_t)jones & 15u) != 0) return bad(OBIT_DFT_EBADARG, "Jones table not 16-byte aligned");
   if (ncomp == 0) return OBIT_DFT_OK;
@@ -186,6 +277,7 @@ extern "C" int obit_dft_beam_jones(const ObitDFTBeamImages* im, const float* pos
   p.crpix1 = im->crpix[1];
   p.cdelt0 = im->cdelt[0];
   p.cdelt1 = im->cdelt[1];
+  p.crota = im->crota;
   p.pixels = im->pixels;
   p.pos = pos;
   p.jones = jones;

@@ -300,6 +300,7 @@ def beam_jones_fp64(images, pos, par_ang: float):
     lib.oracle_beam_jones.restype = None
     lib.oracle_beam_jones(ntype, nx, ny, nplane, _p(px, C.c_float), C.c_float(images.fblank),
                           int(images.hwidth), int(images.projection), d3(*images.crval), d3(*images.crpix),
-                          d3(*images.cdelt), _p(pf, C.c_double), C.c_double(images.refSizeFact),
+                          d3(*images.cdelt), C.c_double(images.crota), _p(pf, C.c_double),
+                          C.c_double(images.refSizeFact),
                           C.c_double(par_ang), _p(pos, C.c_float), pos.shape[0], _p(out, C.c_float))
     return out

@@ -233,10 +233,98 @@ int oracle_beam_apply(const OracleJob *j, const OracleBeam *b, float *vis, doubl
   return 0;
 }
 
+/* Grid offsets (deg) of position (x, y) (deg) in projection proj (0 linear,
+ * 1..8 -SIN -TAN -ARC -NCP -GLS -MER -AIT -STG) about crval, as
+ * CUDAPositionXYpixLM (ObitSystem/Obit/include/CUDASkyGeom.h:91-250) defines
+ * them; returns 0 where the position cannot be projected.  The zenithal
+ * projections are written here through the angle theta from the reference
+ * and their radial functions (sin, tan, theta, 2 tan(theta / 2)); the others
+ * follow the AIPS definitions, with the grid-scaled -MER and -AIT factors. */
+static int grid_offsets(int proj, const double crval[2], const double cdelt[2], double crota, double x,
+                        double y, double *lo, double *mo) {
+  const double d2r = 1.745329252e-2, halfPi = 6.28318530717959 / 4.0;
+  const double dx = x - crval[0];
+  if (dx > 180.0) x -= 360.0;
+  if (dx < -180.0) x += 360.0;
+  *lo = x - crval[0];
+  *mo = y - crval[1];
+  if (proj == 0) return 1;
+  const double a0 = crval[0] * d2r, d0 = crval[1] * d2r, a = x * d2r, d = y * d2r;
+  const double east = sin(a - a0) * cos(d);
+  const double north = sin(d) * cos(d0) - cos(d) * sin(d0) * cos(a - a0);
+  const double ct = sin(d) * sin(d0) + cos(d) * cos(d0) * cos(a - a0);
+  double L, M;
+  if (proj == 1 || proj == 2 || proj == 3 || proj == 8) {
+    if (proj == 1 && ct < 0.0) return 0;
+    if (proj == 2 && ct <= 0.0) return 0;
+    if (proj == 8 && (fabs(d) > halfPi || fabs(1.0 + ct) < 1.0e-5)) return 0;
+    const double st = sqrt(east * east + north * north);
+    const double th = atan2(st, ct);
+    double R;
+    if (proj == 1) R = sin(th);
+    else if (proj == 2) R = tan(th);
+    else if (proj == 3) R = th;
+    else R = 2.0 * tan(th / 2.0);
+    const double f = st > 1e-12 ? R / st : 1.0; /* R(theta) / sin(theta) */
+    L = east * f;
+    M = north * f;
+  } else if (proj == 4) {
+    if (d0 == 0.0) return 0;
+    L = east;
+    M = (cos(d0) - cos(d) * cos(a - a0)) / sin(d0);
+  } else if (proj == 5) {
+    if (fabs(d) > halfPi || fabs(d0) > halfPi) return 0;
+    L = (a - a0) * cos(d);
+    M = d - d0;
+  } else if (proj == 6) {
+    const double rot = crota * d2r;
+    double dy = cdelt[1] * cos(rot) + cdelt[0] * sin(rot);
+    if (dy == 0.0) dy = 1.0;
+    const double q0 = log(tan((crval[1] / 2.0 + 45.0) * d2r));
+    const double q1 = log(tan((crval[1] / 2.0 + 45.0) * d2r + dy / 2.0 * d2r));
+    const double gy = dy * d2r / (q1 - q0);
+    double gx = cos(crval[1] * d2r);
+    if (gx <= 0.0) gx = 1.0;
+    const double t = tan(d / 2.0 + halfPi / 2.0);
+    if (t < 1.0e-5) return 0;
+    L = gx * (a - a0);
+    M = gy * (log(t) - q0);
+  } else if (proj == 7) {
+    const double h = (a - a0) / 2.0;
+    if (fabs(h) > halfPi) return 0;
+    const double rot = crota * d2r;
+    double sy = (cdelt[1] * cos(rot) + cdelt[0] * sin(rot));
+    if (sy == 0.0) sy = 1.0;
+    sy *= d2r;
+    double sx = (cdelt[0] * cos(rot) - cdelt[1] * sin(rot));
+    if (sx == 0.0) sx = 1.0;
+    sx *= d2r;
+    /* Hammer-Aitoff y(dec) at the reference declination, normalised so that
+       one increment along each axis is one increment of the grid */
+#define HA_Y(dec) (sin(dec) / sqrt((1.0 + cos(dec)) / 2.0))
+    double ny = HA_Y(d0 + sy) - HA_Y(d0);
+    if (ny == 0.0) ny = 1.0;
+    double nx = 2.0 * cos(d0) * sin(sx / 2.0);
+    if (nx == 0.0) nx = 1.0;
+    const double gy = sy / ny;
+    const double gx = sx * sqrt((1.0 + cos(d0) * cos(sx / 2.0)) / 2.0) / nx;
+    const double z = sqrt((1.0 + cos(d) * cos(h)) / 2.0);
+    if (fabs(z) < 1.0e-5) return 0;
+    L = 2.0 * gx * cos(d) * sin(h) / z;
+    M = gy * (sin(d) / z - HA_Y(d0));
+#undef HA_Y
+  } else {
+    return 0;
+  }
+  *lo = L / d2r;
+  *mo = M / d2r;
+  return 1;
+}
+
 /* Jones table from beam images, FP64 (test infrastructure): the computation of
  * GetJonesKernel (ObitSystem/Obit/src/ObitCUDABeamModel.cu:1228-1299) with
- * CUDAPositionXYpix (ObitSystem/Obit/include/CUDASkyGeom.h:91-286, linear and
- * -SIN grids), the Lagrange interpolator of CUDABeamInterpPixel /
+ * CUDAPositionXYpix (ObitSystem/Obit/include/CUDASkyGeom.h:91-286, linear grids
+ * and the eight projections of grid_offsets), the Lagrange interpolator of CUDABeamInterpPixel /
  * SetConvKernal (ObitSystem/Obit/include/CUDABeamInterp.h) and InvBeam
  * (ObitCUDABeamModel.cu:66-72), with the unit matrix where the position is
  * off the grid, the gain factor is 10 or more, a parallel hand's real part
@@ -245,7 +333,7 @@ int oracle_beam_apply(const OracleJob *j, const OracleBeam *b, float *vis, doubl
  * jones out: [ntype][ncomp][nplane][8] (XX = P1, XY = X1, YX = X2, YY = P2). */
 void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixels, float fblank,
                        int hwidth, int projection, const double crval[2], const double crpix[2],
-                       const double cdelt[2], const double *planeFreq, double refSizeFact,
+                       const double cdelt[2], double crota, const double *planeFreq, double refSizeFact,
                        double parAng, const float *pos, int ncomp, float *jones) {
   const double d2r = 1.745329252e-2;
   const int iwid = 2 * hwidth + 1;
@@ -254,18 +342,8 @@ void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixel
     for (int c = 0; c < ncomp; c++) {
       float *Jc = jones + ((size_t)t * ncomp + c) * nplane * 8;
       double x = pos[2 * c], y = pos[2 * c + 1];
-      int ok = 1;
-      const double dx = x - crval[0];
-      if (dx > 180.0) x -= 360.0;
-      if (dx < -180.0) x += 360.0;
-      double l = x - crval[0], m = y - crval[1];
-      if (projection == 1) {
-        const double ra0 = crval[0] * d2r, dec0 = crval[1] * d2r, ra = x * d2r, dec = y * d2r;
-        const double sint = sin(dec) * sin(dec0) + cos(dec) * cos(dec0) * cos(ra - ra0);
-        if (sint < 0.0) ok = 0;
-        l = sin(ra - ra0) * cos(dec) / d2r;
-        m = (sin(dec) * cos(dec0) - cos(dec) * sin(dec0) * cos(ra - ra0)) / d2r;
-      }
+      double l, m;
+      const int ok = grid_offsets(projection, crval, cdelt, crota, x, y, &l, &m);
       const double lr = l * cos(parAng) + m * sin(parAng), mr = m * cos(parAng) - l * sin(parAng);
       const double px = lr / cdelt[0] + crpix[0], py = mr / cdelt[1] + crpix[1];
       if (!ok || px < 1.0 || px > nx || py < 1.0 || py > ny) {

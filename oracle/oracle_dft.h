@@ -110,7 +110,7 @@ typedef struct OracleBeam {
  * components of |amp| |coefficient|.  Returns 0, or < 0 for a bad job. */
 void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixels, float fblank,
                        int hwidth, int projection, const double crval[2], const double crpix[2],
-                       const double cdelt[2], const double *planeFreq, double refSizeFact,
+                       const double cdelt[2], double crota, const double *planeFreq, double refSizeFact,
                        double parAng, const float *pos, int ncomp, float *jones);
 int oracle_beam_apply(const OracleJob *job, const OracleBeam *beam, float *vis, double *l1,
                       int nthreads);

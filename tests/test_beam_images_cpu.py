@@ -66,3 +66,74 @@ def test_primary_beam_factor():
     arg = 2.0e-10 * 1.4e9 * 0.5
     g = (1 - 4 * arg * arg) / np.cos(np.pi * arg)
     assert abs(J[0, 0, 0, 0] - g * 0.9) < 1e-5
+
+
+def _lookup_pixel(im, pos, par=0.0):
+    """Pixel (1-relative) the oracle looks up for each position: P1 re and im
+    of the images are 0.001 x and 0.001 y, which the interpolator reproduces."""
+    J = oracle.beam_jones_fp64(im, np.asarray(pos, np.float32), par)
+    return J[0, :, 0, 0] / 0.001, J[0, :, 0, 1] / 0.001
+
+
+def _ramp_images(projection, crval, cdelt=(0.01, 0.01), n=201, crota=0.0):
+    f = lambda x, y, t, q, k: 0.001 * x if q == 0 else (0.001 * y if q == 1 else 0.0)  # noqa: E731
+    im = images(ntype=1, n=n, nplane=1, projection=projection, fn=f)
+    im.crval, im.cdelt, im.crota = crval, cdelt, crota
+    return im
+
+
+def test_projections_known_answers():
+    """Known answers of each projection (CUDASkyGeom.h:91-250) for a position
+    theta north of the reference and one east of it: -SIN sin(theta),
+    -TAN tan(theta), -ARC theta, -STG 2 tan(theta / 2), -NCP and -GLS their
+    defining formulas; -MER and -AIT are scaled so that one increment of
+    declination (and of right ascension, -AIT) at the reference is one pixel."""
+    d2r = 1.745329252e-2
+    ra0, dec0, th = 30.0, 40.0, 0.6  # theta in deg
+    cen = 101.0
+    radial = {1: np.sin, 2: np.tan, 3: lambda a: a, 8: lambda a: 2 * np.tan(a / 2)}
+    for proj, R in radial.items():
+        im = _ramp_images(proj, (ra0, dec0))
+        px, py = _lookup_pixel(im, [[ra0, dec0 + th]])
+        assert abs(px[0] - cen) < 2e-3
+        assert abs(py[0] - (cen + R(th * d2r) / d2r / 0.01)) < 2e-3, proj
+    # -NCP: (cos d0 - cos d cos da) / sin d0 north, sin(da) cos d east
+    im = _ramp_images(4, (ra0, dec0))
+    da, dec = 0.5, 40.3
+    px, py = _lookup_pixel(im, [[ra0 + da, dec]])
+    d, d0, a = dec * d2r, dec0 * d2r, da * d2r
+    assert abs(px[0] - (cen + np.sin(a) * np.cos(d) / d2r / 0.01)) < 2e-3
+    assert abs(py[0] - (cen + (np.cos(d0) - np.cos(d) * np.cos(a)) / np.sin(d0) / d2r / 0.01)) < 2e-3
+    # -GLS: da cos(dec) east, dec - dec0 north
+    im = _ramp_images(5, (ra0, dec0))
+    px, py = _lookup_pixel(im, [[ra0 + da, dec]])
+    assert abs(px[0] - (cen + da * np.cos(d) / 0.01)) < 2e-3
+    assert abs(py[0] - (cen + 0.3 / 0.01)) < 2e-3
+    # -MER and -AIT: one increment north (and east for -AIT) is one pixel
+    for proj in (6, 7):
+        im = _ramp_images(proj, (ra0, dec0), cdelt=(0.02, 0.02))
+        px, py = _lookup_pixel(im, [[ra0, dec0], [ra0, dec0 + 0.02], [ra0, dec0 + 0.2]])
+        assert abs(px[0] - cen) < 2e-3 and abs(py[0] - cen) < 2e-3
+        assert abs(py[1] - (cen + 1)) < 2e-3, proj
+        assert 9.5 < py[2] - cen < 10.5
+    im = _ramp_images(7, (ra0, dec0), cdelt=(0.02, 0.02))
+    px, py = _lookup_pixel(im, [[ra0 + 0.02, dec0]])
+    assert abs(px[0] - (cen + 1)) < 2e-3
+
+
+def test_projections_limits_give_unit():
+    """Positions a projection cannot place give the unit matrix: -SIN past 90
+    degrees from the reference, -TAN at 90 degrees, -NCP about an equatorial
+    reference; all projections agree with the linear offsets near the
+    reference on the equator."""
+    unit = np.array([1, 0, 0, 0, 0, 0, 1, 0], np.float32)
+    for proj, crval, pos in ((1, (0.0, 0.0), [0.0, 91.0]), (2, (0.0, 0.0), [90.0, 0.0]), (4, (10.0, 0.0), [10.0, 0.1])):
+        im = _ramp_images(proj, crval, cdelt=(1.0, 1.0))
+        J = oracle.beam_jones_fp64(im, np.array([pos], np.float32), 0.0)
+        np.testing.assert_array_equal(J[0, 0, 0], unit)
+    for proj in range(9):
+        if proj == 4:
+            continue
+        im = _ramp_images(proj, (0.0, 0.0))
+        px, py = _lookup_pixel(im, [[0.05, -0.03]])
+        assert abs(px[0] - 106.0) < 2e-3 and abs(py[0] - 98.0) < 2e-3, proj

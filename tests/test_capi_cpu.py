@@ -84,6 +84,7 @@ def test_c_header_layout_matches_bindings(tmp_path):
         "GPUVisInfo": [f[0] for f in _lib.GPUVisInfo._fields_],
         "GPUModelInfo": [f[0] for f in _lib.GPUModelInfo._fields_],
         "GPUInfo": [f[0] for f in _lib.GPUInfo._fields_],
+        "ObitDFTBeamImages": [f[0] for f in _lib.ObitDFTBeamImages._fields_],
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "obit_dft.h"', "int main(void){"]
     lines.append('printf("{");')
@@ -101,7 +102,7 @@ def test_c_header_layout_matches_bindings(tmp_path):
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = json.loads(subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout)
     for s, cls in (("GPUVisInfo", _lib.GPUVisInfo), ("GPUModelInfo", _lib.GPUModelInfo),
-                   ("GPUInfo", _lib.GPUInfo)):
+                   ("GPUInfo", _lib.GPUInfo), ("ObitDFTBeamImages", _lib.ObitDFTBeamImages)):
         assert got[s]["sizeof"] == C.sizeof(cls)
         for f, off in got[s]["offsets"].items():
             assert getattr(cls, f).offset == off
