@@ -21,6 +21,7 @@ HERE = Path(__file__).resolve().parent
 LIB_A = HERE / "liboracle_dft.so"
 LIB_B = HERE / "_ref" / "libobit_refcpu.so"
 LIB_J = HERE / "_ref" / "libobit_refjones.so"
+LIB_G = HERE / "_ref" / "libobit_refgeom.so"
 
 
 class OracleJob(C.Structure):
@@ -273,6 +274,23 @@ def ref_jones_cor1(stok: int, flux: float, sin_ph: float, cos_ph: float, J1, J2,
         raise ValueError(f"ref_jones_cor1 returned {rc}")
     o = out.astype(np.float64)
     return o[0::2] + 1j * o[1::2]
+
+
+def have_refgeom() -> bool:
+    return LIB_G.exists()
+
+
+def ref_position_xypix(coord, ctype: str, crval, crpix, cdelt, crota=(0.0, 0.0), rotar: float = 0.0):
+    """The reference's own CUDAPositionXYpix (compiled for the host): the
+    1-relative pixel of position coord (deg) and the reference's status
+    (0 placed, else not)."""
+    lib = C.CDLL(str(LIB_G))
+    lib.ref_position_xypix.restype = C.c_long
+    d2, f2 = C.c_double * 2, C.c_float * 2
+    px = f2()
+    rc = lib.ref_position_xypix(d2(*coord), ctype.encode(), d2(*crval), f2(*crpix), f2(*cdelt), f2(*crota),
+                                C.c_float(rotar), px)
+    return (float(px[0]), float(px[1])), int(rc)
 
 
 def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):

@@ -4,6 +4,7 @@ pixel centres and polynomials of its degree anywhere; off-grid positions,
 blanked windows and gains past the limits give the unit matrix; the parallactic
 angle rotates the lookup position."""
 import numpy as np
+import pytest
 
 import oracle
 from obit_b200.beam import BeamImages
@@ -137,3 +138,32 @@ def test_projections_limits_give_unit():
         im = _ramp_images(proj, (0.0, 0.0))
         px, py = _lookup_pixel(im, [[0.05, -0.03]])
         assert abs(px[0] - 106.0) < 2e-3 and abs(py[0] - 98.0) < 2e-3, proj
+
+
+CTYPES = ["RA---LIN", "RA---SIN", "RA---TAN", "RA---ARC", "RA---NCP", "RA---GLS", "RA---MER", "RA---AIT",
+          "RA---STG"]
+
+
+@pytest.mark.skipif(not oracle.have_refgeom(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("projection", range(9))
+def test_projections_match_the_reference_geometry(projection):
+    """The oracle's lookup pixel against the reference's own CUDAPositionXYpix
+    (CUDASkyGeom.h, compiled for the host by oracle/refgeom.cpp) at random
+    positions about three reference positions, with a parallactic angle and a
+    rotated grid; positions the reference cannot project give the unit
+    matrix."""
+    r = np.random.default_rng(600 + projection)
+    unit = np.array([1, 0, 0, 0, 0, 0, 1, 0], np.float32)
+    for crval in ((0.0, 0.0), (123.0, -35.0), (300.0, 71.0)):
+        im = _ramp_images(projection, crval, cdelt=(0.02, 0.025), crota=12.0)
+        crpix = tuple(float(c) for c in im.crpix)
+        pos = (r.uniform(-1.5, 1.5, (64, 2)) + np.array(crval)).astype(np.float32)
+        par = float(r.uniform(-1, 1))
+        J = oracle.beam_jones_fp64(im, pos, par)
+        for c in range(pos.shape[0]):
+            (rx, ry), rc = oracle.ref_position_xypix(pos[c].astype(np.float64), CTYPES[projection], crval, crpix,
+                                                   im.cdelt, (0.0, im.crota), par)
+            if rc != 0 or not (1.0 <= rx <= 201.0 and 1.0 <= ry <= 201.0):
+                np.testing.assert_array_equal(J[0, c, 0], unit)
+                continue
+            assert abs(J[0, c, 0, 0] / 0.001 - rx) < 1e-4 and abs(J[0, c, 0, 1] / 0.001 - ry) < 1e-4, (crval, c)
