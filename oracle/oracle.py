@@ -293,6 +293,18 @@ def ref_position_xypix(coord, ctype: str, crval, crpix, cdelt, crota=(0.0, 0.0),
     return (float(px[0]), float(px[1])), int(rc)
 
 
+def ref_beam_interp_pixel(plane_stack, fblank: float, hwidth: int, pixel) -> float:
+    """The reference's own CUDABeamInterpPixel (compiled for the host) on one
+    image, plane_stack float32 (nplane, ny, nx), at pixel (x, y, plane), all
+    1-relative."""
+    lib = C.CDLL(str(LIB_G))
+    lib.ref_beam_interp_pixel.restype = C.c_float
+    a = np.ascontiguousarray(plane_stack, dtype=np.float32)
+    nplane, ny, nx = a.shape
+    px = (C.c_float * 3)(*pixel)
+    return float(lib.ref_beam_interp_pixel(_p(a, C.c_float), nx, ny, nplane, C.c_float(fblank), hwidth, px))
+
+
 def apply_refcpu(uv, sky, params=None, nthreads: int | None = None):
     """Reference-faithful CPU restatement (FP32 phase, reference sin/cos)
     applied to a copy of uv.vis; returns the new float32 records."""

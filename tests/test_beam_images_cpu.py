@@ -167,3 +167,49 @@ def test_projections_match_the_reference_geometry(projection):
                 np.testing.assert_array_equal(J[0, c, 0], unit)
                 continue
             assert abs(J[0, c, 0, 0] / 0.001 - rx) < 1e-4 and abs(J[0, c, 0, 1] / 0.001 - ry) < 1e-4, (crval, c)
+
+
+@pytest.mark.skipif(not oracle.have_refgeom(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("hwidth", [1, 2, 3, 4])
+def test_interpolation_matches_the_reference(hwidth):
+    """The oracle's Jones entries against the reference's own
+    CUDABeamInterpPixel (CUDABeamInterp.h, compiled for the host by
+    oracle/refgeom.cpp) at the reference's own pixel of each position, for
+    smooth images with blanked patches, on a -SIN grid with a parallactic
+    angle; where the reference blanks any of the 8 images the oracle gives
+    the unit matrix (the reference lets blanks through the cross terms)."""
+    r = np.random.default_rng(900 + hwidth)
+    n, nplane = 31, 2
+    y, x = np.mgrid[0:n, 0:n].astype(np.float64) / n
+    px = np.zeros((1, 8, nplane, n, n), np.float32)
+    for q in range(8):
+        for k in range(nplane):
+            a, b, c = r.uniform(-1, 1, 3)
+            px[0, q, k] = (0.9 if q in (0, 2) else 0.05) + 0.05 * (a * x + b * y * y + c * np.sin(3 * x * y))
+    for _ in range(3):
+        i0, j0 = r.integers(0, n - 4, 2)
+        q = int(r.integers(0, 8))
+        px[0, q, :, i0:i0 + 3, j0:j0 + 3] = FBLANK
+    im = BeamImages(px, np.array([1.4e9, 1.5e9]), crval=(10.0, 20.0), crpix=(16.0, 16.0), cdelt=(0.05, 0.05),
+                    projection=1, hwidth=hwidth, fblank=FBLANK, refSizeFact=0.0)
+    pos = (r.uniform(-0.8, 0.8, (300, 2)) + np.array(im.crval)).astype(np.float32)
+    par = 0.3
+    J = oracle.beam_jones_fp64(im, pos, par)
+    unit = np.array([1, 0, 0, 0, 0, 0, 1, 0], np.float32)
+    order = [0, 1, 4, 5, 6, 7, 2, 3]  # Jones XX, XY, YX, YY (re, im) from P1, X1, X2, P2
+    compared = blanked = 0
+    for c in range(pos.shape[0]):
+        (rx, ry), rc = oracle.ref_position_xypix(pos[c].astype(np.float64), "RA---SIN", im.crval, im.crpix,
+                                               im.cdelt, (0.0, 0.0), par)
+        if rc != 0 or not (1.0 <= rx <= n and 1.0 <= ry <= n):
+            np.testing.assert_array_equal(J[0, c, 0], unit)
+            continue
+        for k in range(nplane):
+            v = [oracle.ref_beam_interp_pixel(px[0, q], FBLANK, hwidth, (rx, ry, k + 1)) for q in range(8)]
+            if any(val == float(np.float32(FBLANK)) for val in v):
+                np.testing.assert_array_equal(J[0, c, k], unit)
+                blanked += 1
+                continue
+            np.testing.assert_allclose(J[0, c, k], [v[q] for q in order], atol=2e-6)
+            compared += 1
+    assert compared > 300 and blanked > 0
