@@ -335,7 +335,6 @@ void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixel
                        int hwidth, int projection, const double crval[2], const double crpix[2],
                        const double cdelt[2], double crota, const double *planeFreq, double refSizeFact,
                        double parAng, const float *pos, int ncomp, float *jones) {
-  const double d2r = 1.745329252e-2;
   const int iwid = 2 * hwidth + 1;
   const size_t img = (size_t)nplane * ny * nx;
   for (int t = 0; t < ntype; t++)
@@ -346,7 +345,7 @@ void oracle_beam_jones(int ntype, int nx, int ny, int nplane, const float *pixel
       const int ok = grid_offsets(projection, crval, cdelt, crota, x, y, &l, &m);
       const double lr = l * cos(parAng) + m * sin(parAng), mr = m * cos(parAng) - l * sin(parAng);
       const double px = lr / cdelt[0] + crpix[0], py = mr / cdelt[1] + crpix[1];
-      if (!ok || px < 1.0 || px > nx || py < 1.0 || py > ny) {
+      if (!ok || !(px >= 1.0 && px <= nx && py >= 1.0 && py <= ny)) { /* NaN is off the grid */
         for (int k = 0; k < nplane; k++) {
           float *J = Jc + 8 * k;
           for (int e = 0; e < 8; e++) J[e] = (e == 0 || e == 6) ? 1.0f : 0.0f;
