@@ -271,7 +271,11 @@ typedef struct ObitDFTBeamImages {
  * 1.3, or an interpolant is blank (the reference tests P1's real part twice
  * where P2's is meant, and lets blanks through the cross terms).  pos:
  * device [ncomp][2], each component's offset from the pointing centre (deg)
- * in the grid's coordinates.  Asynchronous on `stream`. */
+ * in the grid's coordinates.  Antenna types whose images lie on different
+ * grids (the reference holds a descriptor per type, GetJonesKernel reading
+ * type t's from interpolator 8 t) take one call per type with numAntType = 1,
+ * that type's pixels and grid, and jones advanced by t x ncomp x nplane x 8
+ * floats; every type has the same nplane.  Asynchronous on `stream`. */
 int obit_dft_beam_jones(const ObitDFTBeamImages *images, const float *pos, int ncomp, float parAng,
                         float *jones, void *stream);
 

@@ -142,3 +142,42 @@ def test_random_images(seed):
     unit = np.array([1, 0, 0, 0, 0, 0, 1, 0], np.float32)
     np.testing.assert_array_equal(np.all(got == unit, axis=-1), np.all(want == unit, axis=-1))
     assert np.max(np.abs(got - want)) < 2e-5
+
+
+def test_types_on_different_grids_one_call_per_type():
+    """Antenna types whose beam images lie on different grids: one call per
+    type into its slice of the table equals the oracle per type, and on a
+    shared grid equals the single call over all types."""
+    torch = pytest.importorskip("torch")
+    ntype, nplane, ncomp = 3, 2, 257
+    im = _images(ntype, nplane, projection=1)
+    r = np.random.default_rng(21)
+    pos = r.uniform(-1.6, 1.6, (ncomp, 2)).astype(np.float32)
+    par = -0.41
+    d_pos = torch.from_numpy(pos).cuda()
+    d_all = torch.zeros((ntype, ncomp, nplane, 8), dtype=torch.float32, device="cuda")
+    jones_from_images(im, torch.from_numpy(im.pixels).cuda().data_ptr(), d_pos.data_ptr(), ncomp, par,
+                      d_all.data_ptr())
+    d_per = torch.zeros_like(d_all)
+    keep = []
+    for t in range(ntype):
+        sub = BeamImages(np.ascontiguousarray(im.pixels[t:t + 1]), im.planeFreq, crval=im.crval, crpix=im.crpix,
+                         cdelt=(0.05 + 0.01 * t, 0.05 - 0.005 * t), projection=t, hwidth=t + 1, fblank=FBLANK,
+                         refSizeFact=im.refSizeFact)
+        d_px = torch.from_numpy(sub.pixels).cuda()
+        keep.append((sub, d_px))
+        jones_from_images(sub, d_px.data_ptr(), d_pos.data_ptr(), ncomp, par, d_per[t].data_ptr())
+    d_same = torch.zeros_like(d_all)
+    for t in range(ntype):
+        sub = BeamImages(np.ascontiguousarray(im.pixels[t:t + 1]), im.planeFreq, crval=im.crval, crpix=im.crpix,
+                         cdelt=im.cdelt, projection=im.projection, hwidth=im.hwidth, fblank=FBLANK,
+                         refSizeFact=im.refSizeFact)
+        d_px = torch.from_numpy(sub.pixels).cuda()
+        keep.append((sub, d_px))
+        jones_from_images(sub, d_px.data_ptr(), d_pos.data_ptr(), ncomp, par, d_same[t].data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_same.cpu().numpy(), d_all.cpu().numpy())
+    got = d_per.cpu().numpy()
+    for t, (sub, _) in enumerate(keep[:ntype]):
+        want = oracle.beam_jones_fp64(sub, pos, par)[0]
+        assert np.max(np.abs(got[t] - want)) < 2e-5
